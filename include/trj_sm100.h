@@ -1,0 +1,152 @@
+/*
+ * trj_sm100.h -- C ABI of the B200 (sm_100a) g_ab(r) / S_ab(Q) library.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every call returns an int
+ * status (TRJ_OK == 0, negative on error) and never exits the process; the
+ * message of the last error of a context is read with trj_ctx_last_error().
+ * Device pointers are CUDA global-memory addresses on the context's device.
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * Calls are asynchronous on `stream` unless stated otherwise; device-side
+ * status (bad input data, bounded-wait timeouts) is collected by
+ * trj_ctx_check(), which synchronises the stream.
+ *
+ * The reference implements this path as Fortran subroutines that read module
+ * globals (CUDA Fortran, src/modules/rdf.cuf and src/modules/sq.cuf).  Each
+ * entry point below names the reference routine whose role it takes.
+ * Threading: a context and its plans may be used from one host thread at a
+ * time; use one context per thread, or distinct streams.
+ */
+#ifndef TRJ_SM100_H
+#define TRJ_SM100_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRJ_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define TRJ_API __attribute__((visibility("default")))
+#else
+#define TRJ_API
+#endif
+
+/* status codes */
+#define TRJ_OK               0
+#define TRJ_ERR_INVALID     -1   /* bad argument (shape, range, null pointer)          */
+#define TRJ_ERR_CUDA        -2   /* a CUDA runtime call failed                         */
+#define TRJ_ERR_NOMEM       -3   /* device or host allocation failed                  */
+#define TRJ_ERR_CAPACITY    -4   /* input larger than the plan was sized for          */
+#define TRJ_ERR_DATA        -5   /* non-finite positions or species out of range      */
+#define TRJ_ERR_UNSUPPORTED -6   /* configuration not supported by this build/device  */
+#define TRJ_ERR_TIMEOUT     -7   /* a bounded device-side wait ran out                */
+
+/* S(Q) methods */
+#define TRJ_SQ_PLAIN_FP32    0   /* direct sum, one phase per atom and k-vector (CUDA cores) */
+#define TRJ_SQ_SPLIT_BF16X3  1   /* separable phases, tcgen05 BF16 hi/lo 3-term contraction  */
+
+typedef struct trj_ctx trj_ctx;
+typedef struct trj_rdf_plan trj_rdf_plan;
+typedef struct trj_sq_plan trj_sq_plan;
+
+/* Edge-pair statistics of one or more accumulate calls (device uint64[4]). */
+enum {
+    TRJ_EDGE_ULP = 0,      /* pairs whose outcome changes when rr2 moves one FP32 ulp */
+    TRJ_EDGE_FMA = 1,      /* pairs whose outcome changes under the FMA-contracted rr2 */
+    TRJ_EDGE_COUNTED = 2,  /* pairs counted into the histogram                       */
+    TRJ_EDGE_TESTED = 3    /* candidate pairs tested (cell-list work)                */
+};
+
+TRJ_API int trj_abi_version(void);
+
+/* ---- context --------------------------------------------------------- */
+/* Replaces the device selection and module set-up of gpu_and_header
+ * (src/core/util.f90:54-80) and common_init (src/core/common.cuf:380-468). */
+TRJ_API int trj_ctx_create(int device, trj_ctx** out);
+TRJ_API int trj_ctx_destroy(trj_ctx* ctx);
+TRJ_API const char* trj_ctx_last_error(const trj_ctx* ctx);
+/* Synchronise `stream` and report device-side status raised since the last check
+ * (TRJ_ERR_DATA / TRJ_ERR_TIMEOUT / TRJ_ERR_CAPACITY), then clear it. */
+TRJ_API int trj_ctx_check(trj_ctx* ctx, void* stream);
+TRJ_API int trj_ctx_sm_count(const trj_ctx* ctx);
+/* Kernel timing: when enabled, each accumulate call records CUDA events on its
+ * stream around the plan's main kernel (the cell-pair kernel, the tcgen05 S(Q)
+ * kernel, or the direct-sum kernel); trj_*_kernel_ms reads the last duration
+ * (synchronises on the stop event).  Off by default. */
+TRJ_API int trj_ctx_set_timing(trj_ctx* ctx, int enable);
+/* Number of kernels this library has launched on the context so far. */
+TRJ_API int64_t trj_ctx_launches(const trj_ctx* ctx);
+
+/* ---- frame layout ---------------------------------------------------- */
+/* Replaces the per-frame layout of select_ncdfinput (src/core/netcdf.f90:582-692)
+ * and transfer_cpu_gpu (src/core/common.cuf:368-378), on the device:
+ * folds each coordinate with r -= L*int(r/L) (FP32, truncation) and writes the
+ * atoms species-contiguous, in input order within a species (stable).
+ *   xyz_dev      n x 3 float (device)
+ *   species_dev  n int32 species index 0..nsp-1 (device)
+ *   packed_dev   n x 4 float out: x, y, z, species (int bits in w)
+ *   counts_dev   nsp int64 out: atoms per species
+ * The context keeps the per-block counting scratch; it grows (one cudaMalloc)
+ * the first time a larger frame or species count is seen. */
+TRJ_API int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
+                   int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
+                   void* stream);
+
+/* ---- g_ab(r) --------------------------------------------------------- */
+/* Replaces RDF_init (src/modules/rdf.cuf:51-122) with the rcrdf clip of
+ * select_ncdfinput (src/core/netcdf.f90:610-617): rcrdf_eff = min(rcrdf, min(box)/2),
+ * side2 = rcrdf_eff^2, lsmax = nint(rcrdf_eff/deltar)+1, all in FP32.
+ * n_max: largest frame the plan will accept. */
+TRJ_API int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                        int64_t n_max, trj_rdf_plan** out);
+/* lsmax, nit = nsp(nsp+1)/2, cells per axis (1 = no cell split on that axis),
+ * effective cutoff, side2, device scratch bytes held by the plan. */
+TRJ_API int trj_rdf_plan_info(const trj_rdf_plan* plan, int* lsmax, int* nit, int cells[3],
+                      float* rcrdf_eff, float* side2, int64_t* scratch_bytes);
+/* Replaces RDFcomp's device part (src/modules/rdf.cuf:184-270; kernel rdf_sh
+ * 426-487): adds this frame's unordered-pair counts to hist_dev
+ * (uint64 [nit][lsmax]; row = ind_ij(a,b)-1 of rdf.cuf:741-753, column = bin-1)
+ * and its edge statistics to edge_dev (uint64[4], may be NULL).
+ * packed_dev: output of trj_frame_pack.  box: this frame's box. */
+TRJ_API int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                       uint64_t* hist_dev, uint64_t* edge_dev, void* stream);
+/* Duration (ms) of the last cell-pair kernel launch; needs trj_ctx_set_timing(ctx, 1). */
+TRJ_API int trj_rdf_kernel_ms(trj_rdf_plan* plan, float* ms);
+TRJ_API int trj_rdf_plan_destroy(trj_rdf_plan* plan);
+
+/* ---- S_ab(Q) --------------------------------------------------------- */
+/* Replaces sq_init (src/modules/sq.cuf:150-369) given the k-set it builds:
+ * nvec integer lattice vectors n (k = 2*pi*n/L per axis), each with an output
+ * bin (0..nbins-1) and a weight (multiplicity; 2 for a vector standing for
+ * +k and -k).  dense[v] != 0 marks vectors of a compact region that the
+ * tensor-core method may evaluate through separable phase tiles; the others
+ * are evaluated by the direct sum in either method.
+ * species_counts: atoms per species of the frames to come (host, nsp). */
+TRJ_API int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int32_t* vec_host,
+                       const int32_t* bin_host, const double* weight_host,
+                       const uint8_t* dense_host, int nbins, const int64_t* species_counts,
+                       trj_sq_plan** out);
+/* Vectors evaluated by tensor tiles, tile count, padded tile work (k-slots),
+ * device scratch bytes held by the plan. */
+TRJ_API int trj_sq_plan_info(const trj_sq_plan* plan, int64_t* n_dense, int64_t* n_tiles,
+                     int64_t* tile_slots, int64_t* scratch_bytes);
+/* Replaces SQcalc (src/modules/sq.cuf:58-126; kernels sqfnD 523-591, sqfact
+ * 372-454): adds, for every bin and species pair (a<=b, row ind_ij(a,b)-1),
+ * sum over the bin's vectors of weight * Re(rho_a(k) conj(rho_b(k))) to
+ * out_dev (double [nbins][nit]), rho_a(k) = sum_{j in a} exp(i k.r_j).
+ * method: TRJ_SQ_PLAIN_FP32 or TRJ_SQ_SPLIT_BF16X3. */
+TRJ_API int trj_sq_accumulate(trj_sq_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                      int method, double* out_dev, void* stream);
+/* rho_a(k) of the last accumulate, FP64, [nsp][nvec][2] in the caller's vector order. */
+TRJ_API int trj_sq_rho(trj_sq_plan* plan, double* rho_dev, void* stream);
+/* Duration (ms) of the last main S(Q) kernel launch (tcgen05 contraction for
+ * TRJ_SQ_SPLIT_BF16X3, direct sum for TRJ_SQ_PLAIN_FP32); needs timing enabled. */
+TRJ_API int trj_sq_kernel_ms(trj_sq_plan* plan, float* ms);
+TRJ_API int trj_sq_plan_destroy(trj_sq_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRJ_SM100_H */

@@ -1,0 +1,361 @@
+/*
+ * oracle.c -- CPU restatement of the reference's g_ab(r) and S_ab(Q) arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product path links, loads or calls
+ * this file; only tests/, the smoke check and bench.py's CPU-baseline leg do,
+ * and only as the checker (or as the timed CPU baseline).
+ *
+ * Compiled with -ffp-contract=off so that every FP32 expression rounds once per
+ * operation in the order written (no fused multiply-add), as the reference's
+ * Fortran states it.
+ *
+ * Reference functions restated here (file:line within the reference project):
+ *   pair arithmetic      src/modules/rdf.cuf:451-475   (rdf_sh inner loop)
+ *   pair index           src/modules/rdf.cuf:741-753   (ind_ij)
+ *   histogram layout     src/modules/rdf.cuf:51-66     (lsmax = nint(rcrdf/deltar)+1)
+ *   S(Q) direct sum      src/modules/sq.cuf:523-591    (sqfnD; FP32 phase, FP64 sums)
+ *                        src/modules/sq.cuf:372-454    (sqfact; axis vectors)
+ *
+ * The exact S(Q) oracle is FP64 throughout: phases from the fractional
+ * coordinate s = x/L in FP64, n.s reduced mod 1 in FP64, sin/cos in FP64.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* g(r): reference pair arithmetic                                     */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    float L[3];
+    float side2;
+    float deltar;
+    int lsmax;
+    int nsp;
+} orc_rdf_params;
+
+/* ind_ij (rdf.cuf:741-753), 0-based species a,b -> 0-based pair row. */
+static inline int pair_row(int a, int b, int nsp) {
+    if (a > b) { int t = a; a = b; b = t; }
+    return a * (nsp - 1) - a * (a - 1) / 2 + b;
+}
+
+/* xd = xd - sidel*nint(xd/sidel)  (rdf.cuf:457-459); NINT rounds half away from zero. */
+static inline float min_image(float d, float L) {
+    float q = d / L;
+    float n = roundf(q);
+    float s = L * n;
+    return d - s;
+}
+
+/* Outcome of one pair: bin 1..lsmax, or 0 when not counted (rdf.cuf:461-467). */
+static inline int pair_outcome(float rr2, const orc_rdf_params* p) {
+    if (!(rr2 < p->side2)) return 0;
+    float rr = sqrtf(rr2);
+    float q = rr / p->deltar;
+    int ind = (int)roundf(q);
+    if (ind <= p->lsmax && ind > 0) return ind;
+    return 0;
+}
+
+typedef struct {
+    uint64_t edge_ulp;   /* outcome changes when rr2 moves by one FP32 ulp */
+    uint64_t edge_fma;   /* outcome changes under the FMA-contracted rr2    */
+    uint64_t counted;    /* pairs counted into the histogram               */
+} orc_edge_stats;
+
+/* One unordered pair: accumulate its count and edge statistics. */
+static inline void do_pair(const float* pi, int si, const float* pj, int sj,
+                           const orc_rdf_params* p, uint64_t* hist, orc_edge_stats* e) {
+    float xd = pj[0] - pi[0];
+    float yd = pj[1] - pi[1];
+    float zd = pj[2] - pi[2];
+    xd = min_image(xd, p->L[0]);
+    yd = min_image(yd, p->L[1]);
+    zd = min_image(zd, p->L[2]);
+    float x2 = xd * xd, y2 = yd * yd, z2 = zd * zd;
+    float rr2 = (x2 + y2) + z2;
+    /* Anything at or beyond 1.001*side2 cannot reach the cutoff by an ulp or by FMA. */
+    if (!(rr2 < p->side2 * 1.001f)) return;
+    int o = pair_outcome(rr2, p);
+    if (o) {
+        hist[(size_t)pair_row(si, sj, p->nsp) * p->lsmax + (o - 1)] += 1;
+        e->counted += 1;
+    }
+    int olo = pair_outcome(nextafterf(rr2, -INFINITY), p);
+    int ohi = pair_outcome(nextafterf(rr2, INFINITY), p);
+    if (olo != o || ohi != o) e->edge_ulp += 1;
+    float rr2f = fmaf(zd, zd, fmaf(yd, yd, x2));
+    if (pair_outcome(rr2f, p) != o) e->edge_fma += 1;
+}
+
+/*
+ * All-pairs g(r) over one frame (the reference's O(N^2) algorithm).
+ * pos: N x 3 FP32 (already folded, species-contiguous or not: order is irrelevant).
+ * sp:  N species indices (0-based).
+ * hist: nit x lsmax uint64, accumulated (+=).
+ */
+ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
+                                 const float box[3], float side2, float deltar,
+                                 int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
+    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp};
+    int nit = nsp * (nsp + 1) / 2;
+    int nthr = 1;
+#ifdef _OPENMP
+    nthr = omp_get_max_threads();
+#endif
+    size_t hsz = (size_t)nit * lsmax;
+    uint64_t* priv = (uint64_t*)calloc((size_t)nthr * hsz, sizeof(uint64_t));
+    orc_edge_stats* es = (orc_edge_stats*)calloc((size_t)nthr, sizeof(orc_edge_stats));
+#pragma omp parallel
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        uint64_t* h = priv + (size_t)t * hsz;
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t j = i + 1; j < n; ++j)
+                do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]);
+    }
+    for (int t = 0; t < nthr; ++t) {
+        for (size_t k = 0; k < hsz; ++k) hist[k] += priv[(size_t)t * hsz + k];
+        edge3[0] += es[t].edge_ulp;
+        edge3[1] += es[t].edge_fma;
+        edge3[2] += es[t].counted;
+    }
+    free(priv);
+    free(es);
+}
+
+/*
+ * Linked-cell g(r) with identical per-pair arithmetic.  Cells are built from
+ * the wrapped coordinate; a pair is tested once, from its lower original index,
+ * over the 27-cell neighbourhood.  Requires >= 3 cells per axis (else falls
+ * back to all pairs).  Cell edge >= rcut*(1+2^-10) so that no pair whose FP32
+ * rr2 is below side2 is outside the neighbourhood.
+ */
+/* Same, restricted to home atoms i in [i0, i1) (pairs (i, j>i)); used to time a bounded
+ * sample of a large frame for the CPU baseline.  i0=0, i1=n is the whole frame. */
+ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t n,
+                                    const float box[3], float side2, float deltar,
+                                    int lsmax, int nsp, uint64_t* hist, uint64_t* edge3,
+                                    int64_t i0, int64_t i1);
+
+ORC_EXPORT void orc_rdf_cells(const float* pos, const int32_t* sp, int64_t n,
+                              const float box[3], float side2, float deltar,
+                              int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
+    orc_rdf_cells_range(pos, sp, n, box, side2, deltar, lsmax, nsp, hist, edge3, 0, n);
+}
+
+ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t n,
+                                    const float box[3], float side2, float deltar,
+                                    int lsmax, int nsp, uint64_t* hist, uint64_t* edge3,
+                                    int64_t i0, int64_t i1) {
+    double rc = sqrt((double)side2) * (1.0 + 1.0 / 1024.0);
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+        nc[d] = (int)floor((double)box[d] / rc);
+        if (nc[d] < 3) { orc_rdf_allpairs(pos, sp, n, box, side2, deltar, lsmax, nsp, hist, edge3); return; }
+    }
+    int64_t ncell = (int64_t)nc[0] * nc[1] * nc[2];
+    int64_t* head = (int64_t*)malloc(sizeof(int64_t) * ncell);
+    int64_t* next = (int64_t*)malloc(sizeof(int64_t) * n);
+    int32_t* cellof = (int32_t*)malloc(sizeof(int32_t) * n * 3);
+    for (int64_t c = 0; c < ncell; ++c) head[c] = -1;
+    for (int64_t i = n - 1; i >= 0; --i) {
+        int cc[3];
+        for (int d = 0; d < 3; ++d) {
+            double L = box[d];
+            double w = (double)pos[3 * i + d];
+            w = w - L * floor(w / L);
+            int k = (int)floor(w / L * nc[d]);
+            if (k < 0) k = 0;
+            if (k >= nc[d]) k = nc[d] - 1;
+            cc[d] = k;
+            cellof[3 * i + d] = k;
+        }
+        int64_t c = ((int64_t)cc[0] * nc[1] + cc[1]) * nc[2] + cc[2];
+        next[i] = head[c];
+        head[c] = i;
+    }
+    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp};
+    int nit = nsp * (nsp + 1) / 2;
+    int nthr = 1;
+#ifdef _OPENMP
+    nthr = omp_get_max_threads();
+#endif
+    size_t hsz = (size_t)nit * lsmax;
+    uint64_t* priv = (uint64_t*)calloc((size_t)nthr * hsz, sizeof(uint64_t));
+    orc_edge_stats* es = (orc_edge_stats*)calloc((size_t)nthr, sizeof(orc_edge_stats));
+#pragma omp parallel
+    {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        uint64_t* h = priv + (size_t)t * hsz;
+#pragma omp for schedule(dynamic, 256)
+        for (int64_t i = i0; i < i1; ++i) {
+            for (int dx = -1; dx <= 1; ++dx)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        int cx = (cellof[3 * i] + dx + nc[0]) % nc[0];
+                        int cy = (cellof[3 * i + 1] + dy + nc[1]) % nc[1];
+                        int cz = (cellof[3 * i + 2] + dz + nc[2]) % nc[2];
+                        int64_t c = ((int64_t)cx * nc[1] + cy) * nc[2] + cz;
+                        for (int64_t j = head[c]; j >= 0; j = next[j])
+                            if (j > i) do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]);
+                    }
+        }
+    }
+    for (int t = 0; t < nthr; ++t) {
+        for (size_t k = 0; k < hsz; ++k) hist[k] += priv[(size_t)t * hsz + k];
+        edge3[0] += es[t].edge_ulp;
+        edge3[1] += es[t].edge_fma;
+        edge3[2] += es[t].counted;
+    }
+    free(priv);
+    free(es);
+    free(head);
+    free(next);
+    free(cellof);
+}
+
+/* ------------------------------------------------------------------ */
+/* S(Q): exact FP64 rho_a(k)                                           */
+/* ------------------------------------------------------------------ */
+
+/*
+ * rho[a][v] = sum_{j in species a} exp(i 2 pi n_v . s_j),  s_j = x_j / L (FP64).
+ * pos: N x 3 FP32 species-contiguous; sp_off: nsp+1 offsets; vec: nvec x 3 ints.
+ * rho: nsp x nvec x 2 doubles (re, im), overwritten.
+ *
+ * Separable evaluation: per atom, e^{i 2 pi n s} for every needed n on each
+ * axis is computed by a direct FP64 sincos of the reduced fraction, and the
+ * 3-factor product is taken in FP64.
+ */
+ORC_EXPORT void orc_rho_fp64(const float* pos, int64_t n, const int64_t* sp_off, int nsp,
+                             const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int64_t v = 0; v < nvec; ++v)
+        for (int d = 0; d < 3; ++d) {
+            if (vec[3 * v + d] < lo[d]) lo[d] = vec[3 * v + d];
+            if (vec[3 * v + d] > hi[d]) hi[d] = vec[3 * v + d];
+        }
+    int span[3], off[3];
+    for (int d = 0; d < 3; ++d) { span[d] = hi[d] - lo[d] + 1; off[d] = -lo[d]; }
+    int tsz = span[0] + span[1] + span[2];
+    memset(rho, 0, sizeof(double) * 2 * (size_t)nsp * nvec);
+    const int B = 64;
+    for (int a = 0; a < nsp; ++a) {
+        int64_t j0 = sp_off[a], j1 = sp_off[a + 1];
+        int64_t nblk = (j1 - j0 + B - 1) / B;
+        int nthr = 1;
+#ifdef _OPENMP
+        nthr = omp_get_max_threads();
+#endif
+        double* acc = (double*)calloc((size_t)nthr * nvec * 2, sizeof(double));
+#pragma omp parallel
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            double* my = acc + (size_t)t * nvec * 2;
+            double* tab = (double*)malloc(sizeof(double) * 2 * (size_t)tsz * B);
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t b = 0; b < nblk; ++b) {
+                int64_t jb = j0 + b * B, je = jb + B < j1 ? jb + B : j1;
+                int cnt = (int)(je - jb);
+                for (int q = 0; q < cnt; ++q) {
+                    const float* r = pos + 3 * (jb + q);
+                    double* tq = tab + (size_t)2 * tsz * q;
+                    int base = 0;
+                    for (int d = 0; d < 3; ++d) {
+                        double s = (double)r[d] / (double)box[d];
+                        for (int m = 0; m < span[d]; ++m) {
+                            double t2 = (double)(m - off[d]) * s;
+                            t2 -= nearbyint(t2);
+                            double ang = 2.0 * M_PI * t2;
+                            tq[2 * (base + m)] = cos(ang);
+                            tq[2 * (base + m) + 1] = sin(ang);
+                        }
+                        base += span[d];
+                    }
+                }
+                for (int64_t v = 0; v < nvec; ++v) {
+                    int ix = vec[3 * v] + off[0];
+                    int iy = span[0] + vec[3 * v + 1] + off[1];
+                    int iz = span[0] + span[1] + vec[3 * v + 2] + off[2];
+                    double sr = 0.0, si = 0.0;
+                    for (int q = 0; q < cnt; ++q) {
+                        const double* tq = tab + (size_t)2 * tsz * q;
+                        double xr = tq[2 * ix], xi = tq[2 * ix + 1];
+                        double yr = tq[2 * iy], yi = tq[2 * iy + 1];
+                        double zr = tq[2 * iz], zi = tq[2 * iz + 1];
+                        double pr = xr * yr - xi * yi, pi2 = xr * yi + xi * yr;
+                        sr += pr * zr - pi2 * zi;
+                        si += pr * zi + pi2 * zr;
+                    }
+                    my[2 * v] += sr;
+                    my[2 * v + 1] += si;
+                }
+            }
+            free(tab);
+        }
+        for (int t = 0; t < nthr; ++t)
+            for (int64_t v = 0; v < nvec; ++v) {
+                rho[((size_t)a * nvec + v) * 2] += acc[((size_t)t * nvec + v) * 2];
+                rho[((size_t)a * nvec + v) * 2 + 1] += acc[((size_t)t * nvec + v) * 2 + 1];
+            }
+        free(acc);
+    }
+}
+
+/*
+ * The reference's own S(Q) arithmetic on the CPU (sqfnD, sq.cuf:537-581):
+ * kf = n*fk in FP32, phase = (y*kf2 + x*kf1) + z*kf3 in FP32, cos/sin of that
+ * FP32 phase (libm sinf/cosf here, the GPU intrinsics __cosf/__sinf there),
+ * FP64 sums per species.  Used as the timed CPU baseline, not as truth.
+ * rho: nsp x nvec x 2 doubles, overwritten.
+ */
+ORC_EXPORT void orc_rho_ref32(const float* pos, int64_t n, const int64_t* sp_off, int nsp,
+                              const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
+    const float twopi = 2.0f * 3.14159274f;
+    float fk[3] = {twopi / box[0], twopi / box[1], twopi / box[2]};
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t v = 0; v < nvec; ++v) {
+        float kf1 = (float)vec[3 * v] * fk[0];
+        float kf2 = (float)vec[3 * v + 1] * fk[1];
+        float kf3 = (float)vec[3 * v + 2] * fk[2];
+        for (int a = 0; a < nsp; ++a) {
+            double sc = 0.0, ss = 0.0;
+            for (int64_t j = sp_off[a]; j < sp_off[a + 1]; ++j) {
+                const float* r = pos + 3 * j;
+                float ph = r[1] * kf2 + r[0] * kf1;
+                ph = ph + r[2] * kf3;
+                sc += (double)cosf(ph);
+                ss += (double)sinf(ph);
+            }
+            rho[((size_t)a * nvec + v) * 2] = sc;
+            rho[((size_t)a * nvec + v) * 2 + 1] = ss;
+        }
+    }
+}
+
+ORC_EXPORT int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

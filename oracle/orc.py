@@ -1,0 +1,181 @@
+"""Python side of the CPU oracle.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, the smoke check and bench.py's CPU-baseline leg import this module,
+and only as the checker (or the timed CPU baseline).  It restates the
+reference's algorithm for the g_ab(r) / S_ab(Q) path on the CPU:
+
+* layout (select_ncdfinput, src/core/netcdf.f90:582-692): FP32 fold
+  r - L*int(r/L) and a stable species-contiguous order;
+* pair counts (rdf_sh, src/modules/rdf.cuf:451-475) in oracle.c, all-pairs or
+  linked cells, with the reference's FP32 operation order and NINT;
+* rho_a(k) exactly in FP64 (oracle.c, orc_rho_fp64);
+* the reference's FP32-phase S(Q) arithmetic (sqfnD, src/modules/sq.cuf:537-581)
+  for the timed CPU baseline (orc_rho_ref32);
+* a pure-Python loop restatement of sq_init's n(Q) count (sq.cuf:328-342) for
+  small cross-checks of the product's vectorised version.
+
+Pinning: the n(Q) counts, Q columns and g(r) row grids of the reference's example
+outputs (tests/golden/examples.json, made by tests/golden/make_golden.py) are
+reproduced by the k-set/bin logic; pair counts and rho values are pinned to the
+restated arithmetic only (the reference's trajectories are not shipped).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liborc.so")
+F32 = np.float32
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "oracle.c")):
+            build()
+        L = ctypes.CDLL(LIB)
+        vp, i64, f32, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_int
+        for name in ("orc_rdf_allpairs", "orc_rdf_cells"):
+            fn = getattr(L, name)
+            fn.restype = None
+            fn.argtypes = [vp, vp, i64, vp, f32, f32, i32, i32, vp, vp]
+        L.orc_rdf_cells_range.restype = None
+        L.orc_rdf_cells_range.argtypes = [vp, vp, i64, vp, f32, f32, i32, i32, vp, vp, i64, i64]
+        for name in ("orc_rho_fp64", "orc_rho_ref32"):
+            fn = getattr(L, name)
+            fn.restype = None
+            fn.argtypes = [vp, i64, vp, i32, vp, i64, vp, vp]
+        L.orc_num_threads.restype = i32
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def layout(xyz: np.ndarray, species: np.ndarray, box, nsp: int):
+    """Fold + stable species-contiguous order; returns (pos N x 3 FP32, species N, offsets nsp+1)."""
+    xyz = np.asarray(xyz, F32)
+    box32 = np.asarray(box, F32)
+    q = (xyz / box32).astype(F32)
+    folded = (xyz - (box32 * np.trunc(q)).astype(F32)).astype(F32)
+    order = np.argsort(species, kind="stable")
+    sp = np.asarray(species, np.int32)[order]
+    off = np.zeros(nsp + 1, np.int64)
+    off[1:] = np.cumsum(np.bincount(sp, minlength=nsp))
+    return np.ascontiguousarray(folded[order]), np.ascontiguousarray(sp), off
+
+
+def rdf_counts(pos: np.ndarray, species: np.ndarray, box, side2: float, deltar: float, lsmax: int, nsp: int,
+               cells: bool = False):
+    """uint64 [nit][lsmax] pair counts and (edge_ulp, edge_fma, counted) of one frame."""
+    pos = np.ascontiguousarray(pos, F32)
+    sp = np.ascontiguousarray(species, np.int32)
+    nit = nsp * (nsp + 1) // 2
+    hist = np.zeros((nit, lsmax), np.uint64)
+    edge = np.zeros(3, np.uint64)
+    b = np.asarray(box, F32)
+    fn = lib().orc_rdf_cells if cells else lib().orc_rdf_allpairs
+    fn(_p(pos), _p(sp), pos.shape[0], _p(b), float(F32(side2)), float(F32(deltar)), int(lsmax), int(nsp),
+       _p(hist), _p(edge))
+    return hist, edge
+
+
+def rdf_counts_range(pos, species, box, side2, deltar, lsmax, nsp, i0, i1):
+    """Linked-cell counts of pairs (i, j>i) with home atom i in [i0, i1)."""
+    pos = np.ascontiguousarray(pos, F32)
+    sp = np.ascontiguousarray(species, np.int32)
+    hist = np.zeros((nsp * (nsp + 1) // 2, lsmax), np.uint64)
+    edge = np.zeros(3, np.uint64)
+    b = np.asarray(box, F32)
+    lib().orc_rdf_cells_range(_p(pos), _p(sp), pos.shape[0], _p(b), float(F32(side2)), float(F32(deltar)),
+                              int(lsmax), int(nsp), _p(hist), _p(edge), int(i0), int(i1))
+    return hist, edge
+
+
+def rho_fp64(pos: np.ndarray, offsets: np.ndarray, box, vectors: np.ndarray) -> np.ndarray:
+    """Exact rho_a(k): (nsp, nvec) complex128."""
+    pos = np.ascontiguousarray(pos, F32)
+    off = np.ascontiguousarray(offsets, np.int64)
+    v = np.ascontiguousarray(vectors, np.int32)
+    nsp = off.shape[0] - 1
+    out = np.zeros((nsp, v.shape[0], 2), np.float64)
+    b = np.asarray(box, F32)
+    lib().orc_rho_fp64(_p(pos), pos.shape[0], _p(off), nsp, _p(b), v.shape[0], _p(v), _p(out))
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def rho_ref32(pos: np.ndarray, offsets: np.ndarray, box, vectors: np.ndarray) -> np.ndarray:
+    """The reference's FP32-phase arithmetic (CPU baseline): (nsp, nvec) complex128."""
+    pos = np.ascontiguousarray(pos, F32)
+    off = np.ascontiguousarray(offsets, np.int64)
+    v = np.ascontiguousarray(vectors, np.int32)
+    nsp = off.shape[0] - 1
+    out = np.zeros((nsp, v.shape[0], 2), np.float64)
+    b = np.asarray(box, F32)
+    lib().orc_rho_ref32(_p(pos), pos.shape[0], _p(off), nsp, _p(b), v.shape[0], _p(v), _p(out))
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def bin_sums(rho: np.ndarray, bins: np.ndarray, weights: np.ndarray, nbins: int) -> np.ndarray:
+    """[nbins][nit] sums of w Re(rho_a conj(rho_b)) in ind_ij row order."""
+    nsp = rho.shape[0]
+    rows = [(a, b) for a in range(nsp) for b in range(a, nsp)]
+    out = np.zeros((nbins, len(rows)))
+    for r, (a, b) in enumerate(rows):
+        val = weights * (rho[a] * np.conj(rho[b])).real
+        np.add.at(out[:, r], bins, val)
+    return out
+
+
+def nq_loops(L: float, qmax: float, qmin: float) -> list:
+    """n(Q) of sq_init for a cubic box, as plain loops over FP32 scalars (sq.cuf:159-193, 328-342)."""
+    f = F32
+    pi = f(3.1415926535898)
+    fk = f(f(f(2.0) * pi) / f(L))
+    dq = fk
+    nqmax = _nint(f(f(qmax) / dq))
+    l = _nint(f(f(qmin) / fk))
+    if l % 4 != 0:
+        l = l - 4 + l % 4
+    qm = f(fk * f(l))
+    nq = [0] * (nqmax + 1)
+    if l <= 1:
+        return [0] + [3] * nqmax
+    indm = 0
+    for i in range(l):
+        a = f(f(f(i) * fk) * f(f(i) * fk))
+        for j in range(l):
+            b = f(f(f(j) * fk) * f(f(j) * fk))
+            ab = f(a + b)
+            for k in range(l):
+                if i + j + k == 0:
+                    continue
+                c = f(f(f(k) * fk) * f(f(k) * fk))
+                rr = f(math.sqrt(float(f(ab + c))))
+                if rr < qm:
+                    ind = _nint(f(rr / dq))
+                    indm = max(indm, ind)
+                    if ind <= nqmax:
+                        nq[ind] += 1
+    for i in range(indm + 1, nqmax + 1):
+        nq[i] = 3
+    return nq
+
+
+def _nint(x) -> int:
+    x = float(x)
+    return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))

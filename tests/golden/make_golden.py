@@ -1,0 +1,68 @@
+"""Extracts known-answer vectors from the reference's shipped example outputs.
+
+Run in a checkout that has the reference project next to it:
+
+    python tests/golden/make_golden.py /path/to/trj_analysis
+
+It reads ``examples/3D/<name>/{input.nml, sq.dat, sqmix.dat, gmixsim.dat}`` and
+writes ``tests/golden/examples.json``: per example, the /INPUT_RDF/ and
+/INPUT_SQ/ parameters, nsp, the header lines, the Q column (as printed), the
+n(Q) column, and the r column / row count of gmixsim.dat.  The g and S values
+themselves are not kept: the trajectories that produced them are not shipped,
+so they cannot be regenerated.  Only the columns that depend on the box and
+the input parameters alone are kept.
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+EXAMPLES = ["LJmix", "salr", "meam-dyn", "Conf", "RTIL+H20_rigid"]
+
+
+def _nml_value(text: str, group: str, key: str):
+    m = re.search(r"&%s(.*?)\n\s*/" % group, text, re.S | re.I)
+    if not m:
+        return None
+    body = m.group(1)
+    m2 = re.search(r"^\s*%s\s*=\s*([^!\n]*)" % key, body, re.M | re.I)
+    if not m2:
+        return None
+    return m2.group(1).strip()
+
+
+def main(ref_root: str) -> None:
+    out = {}
+    for name in EXAMPLES:
+        d = os.path.join(ref_root, "examples", "3D", name)
+        nml = open(os.path.join(d, "input.nml")).read()
+        ex = {
+            "nsp": int(_nml_value(nml, "INPUT", "nsp")),
+            "deltar": float(_nml_value(nml, "INPUT_RDF", "deltar")),
+            "rcrdf": float(_nml_value(nml, "INPUT_RDF", "rcrdf")),
+            "qmax": float(_nml_value(nml, "INPUT_SQ", "qmax")),
+            "qmin": float(_nml_value(nml, "INPUT_SQ", "qmin")),
+        }
+        sq = open(os.path.join(d, "sq.dat")).read().splitlines()
+        ex["sq_header"] = sq[0]
+        rows = [r.split() for r in sq[1:] if r.strip()]
+        ex["sq_q"] = [r[0] for r in rows]
+        ex["sq_nq"] = [int(r[-1]) for r in rows]
+        mix = open(os.path.join(d, "sqmix.dat")).read().splitlines()
+        ex["sqmix_header"] = mix[0]
+        gpath = os.path.join(d, "gmixsim.dat")
+        if os.path.exists(gpath):
+            g = open(gpath).read().splitlines()
+            ex["gmix_header"] = g[0]
+            ex["gmix_r"] = [r.split()[0] for r in g[1:] if r.strip()]
+        out[name] = ex
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "examples.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", path)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TRJ_REFERENCE", "."))

@@ -1,0 +1,97 @@
+"""Known-answer checks of the oracle and the host-side k-set/bin logic against the
+reference's shipped example outputs (tests/golden/examples.json).
+
+Pinned columns: n(Q) (sq.dat last column) and Q = i*dq (first column) of
+examples/3D/{LJmix, meam-dyn, salr}, and the r grid / row count of gmixsim.dat.
+The boxes are cubic; L is recovered as the FP32 value whose 2*pi/L reproduces
+every printed Q.  salr's sq.dat was written by an older version that printed
+only the first 51 Q values on the i*dq grid; its n(Q) column matches on all rows.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import orc
+from trj_analysis_b200 import refsem
+from trj_analysis_b200.refsem import F32
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "examples.json")))
+
+
+def recover_box(qcol, rows=None):
+    rows = len(qcol) if rows is None else rows
+    guess = F32(float(qcol[0]))
+    base = int(np.frombuffer(np.array([guess], F32).tobytes(), np.uint32)[0])
+    for off in range(-4000, 4000):
+        dq = np.frombuffer(np.array([base + off], np.uint32).tobytes(), F32)[0]
+        if all(f"{F32(F32(i + 1) * dq):.7f}" == qcol[i] for i in range(rows)):
+            L = F32(refsem.TWOPI32 / dq)
+            for c in (L, np.nextafter(L, F32(np.inf)), np.nextafter(L, F32(0))):
+                if F32(refsem.TWOPI32 / c) == dq:
+                    return F32(c)
+    raise AssertionError("no FP32 box reproduces the Q column")
+
+
+CASES = [("LJmix", None), ("meam-dyn", None), ("salr", 51)]
+
+
+@pytest.mark.parametrize("name,qrows", CASES)
+def test_nq_column_matches_reference(name, qrows):
+    ex = GOLD[name]
+    L = recover_box(ex["sq_q"], qrows)
+    ks = refsem.reference_kset([L, L, L], ex["qmax"], ex["qmin"])
+    gold = np.array(ex["sq_nq"])
+    got = ks.nq[1:1 + gold.size]
+    assert np.array_equal(got, gold)
+
+
+@pytest.mark.parametrize("name,qrows", CASES)
+def test_q_column_matches_reference(name, qrows):
+    ex = GOLD[name]
+    L = recover_box(ex["sq_q"], qrows)
+    ks = refsem.reference_kset([L, L, L], ex["qmax"], ex["qmin"])
+    q = ks.q_column()
+    rows = len(ex["sq_q"]) if qrows is None else qrows
+    assert [f"{v:.7f}" for v in q[:rows]] == ex["sq_q"][:rows]
+    if name == "LJmix":
+        # meam-dyn's file stops one row short of nint(qmax/dq) (an older writer).
+        assert ks.nqmax == len(ex["sq_q"])
+
+
+def test_nq_loops_restatement_agrees():
+    ex = GOLD["LJmix"]
+    L = recover_box(ex["sq_q"])
+    loops = orc.nq_loops(float(L), ex["qmax"], ex["qmin"])
+    ks = refsem.reference_kset([L, L, L], ex["qmax"], ex["qmin"])
+    assert list(ks.nq) == loops
+
+
+@pytest.mark.parametrize("name,qrows", CASES)
+def test_gmix_grid_matches_reference(name, qrows):
+    ex = GOLD[name]
+    L = recover_box(ex["sq_q"], qrows)
+    p = refsem.rdf_params(ex["nsp"], ex["deltar"], ex["rcrdf"], [L, L, L])
+    rows = p.lsmax - 2
+    assert rows == len(ex["gmix_r"])
+    r = [f"{F32(F32(i) * F32(ex['deltar'])):.5f}" for i in range(1, rows + 1)]
+    assert r == ex["gmix_r"]
+
+
+def test_headers_match_reference():
+    from trj_analysis_b200 import writers
+    assert GOLD["LJmix"]["sq_header"] == writers.SQ_HEADER_BINARY
+    assert GOLD["salr"]["sq_header"] == writers.SQ_HEADER
+    assert writers.sqmix_header(2)[0] == GOLD["LJmix"]["sqmix_header"]
+    assert writers.sqmix_header(1)[0] == GOLD["salr"]["sqmix_header"]
+    labels = [f"g_{j + 1}{k + 1}(r)" for j in range(2) for k in range(j, 2)]
+    assert writers._group_header("#       r        " + " " * 9, labels, 16, " " * 9)[0] == GOLD["LJmix"]["gmix_header"]
+
+
+def test_meam_dyn_needs_fp32_geometry():
+    """The FP64 evaluation of rr < qmin would give a different last full shell (2922 vs 2928)."""
+    ex = GOLD["meam-dyn"]
+    L = recover_box(ex["sq_q"])
+    ks = refsem.reference_kset([L, L, L], ex["qmax"], ex["qmin"])
+    assert 2928 in list(ks.nq)

@@ -1,0 +1,282 @@
+"""Reference-facing operators for the g_ab(r) / S_ab(Q) path.
+
+The reference drives this path through Fortran subroutines that share module
+globals: ``RDF_init`` / ``RDFcomp`` / ``printrdf`` (src/modules/rdf.cuf:51,184;
+src/core/log.f90:414) and ``sq_init`` / ``SQcalc`` / ``sq_transfer_gpu_cpu`` /
+``printSQ`` (src/modules/sq.cuf:150,58,128; src/core/log.f90:317), called from
+the frame loop of src/main/trj_analysis.f90:173-242 after ``select_ncdfinput``
+(src/core/netcdf.f90:582).  :class:`Session` holds that state explicitly and
+keeps the routine names; the arithmetic runs in libtrj_sm100.so.
+
+Differences from the reference, by design:
+* pair counts are exact uint64 (the reference sums FP32 copies of per-block int32
+  histograms on the host, rdf.cuf:301-310, which loses exactness above 2^24);
+* S(Q) sums are FP64 with a fixed reduction order (the reference adds FP32 atomics,
+  sq.cuf:447,449,584);
+* normalisations (printrdf, printSQ) are evaluated in FP64;
+* histograms and S(Q) sums stay on the device across frames; nothing is copied
+  back per frame.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Dict, Iterable, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import engine, refsem, writers
+from .frames import Frame
+from .refsem import F32
+
+
+@dataclasses.dataclass
+class Config:
+    """The /INPUT/, /INPUT_SP/, /INPUT_RDF/ and /INPUT_SQ/ keys this path uses (input.f90:64-75)."""
+    nsp: int = 1
+    sp_types_selected: Sequence[int] = (1,)
+    run_rdf: bool = True
+    run_sq: bool = True
+    deltar: float = 0.02
+    rcrdf: float = 0.0             # <= 0: half the smallest box edge
+    qmax: float = 10.0
+    qmin: float = 3.0
+    bsc: Optional[Sequence[float]] = None   # per sp_types_selected entry; default 1.0
+    kset: str = "ref"              # ref | full | full+axes | full+sampled
+    method: str = "split"          # split (tcgen05 split-BF16) | plain (FP32 direct sum)
+    per_shell: int = 200
+    seed: int = 0
+    units: str = "lj"
+
+    def bsc_list(self) -> List[float]:
+        return list(self.bsc) if self.bsc is not None else [1.0] * self.nsp
+
+
+class Session:
+    """Per-trajectory state of the g(r)/S(Q) path on one device."""
+
+    def __init__(self, cfg: Config, device: int = 0, n_max: Optional[int] = None,
+                 ctx: Optional[engine.Context] = None, stream: Optional[torch.cuda.Stream] = None):
+        self.cfg = cfg
+        self.ctx = ctx if ctx is not None else engine.Context(device)
+        self.stream = stream
+        self.n_max = n_max
+        self.nconf = 0
+        self.first = True
+        self.species_lut = None
+        self.ntype = None
+        self.box = None
+        self.volumen = None
+        self.bsc_sp = None
+        self.stage = None
+        self.rdf = None
+        self.sq = None
+        self.hist = None
+        self.edge = None
+        self.sq_out = None
+        self.kset = None
+        self.n = 0
+
+    # ---- layout (select_ncdfinput) ------------------------------------------------
+    def _species_of(self, types: np.ndarray) -> np.ndarray:
+        if self.species_lut is None:
+            sp, wtypes, perm = refsem.species_by_first_appearance(types, self.cfg.sp_types_selected)
+            if len(wtypes) != self.cfg.nsp:
+                raise ValueError(f"selected types {list(self.cfg.sp_types_selected)} not all in the frame "
+                                 f"(found {wtypes})")
+            lut = np.full(int(max(types.max(), max(self.cfg.sp_types_selected))) + 2, -1, np.int32)
+            for s, t in enumerate(wtypes):
+                lut[t] = s
+            self.species_lut = lut
+            b = self.cfg.bsc_list()
+            self.bsc_sp = np.array([b[perm[s]] for s in range(self.cfg.nsp)], np.float32)
+            self.wtypes = wtypes
+        t = np.asarray(types)
+        if t.max() >= self.species_lut.shape[0] or t.min() < 0:
+            raise ValueError("frame holds a type id outside the first frame's range")
+        return self.species_lut[t]
+
+    def select_ncdfinput(self, frame: Frame) -> None:
+        """Species numbering, host->device copy, fold and species-contiguous order."""
+        species = self._species_of(frame.types)
+        keep = species >= 0
+        xyz = frame.xyz if keep.all() else frame.xyz[keep]
+        species = species if keep.all() else species[keep]
+        if self.stage is None:
+            n_max = self.n_max or xyz.shape[0]
+            self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp)
+        self.box = np.asarray(frame.box, np.float32)
+        self.volumen = refsem.volume(self.box)
+        self.ntype = np.bincount(species, minlength=self.cfg.nsp).astype(np.int64)
+        self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream)
+
+    # ---- g(r) -----------------------------------------------------------------------
+    def RDF_init(self) -> None:
+        c = self.cfg
+        self.rdf = engine.RdfPlan(self.ctx, c.nsp, c.deltar, c.rcrdf, self.box, self.stage.n_max)
+        self.hist = self.rdf.new_hist()
+        self.edge = torch.zeros(4, dtype=torch.int64, device=self.ctx.torch_device)
+
+    def RDFcomp(self) -> None:
+        self.rdf.accumulate(self.stage.packed, self.n, self.box, self.hist, self.edge, stream=self.stream)
+
+    # ---- S(Q) -----------------------------------------------------------------------
+    def sq_init(self) -> None:
+        c = self.cfg
+        self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell)
+        self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype)
+        self.sq_out = self.sq.new_out()
+
+    def SQcalc(self) -> None:
+        self.sq.accumulate(self.stage.packed, self.n, self.box, self.sq_out, engine.METHODS[self.cfg.method],
+                           stream=self.stream)
+
+    # ---- frame loop (trj_analysis.f90:173-242) ---------------------------------------
+    def add_frame(self, frame: Frame) -> None:
+        self.select_ncdfinput(frame)
+        if self.first:
+            if self.cfg.run_rdf:
+                self.RDF_init()
+            if self.cfg.run_sq:
+                self.sq_init()
+            self.first = False
+        if self.cfg.run_rdf:
+            self.RDFcomp()
+        if self.cfg.run_sq:
+            self.SQcalc()
+        self.nconf += 1
+
+    def run(self, frames: Iterable[Frame], check_every: int = 0) -> "Session":
+        for k, f in enumerate(frames):
+            self.add_frame(f)
+            if check_every and (k + 1) % check_every == 0:
+                self.ctx.check(self.stream)
+        self.ctx.check(self.stream)
+        return self
+
+    # ---- results ----------------------------------------------------------------------
+    def rdf_transfer(self) -> np.ndarray:
+        """uint64 [nit][lsmax] pair counts summed over frames."""
+        return self.hist.cpu().numpy().astype(np.uint64)
+
+    def edge_stats(self) -> Dict[str, int]:
+        e = self.edge.cpu().numpy()
+        return {"edge_ulp": int(e[0]), "edge_fma": int(e[1]), "counted": int(e[2]), "tested": int(e[3])}
+
+    def sq_transfer_gpu_cpu(self) -> np.ndarray:
+        """FP64 [nbins][nit] sums of w Re(rho_a conj(rho_b))."""
+        return self.sq_out.cpu().numpy()
+
+    def rdf_results(self) -> Dict[str, np.ndarray]:
+        return normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
+                             self.ntype, self.nconf)
+
+    def sq_results(self) -> Dict[str, np.ndarray]:
+        return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf)
+
+    def printrdf(self, outdir: str = ".") -> List[str]:
+        res = self.rdf_results()
+        return writers.write_gmixsim(outdir, res["r"], res["g"], self.cfg.nsp)
+
+    def printSQ(self, outdir: str = ".") -> List[str]:
+        res = self.sq_results()
+        return writers.write_sq(outdir, res["q"], res["s_nn"], res["nq"], res["s_self"], res.get("binary"))
+
+    def suggested_rcl(self) -> float:
+        """First minimum of the total g(r) after its first peak (rdf.cuf:313-352, 755-822)."""
+        return first_minimum(self.rdf_transfer(), self.rdf.lsmax, self.cfg.deltar, self.volumen,
+                             int(self.ntype.sum()))
+
+    def close(self) -> None:
+        for obj in (self.sq, self.rdf):
+            if obj is not None:
+                obj.close()
+
+
+def shell_volumes(lsmax: int, deltar: float) -> np.ndarray:
+    """4 pi/3 ((r+dr/2)^3 - (r-dr/2)^3) for r = i*dr, i = 1..lsmax (log.f90:475-478)."""
+    dr = float(F32(deltar))
+    ri = np.array([float(F32(F32(i) * F32(deltar))) for i in range(1, lsmax + 1)])
+    return 4.0 * math.pi * ((ri + dr / 2) ** 3 - (ri - dr / 2) ** 3) / 3.0, ri
+
+
+def normalise_rdf(hist: np.ndarray, nsp: int, lsmax: int, deltar: float, volumen: float, ntype: np.ndarray,
+                  nconf: int) -> Dict[str, np.ndarray]:
+    """printrdf's g_jl(r_i) = (j/l+1) V H_jl(i) / (dV_i N_l N_j Nconf) for i = 1..lsmax-2 (FP64)."""
+    dv, ri = shell_volumes(lsmax, deltar)
+    nrow = max(lsmax - 2, 0)
+    g = np.zeros((nrow, nsp, nsp))
+    h = hist.astype(np.float64)
+    for j in range(nsp):
+        for l in range(j, nsp):
+            row = refsem.pair_row(j, l, nsp)
+            fac = 2.0 if j == l else 1.0
+            v = fac * volumen * h[row, :nrow] / (dv[:nrow] * float(ntype[l]) * float(ntype[j]) * nconf)
+            g[:, j, l] = v
+            g[:, l, j] = v
+    # total g(r) with the 2V/(dV N^2) normalisation of RDFcomp (rdf.cuf:313-341), per frame
+    n = float(np.sum(ntype))
+    gtot = 2.0 * volumen * h[:, :nrow].sum(axis=0) / (dv[:nrow] * n * n * nconf)
+    return {"r": ri[:nrow].astype(np.float32), "g": g, "gtot": gtot}
+
+
+def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, natms: int) -> float:
+    dv, _ = shell_volumes(lsmax, deltar)
+    g = np.zeros(lsmax + 1)
+    g[1:] = 2.0 * volumen * hist.astype(np.float64).sum(axis=0) / (dv * natms * natms)
+    nrdf = lsmax
+    imax = 1
+    for i in range(2, nrdf):
+        if g[i] > 0.1 and g[i] > g[i - 1] and g[i] > g[i + 1]:
+            imax = i
+            break
+    if imax == 1:
+        imax = int(np.argmax(g[1:nrdf + 1])) + 1
+    imin = imax + 1
+    for i in range(imax + 1, nrdf):
+        if g[i] < g[i - 1] and g[i] < g[i + 1]:
+            imin = i
+            break
+    if 0 < imin < nrdf:
+        x1, x2, x3 = deltar * (imin - 1), deltar * imin, deltar * (imin + 1)
+        y1, y2, y3 = g[imin - 1], g[imin], g[imin + 1]
+        den = y1 - 2.0 * y2 + y3
+        return x2 + 0.5 * (y1 - y3) / den * (x3 - x1) / 2.0 if abs(den) > 1e-12 else x2
+    return deltar * imin
+
+
+def normalise_sq(out: np.ndarray, kset: refsem.KSet, ntype: np.ndarray, bsc: np.ndarray,
+                 nconf: int) -> Dict[str, np.ndarray]:
+    """printSQ (log.f90:317-412) in FP64: S_NN = sqf/(baver^2 N Nconf nq), S_aa = sqfp_a/(N_a Nconf nq),
+    and for two species with bsc = 1 the Bhatia-Thornton S_cc and the partials s11, s22, s12.
+    Also returns every species-pair S_ab = sum Re(rho_a rho_b*)/(sqrt(N_a N_b) Nconf nq)."""
+    nsp = ntype.shape[0]
+    n = float(ntype.sum())
+    b = np.asarray(bsc, np.float64)
+    rows = refsem.pair_rows(nsp)
+    sqf = np.zeros(out.shape[0])
+    for r, (a, c) in enumerate(rows):
+        sqf += (1.0 if a == c else 2.0) * b[a] * b[c] * out[:, r]
+    baver = float((ntype * b).sum() / n)
+    sqf = sqf / baver ** 2
+    nq = kset.nq.astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        den = np.where(nq > 0, nq, np.nan)
+        s_nn = sqf / (n * nconf * den)
+        s_self = np.stack([out[:, refsem.pair_row(a, a, nsp)] / (ntype[a] * nconf * den) for a in range(nsp)],
+                          axis=1)
+        s_pair = np.stack([out[:, r] / (math.sqrt(ntype[a] * ntype[c]) * nconf * den) for r, (a, c) in
+                           enumerate(rows)], axis=1)
+    sl = slice(1, kset.nqmax + 1)
+    res = {"q": kset.q_column(), "s_nn": s_nn[sl], "nq": kset.nq[sl], "s_self": s_self[sl], "s_pair": s_pair[sl],
+           "sqf": sqf[sl]}
+    if nsp == 2 and np.all(np.abs(b - 1.0) <= 1e-4):
+        x1, x2 = ntype[0] / n, ntype[1] / n
+        s11 = x1 * s_self[sl, 0]
+        s22 = x2 * s_self[sl, 1]
+        s12 = 0.5 * (s_nn[sl] - s11 - s22)
+        scc = x2 ** 2 * s11 + x1 ** 2 * s22 - 2 * x1 * x2 * s12
+        res["binary"] = {"scc": scc, "s11": s11, "s22": s22, "s12": s12}
+    return res

@@ -1,0 +1,281 @@
+// ctx.cu -- context, error reporting, and the device frame-layout step.
+//
+// The layout step restates select_ncdfinput (reference src/core/netcdf.f90:582-692):
+// species-contiguous order (stable within a species, netcdf.f90:625-687) and the
+// periodic fold r = r - L*int(r/L) (netcdf.f90:681), both on the device.
+#include <stdarg.h>
+
+#include "trj_common.cuh"
+
+int trj_fail(trj_ctx* ctx, int code, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return code;
+}
+
+extern "C" int trj_abi_version(void) { return TRJ_ABI_VERSION; }
+
+extern "C" int trj_ctx_create(int device, trj_ctx** out) {
+    if (!out) return TRJ_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return TRJ_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return TRJ_ERR_INVALID;
+    trj_ctx* ctx = new trj_ctx();
+    ctx->device = device;
+    trj_device_guard g(device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete ctx;
+        return TRJ_ERR_CUDA;
+    }
+    if (prop.major != 10) {
+        // This build carries sm_100a code only.
+        delete ctx;
+        return TRJ_ERR_UNSUPPORTED;
+    }
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    if (cudaMalloc(&ctx->status_dev, 8 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMallocHost(&ctx->status_host, 8 * sizeof(unsigned)) != cudaSuccess) {
+        if (ctx->status_dev) cudaFree(ctx->status_dev);
+        delete ctx;
+        return TRJ_ERR_NOMEM;
+    }
+    cudaMemset(ctx->status_dev, 0, 8 * sizeof(unsigned));
+    cudaDeviceSynchronize();
+    *out = ctx;
+    return TRJ_OK;
+}
+
+extern "C" int trj_ctx_destroy(trj_ctx* ctx) {
+    if (!ctx) return TRJ_OK;
+    {
+        trj_device_guard g(ctx->device);
+        if (ctx->status_dev) cudaFree(ctx->status_dev);
+        if (ctx->status_host) cudaFreeHost(ctx->status_host);
+        if (ctx->pack_scratch) cudaFree(ctx->pack_scratch);
+    }
+    delete ctx;
+    return TRJ_OK;
+}
+
+extern "C" const char* trj_ctx_last_error(const trj_ctx* ctx) {
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+extern "C" int trj_ctx_sm_count(const trj_ctx* ctx) { return ctx ? ctx->sm_count : 0; }
+
+extern "C" int64_t trj_ctx_launches(const trj_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int trj_ctx_set_timing(trj_ctx* ctx, int enable) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    ctx->timing = enable != 0;
+    return TRJ_OK;
+}
+
+int trj_kernel_timer::elapsed(trj_ctx* ctx, float* ms) {
+    if (!ms) return trj_fail(ctx, TRJ_ERR_INVALID, "kernel_ms: null output");
+    if (!recorded) return trj_fail(ctx, TRJ_ERR_INVALID, "kernel_ms: no timed launch (enable timing first)");
+    trj_device_guard g(ctx->device);
+    TRJ_CUDA_TRY(ctx, cudaEventSynchronize(stop));
+    TRJ_CUDA_TRY(ctx, cudaEventElapsedTime(ms, start, stop));
+    return TRJ_OK;
+}
+
+extern "C" int trj_ctx_check(trj_ctx* ctx, void* stream) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    TRJ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->status_host, ctx->status_dev, 8 * sizeof(unsigned),
+                                      cudaMemcpyDeviceToHost, s));
+    TRJ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    unsigned st = ctx->status_host[0];
+    if (st) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->status_dev, 0, 8 * sizeof(unsigned), s));
+    if (st & TRJ_DEV_TIMEOUT)
+        return trj_fail(ctx, TRJ_ERR_TIMEOUT, "device-side bounded wait timed out (status 0x%x)", st);
+    if (st & TRJ_DEV_BAD_DATA)
+        return trj_fail(ctx, TRJ_ERR_DATA, "non-finite coordinate or species index out of range");
+    if (st & TRJ_DEV_COUNT_MISMATCH)
+        return trj_fail(ctx, TRJ_ERR_DATA, "species counts of the frame differ from the plan's");
+    if (st & TRJ_DEV_CAPACITY)
+        return trj_fail(ctx, TRJ_ERR_CAPACITY, "device-side capacity exceeded (status 0x%x)", st);
+    return TRJ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Frame layout: fold + stable species partition.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kPackThreads = 256;
+constexpr int kPackRounds = 4;
+constexpr int kPackChunk = kPackThreads * kPackRounds;  // atoms per block
+constexpr int kMaxSpecies = 16;
+
+__global__ void pack_count_kernel(const float* __restrict__ xyz, const int32_t* __restrict__ sp,
+                                  int64_t n, int nsp, int32_t* __restrict__ block_counts,
+                                  unsigned* status) {
+    __shared__ int cnt[kMaxSpecies];
+    if (threadIdx.x < kMaxSpecies) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * kPackChunk;
+    bool bad = false;
+    for (int r = 0; r < kPackRounds; ++r) {
+        int64_t i = base + r * kPackThreads + threadIdx.x;
+        if (i < n) {
+            int s = sp[i];
+            float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+            if (s < 0 || s >= nsp || !isfinite(x) || !isfinite(y) || !isfinite(z)) bad = true;
+            if (s >= 0 && s < nsp) atomicAdd(&cnt[s], 1);
+        }
+    }
+    if (bad) trj_raise(status, TRJ_DEV_BAD_DATA);
+    __syncthreads();
+    if (threadIdx.x < nsp) block_counts[(int64_t)blockIdx.x * nsp + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// One block: exclusive scan of per-block counts, species after species.
+__global__ void pack_scan_kernel(int32_t* __restrict__ block_counts, int64_t nblocks, int nsp,
+                                 int64_t* __restrict__ counts_out, int64_t* __restrict__ block_base) {
+    __shared__ int64_t partial[1024];
+    __shared__ int64_t species_base;
+    if (threadIdx.x == 0) species_base = 0;
+    __syncthreads();
+    int64_t per = (nblocks + blockDim.x - 1) / blockDim.x;
+    for (int s = 0; s < nsp; ++s) {
+        int64_t b0 = threadIdx.x * per, b1 = b0 + per < nblocks ? b0 + per : nblocks;
+        int64_t sum = 0;
+        for (int64_t b = b0; b < b1; ++b) sum += block_counts[b * nsp + s];
+        partial[threadIdx.x] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t run = 0;
+            for (unsigned t = 0; t < blockDim.x; ++t) {
+                int64_t v = partial[t];
+                partial[t] = run;
+                run += v;
+            }
+            counts_out[s] = run;
+        }
+        __syncthreads();
+        int64_t run = species_base + partial[threadIdx.x];
+        for (int64_t b = b0; b < b1; ++b) {
+            block_base[b * nsp + s] = run;
+            run += block_counts[b * nsp + s];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) species_base += counts_out[s];
+        __syncthreads();
+    }
+}
+
+// FP32 fold of the reference: r - L*int(r/L), each operation rounded once.
+__device__ __forceinline__ float fold_ref(float r, float L) {
+    float q = __fdiv_rn(r, L);
+    float t = truncf(q);
+    return __fsub_rn(r, __fmul_rn(L, t));
+}
+
+__global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t* __restrict__ sp,
+                                    int64_t n, int nsp, float Lx, float Ly, float Lz,
+                                    const int64_t* __restrict__ block_base,
+                                    float4* __restrict__ packed) {
+    __shared__ int64_t base[kMaxSpecies];
+    __shared__ int warp_cnt[kPackThreads / 32][kMaxSpecies];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (threadIdx.x < nsp) base[threadIdx.x] = block_base[(int64_t)blockIdx.x * nsp + threadIdx.x];
+    for (int k = threadIdx.x; k < (kPackThreads / 32) * kMaxSpecies; k += blockDim.x)
+        (&warp_cnt[0][0])[k] = 0;
+    __syncthreads();
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int64_t start = (int64_t)blockIdx.x * kPackChunk;
+    for (int r = 0; r < kPackRounds; ++r) {
+        int64_t i = start + r * kPackThreads + threadIdx.x;
+        int s = -1;
+        if (i < n) {
+            s = sp[i];
+            if (s < 0 || s >= nsp) s = -1;  // flagged by pack_count_kernel; dropped here
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, s);
+        int rank = __popc(peers & lt_mask);
+        if (s >= 0 && rank == 0) warp_cnt[warp][s] = __popc(peers);
+        __syncthreads();
+        if (s >= 0) {
+            int64_t off = base[s];
+            for (int w = 0; w < warp; ++w) off += warp_cnt[w][s];
+            off += rank;
+            float4 v;
+            v.x = fold_ref(xyz[3 * i], Lx);
+            v.y = fold_ref(xyz[3 * i + 1], Ly);
+            v.z = fold_ref(xyz[3 * i + 2], Lz);
+            v.w = __int_as_float(s);
+            packed[off] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < nsp) {
+            int tot = 0;
+            for (int w = 0; w < kPackThreads / 32; ++w) {
+                tot += warp_cnt[w][threadIdx.x];
+                warp_cnt[w][threadIdx.x] = 0;
+            }
+            base[threadIdx.x] += tot;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
+                              int64_t n, int nsp, const float box[3], float* packed_dev,
+                              int64_t* counts_dev, void* stream) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    if (n < 0 || nsp < 1 || nsp > kMaxSpecies || !box)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: n=%lld nsp=%d (1..%d)", (long long)n,
+                        nsp, kMaxSpecies);
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: box edges must be positive");
+    if (n > 0 && (!xyz_dev || !species_dev || !packed_dev))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: null pointer");
+    if (!counts_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: null counts");
+    if (((uintptr_t)packed_dev) % 16 != 0)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: packed_dev must be 16-byte aligned");
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t nblocks = (n + kPackChunk - 1) / kPackChunk;
+    if (nblocks == 0) {
+        TRJ_CUDA_TRY(ctx, cudaMemsetAsync(counts_dev, 0, sizeof(int64_t) * nsp, s));
+        return TRJ_OK;
+    }
+    if (nblocks > (int64_t)INT32_MAX) return trj_fail(ctx, TRJ_ERR_INVALID, "frame too large");
+    size_t need = (size_t)nblocks * nsp * (sizeof(int32_t) + sizeof(int64_t)) + 256;
+    if (need > ctx->pack_scratch_bytes) {
+        if (ctx->pack_scratch) cudaFree(ctx->pack_scratch);
+        ctx->pack_scratch = nullptr;
+        ctx->pack_scratch_bytes = 0;
+        if (cudaMalloc(&ctx->pack_scratch, need) != cudaSuccess)
+            return trj_fail(ctx, TRJ_ERR_NOMEM, "trj_frame_pack: scratch of %zu bytes", need);
+        ctx->pack_scratch_bytes = need;
+    }
+    int64_t* block_base = (int64_t*)ctx->pack_scratch;
+    int32_t* block_counts = (int32_t*)(block_base + nblocks * nsp);
+    pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp,
+                                                                 block_counts, ctx->status_dev);
+    pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
+    pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(
+        xyz_dev, species_dev, n, nsp, box[0], box[1], box[2], block_base, (float4*)packed_dev);
+    ctx->launches += 3;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}

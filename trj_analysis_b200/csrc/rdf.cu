@@ -1,0 +1,537 @@
+// rdf.cu -- species-resolved pair-distance histogram g_ab(r) on sm_100a.
+//
+// Restates the arithmetic of the reference kernel rdf_sh (src/modules/rdf.cuf:426-487):
+// per unordered pair, FP32 minimum image xd -= L*nint(xd/L) per axis, rr2 = (xd^2+yd^2)+zd^2,
+// counted when rr2 < side2 into bin nint(sqrt_rn(rr2)/deltar) if 1 <= bin <= lsmax, row
+// ind_ij(species_i, species_j).  Every FP32 operation is the explicitly rounded intrinsic
+// (__fsub_rn/__fmul_rn/__fadd_rn/__fsqrt_rn/__fdiv_rn), so no FMA contraction changes it.
+//
+// Unlike the reference's O(N^2) sweep, candidate pairs come from a linked-cell grid:
+// cells of edge >= rcut*(1+2^-10), a half-shell stencil (13 neighbour cells + self) so each
+// pair is tested once.  The per-pair arithmetic is sign-symmetric (IEEE subtraction, NINT
+// half-away-from-zero), so the order (i,j) or (j,i) gives the same rr2 and the same bin;
+// the counts equal the all-pairs sweep exactly.  Axes with fewer than 3 cells are not split
+// (one cell along that axis); a frame with no split axis is the all-pairs case.
+//
+// Neighbour-cell atoms are staged into shared memory with 1-D TMA bulk copies
+// (cp.async.bulk, no multicast), double-buffered on mbarriers; each warp counts into its own
+// uint32 shared histogram replica; replicas are merged with 64-bit global atomics at exit.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "trj_common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;       // threads per CTA = home atoms per task
+constexpr int kJChunk = 1024;       // neighbour atoms per staged buffer (16 KB)
+constexpr int kMaxOffsets = 14;
+
+struct RdfParams {
+    float L[3];
+    float t0[3], t1[3], t2[3];  // |dx| < t0 -> n=0 ; t1 < |dx| < t2 -> n=+-1 ; else exact
+    float side2, side2_lo, side2_hi;
+    float deltar, inv_deltar;
+    int lsmax, nsp, nit;
+    int nc[3];
+    int ncell;
+    int noff;
+    int hsplit;
+    int nrep;
+    int off[kMaxOffsets][3];
+    int64_t nitems;
+};
+
+struct TaskInfo {
+    int sa, na;        // home cell start/count in the sorted array
+    int sb;            // first staged neighbour atom (global index into sorted)
+    int jcount;        // staged atoms
+    int jlocal0;       // index within the neighbour cell of the first staged atom
+    int hc;            // home chunk
+    int self;          // home cell == neighbour cell
+    int valid;         // 0 = no more tasks
+};
+
+__device__ __forceinline__ float min_image_exact(float d, float L) {
+    float n = roundf(__fdiv_rn(d, L));
+    return __fsub_rn(d, __fmul_rn(L, n));
+}
+
+// Minimum image of the reference; fast exact branches for |d| far from L/2 and 3L/2.
+__device__ __forceinline__ float min_image(float d, float L, float t0, float t1, float t2) {
+    float a = fabsf(d);
+    if (a < t0) return d;
+    if (a > t1 && a < t2) return __fsub_rn(d, __fmul_rn(L, copysignf(1.0f, d)));
+    return min_image_exact(d, L);
+}
+
+__device__ __forceinline__ int outcome(float rr2, const RdfParams& p) {
+    if (!(rr2 < p.side2)) return 0;
+    float rr = __fsqrt_rn(rr2);
+    float q = __fdiv_rn(rr, p.deltar);
+    int ind = (int)roundf(q);
+    return (ind <= p.lsmax && ind > 0) ? ind : 0;
+}
+
+// Task iterator run by thread 0: items w = blockIdx.x + k*gridDim.x; item = (cell, offset,
+// home split); tasks = (home chunk, neighbour chunk) of the item.
+struct TaskGen {
+    int64_t w;
+    int hc, jc;
+    int started;
+};
+
+__device__ __forceinline__ int wrapc(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+
+__device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restrict__ cstart,
+                          const int32_t* __restrict__ ccount, TaskInfo& t) {
+    for (;;) {
+        if (!g.started) {
+            g.started = 1;
+            g.w = blockIdx.x;
+            g.hc = -1;
+            g.jc = 0;
+        }
+        if (g.w >= p.nitems) {
+            t.valid = 0;
+            return false;
+        }
+        int64_t w = g.w;
+        int h = (int)(w % p.hsplit);
+        int64_t r = w / p.hsplit;
+        int o = (int)(r % p.noff);
+        int c = (int)(r / p.noff);
+        int cz = c % p.nc[2];
+        int cy = (c / p.nc[2]) % p.nc[1];
+        int cx = c / (p.nc[2] * p.nc[1]);
+        int c2 = (wrapc(cx + p.off[o][0], p.nc[0]) * p.nc[1] + wrapc(cy + p.off[o][1], p.nc[1])) * p.nc[2] +
+                 wrapc(cz + p.off[o][2], p.nc[2]);
+        int na = ccount[c], nb = ccount[c2];
+        int self = (o == 0);
+        if (g.hc < 0) {
+            g.hc = h;
+            g.jc = 0;
+        }
+        // advance within the item
+        while (true) {
+            if (g.hc * kThreads >= na) break;  // item done
+            int jfirst = self ? g.hc * kThreads : 0;
+            int jtot = nb - jfirst;
+            int jstart = jfirst + g.jc * kJChunk;
+            if (jtot <= 0 || jstart >= nb) {
+                g.hc += p.hsplit;
+                g.jc = 0;
+                continue;
+            }
+            t.sa = cstart[c];
+            t.na = na;
+            t.sb = cstart[c2] + jstart;
+            t.jcount = min(kJChunk, nb - jstart);
+            t.jlocal0 = jstart;
+            t.hc = g.hc;
+            t.self = self;
+            t.valid = 1;
+            g.jc += 1;
+            return true;
+        }
+        g.w += gridDim.x;
+        g.hc = -1;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
+                                                             const int32_t* __restrict__ cstart,
+                                                             const int32_t* __restrict__ ccount,
+                                                             unsigned long long* __restrict__ hist_g,
+                                                             unsigned long long* __restrict__ edge_g,
+                                                             unsigned* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* buf = reinterpret_cast<float4*>(smem);                       // [2][kJChunk]
+    unsigned* hist = reinterpret_cast<unsigned*>(smem + 2 * kJChunk * sizeof(float4));
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ TaskInfo tinfo[2];
+    __shared__ int rowtab[16 * 16];
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x, warp = tid / 32;
+    const int hsz = p.nit * p.lsmax;
+    unsigned* myhist = hist + (size_t)(warp % p.nrep) * hsz;
+    for (int k = tid; k < p.nrep * hsz; k += blockDim.x) hist[k] = 0u;
+    for (int k = tid; k < p.nsp * p.nsp; k += blockDim.x) rowtab[k] = trj_pair_row(k / p.nsp, k % p.nsp, p.nsp);
+    TaskGen gen;
+    gen.started = 0;
+    unsigned issued[2] = {0u, 0u};  // copies issued per staging slot (thread 0)
+    if (tid == 0) {
+        abort_flag = 0;
+        trj_mbar_init(&bars[0], 1);
+        trj_mbar_init(&bars[1], 1);
+        trj_fence_mbar_init();
+        if (next_task(gen, p, cstart, ccount, tinfo[0])) {
+            trj_mbar_arrive_expect_tx(&bars[0], tinfo[0].jcount * 16u);
+            trj_bulk_g2s(buf, sorted + tinfo[0].sb, tinfo[0].jcount * 16u, &bars[0]);
+            issued[0] = 1;
+        }
+    }
+    unsigned long long n_ulp = 0, n_fma = 0, n_counted = 0, n_tested = 0;
+    for (int t = 0;; ++t) {
+        __syncthreads();
+        const int slot = t & 1;
+        const TaskInfo ti = tinfo[slot];
+        if (!ti.valid || abort_flag) break;
+        if (tid == 0) {
+            TaskInfo nx;
+            if (next_task(gen, p, cstart, ccount, nx)) {
+                trj_mbar_arrive_expect_tx(&bars[slot ^ 1], nx.jcount * 16u);
+                trj_bulk_g2s(buf + (slot ^ 1) * kJChunk, sorted + nx.sb, nx.jcount * 16u, &bars[slot ^ 1]);
+                issued[slot ^ 1] += 1;
+            }
+            tinfo[slot ^ 1] = nx;
+        }
+        if (!trj_mbar_wait(&bars[slot], (t >> 1) & 1)) {
+            trj_raise(status, TRJ_DEV_TIMEOUT);
+            abort_flag = 1;
+            continue;  // the barrier at the loop head sees the flag
+        }
+        const int il = ti.hc * kThreads + tid;
+        float4 ai = il < ti.na ? sorted[ti.sa + il] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int si = __float_as_int(ai.w);
+        // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
+        const bool has_i = il < ti.na && (unsigned)si < (unsigned)p.nsp;
+        const float4* bj = buf + slot * kJChunk;
+        // For a self task, only j > i (indices within the same cell).
+        int jbeg = 0;
+        if (ti.self) jbeg = max(0, il + 1 - ti.jlocal0);
+        if (!has_i) jbeg = ti.jcount;
+        n_tested += (unsigned long long)max(0, ti.jcount - jbeg);
+        for (int jj = jbeg; jj < ti.jcount; ++jj) {
+            const float4 b = bj[jj];
+            float dx = min_image(__fsub_rn(b.x, ai.x), p.L[0], p.t0[0], p.t1[0], p.t2[0]);
+            float dy = min_image(__fsub_rn(b.y, ai.y), p.L[1], p.t0[1], p.t1[1], p.t2[1]);
+            float dz = min_image(__fsub_rn(b.z, ai.z), p.L[2], p.t0[2], p.t1[2], p.t2[2]);
+            float x2 = __fmul_rn(dx, dx);
+            float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            if (rr2 < p.side2_hi) {
+                float rr = __fsqrt_rn(rr2);
+                float q = __fmul_rn(rr, p.inv_deltar);
+                float fq = q - floorf(q);
+                float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
+                int ind;
+                if (rr2 >= p.side2_lo || fabsf(fq - 0.5f) <= win) {
+                    ind = outcome(rr2, p);
+                    int olo = outcome(nextafterf(rr2, -INFINITY), p);
+                    int ohi = outcome(nextafterf(rr2, INFINITY), p);
+                    n_ulp += (olo != ind || ohi != ind);
+                    float rr2f = fmaf(dz, dz, fmaf(dy, dy, x2));
+                    n_fma += (outcome(rr2f, p) != ind);
+                } else {
+                    ind = __float2int_rn(q);
+                    if (ind > p.lsmax) ind = 0;
+                }
+                const int sj = __float_as_int(b.w);
+                if (ind > 0 && (unsigned)sj < (unsigned)p.nsp) {
+                    int row = rowtab[si * p.nsp + sj];
+                    atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
+                    ++n_counted;
+                }
+            }
+        }
+    }
+    if (tid == 0 && abort_flag) {
+        // Let copies still in flight land before the CTA exits (bounded).
+        for (int sl = 0; sl < 2; ++sl)
+            if (issued[sl]) trj_mbar_wait(&bars[sl], (issued[sl] - 1) & 1);
+    }
+    __syncthreads();
+    // Merge replicas into the global uint64 histogram.
+    for (int k = tid; k < hsz; k += blockDim.x) {
+        unsigned long long s = 0;
+        for (int r = 0; r < p.nrep; ++r) s += hist[(size_t)r * hsz + k];
+        if (s) atomicAdd(&hist_g[k], s);
+    }
+    if (edge_g) {
+        for (int off = 16; off > 0; off >>= 1) {
+            n_ulp += __shfl_down_sync(0xffffffffu, n_ulp, off);
+            n_fma += __shfl_down_sync(0xffffffffu, n_fma, off);
+            n_counted += __shfl_down_sync(0xffffffffu, n_counted, off);
+            n_tested += __shfl_down_sync(0xffffffffu, n_tested, off);
+        }
+        if ((tid & 31) == 0) {
+            if (n_ulp) atomicAdd(&edge_g[TRJ_EDGE_ULP], n_ulp);
+            if (n_fma) atomicAdd(&edge_g[TRJ_EDGE_FMA], n_fma);
+            if (n_counted) atomicAdd(&edge_g[TRJ_EDGE_COUNTED], n_counted);
+            if (n_tested) atomicAdd(&edge_g[TRJ_EDGE_TESTED], n_tested);
+        }
+    }
+}
+
+// Cell of each atom from its wrapped coordinate; per-cell counts and slots.
+__global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n, float Lx, float Ly,
+                                   float Lz, int ncx, int ncy, int ncz, int32_t* __restrict__ ccount,
+                                   int32_t* __restrict__ acell, int32_t* __restrict__ aslot) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = packed[i];
+    float L[3] = {Lx, Ly, Lz};
+    int nc[3] = {ncx, ncy, ncz};
+    float r[3] = {v.x, v.y, v.z};
+    int k[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float w = r[d] - L[d] * floorf(r[d] / L[d]);
+        int c = (int)(w * ((float)nc[d] / L[d]));
+        c = c < 0 ? 0 : (c >= nc[d] ? nc[d] - 1 : c);
+        k[d] = c;
+    }
+    int c = (k[0] * ncy + k[1]) * ncz + k[2];
+    acell[i] = c;
+    aslot[i] = atomicAdd(&ccount[c], 1);
+}
+
+__global__ void cell_scatter_kernel(const float4* __restrict__ packed, int64_t n,
+                                    const int32_t* __restrict__ acell, const int32_t* __restrict__ aslot,
+                                    const int32_t* __restrict__ cstart, float4* __restrict__ sorted) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    sorted[cstart[acell[i]] + aslot[i]] = packed[i];
+}
+
+// Single-block exclusive scan of int32 counts (length up to a few million).
+__global__ void scan_exclusive_kernel(const int32_t* __restrict__ in, int32_t* __restrict__ out, int n) {
+    __shared__ int32_t part[1024];
+    int per = (n + blockDim.x - 1) / blockDim.x;
+    int b0 = threadIdx.x * per, b1 = min(n, b0 + per);
+    int32_t s = 0;
+    for (int k = b0; k < b1; ++k) s += in[k];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+        int32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int32_t run = part[threadIdx.x] - s;
+    for (int k = b0; k < b1; ++k) {
+        out[k] = run;
+        run += in[k];
+    }
+    if (threadIdx.x == blockDim.x - 1) out[n] = part[threadIdx.x];
+}
+
+}  // namespace
+
+struct trj_rdf_plan {
+    trj_ctx* ctx = nullptr;
+    int nsp = 0, nit = 0, lsmax = 0;
+    float deltar = 0.f, rcrdf_eff = 0.f, side2 = 0.f;
+    int64_t n_max = 0;
+    int ncell_cap = 0;
+    int nc[3] = {1, 1, 1};
+    int32_t* ccount = nullptr;  // ncell_cap
+    int32_t* cstart = nullptr;  // ncell_cap + 1
+    int32_t* acell = nullptr;   // n_max
+    int32_t* aslot = nullptr;   // n_max
+    float4* sorted = nullptr;   // n_max
+    int64_t scratch_bytes = 0;
+    trj_kernel_timer timer;
+};
+
+static int nint_host(float x) {  // Fortran NINT: half away from zero
+    double v = (double)x;
+    return (int)(v >= 0 ? floor(v + 0.5) : -floor(-v + 0.5));
+}
+
+// Cells per axis for cutoff^2 side2 in box L; axes with < 3 cells are not split.
+static void cells_for(const float L[3], float side2, int nc[3]) {
+    double rc = sqrt((double)side2) * (1.0 + 1.0 / 1024.0);
+    for (int d = 0; d < 3; ++d) {
+        int k = rc > 0 ? (int)floor((double)L[d] / rc) : 1;
+        if (k < 3) k = 1;
+        if (k > 1024) k = 1024;
+        nc[d] = k;
+    }
+}
+
+extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                                   int64_t n_max, trj_rdf_plan** out) {
+    if (!ctx || !out || !box) return TRJ_ERR_INVALID;
+    *out = nullptr;
+    if (nsp < 1 || nsp > 16) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan: nsp=%d (1..16)", nsp);
+    if (!(deltar > 0.f)) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan: deltar must be > 0");
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan: box edges must be positive");
+    if (n_max < 0 || n_max > (int64_t)INT32_MAX)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan: n_max out of range");
+    trj_rdf_plan* p = new trj_rdf_plan();
+    p->ctx = ctx;
+    p->nsp = nsp;
+    p->nit = nsp * (nsp + 1) / 2;
+    p->deltar = deltar;
+    // select_ncdfinput (netcdf.f90:610-617): side = minval(L); rcrdf = min(rcrdf, side/2)
+    float side = fminf(box[0], fminf(box[1], box[2]));
+    float half = side / 2.0f;
+    float rc = fminf(rcrdf, half);
+    if (!(rc > 0.f)) rc = half;  // rcrdf <= 0 means half the box (netcdf.f90:613-617)
+    p->rcrdf_eff = rc;
+    p->side2 = rc * rc;
+    // RDF_init (rdf.cuf:55-59)
+    p->lsmax = nint_host(rc / deltar) + 1;
+    p->n_max = n_max;
+    size_t hist_bytes = (size_t)p->nit * p->lsmax * 4;
+    size_t budget = ctx->smem_optin - 2 * kJChunk * sizeof(float4) - 4096;
+    if (hist_bytes > budget) {
+        delete p;
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED,
+                        "rdf plan: histogram of %zu bytes exceeds shared memory (%zu); increase deltar "
+                        "or reduce rcrdf", hist_bytes, budget);
+    }
+    cells_for(box, p->side2, p->nc);
+    int ncell = p->nc[0] * p->nc[1] * p->nc[2];
+    // Room for a box up to 25% smaller per axis (more cells) without re-planning.
+    p->ncell_cap = std::max(ncell * 2 + 64, 64);
+    trj_device_guard g(ctx->device);
+    size_t bytes = sizeof(int32_t) * (size_t)(2 * p->ncell_cap + 1) +
+                   (sizeof(int32_t) * 2 + sizeof(float4)) * (size_t)std::max<int64_t>(n_max, 1);
+    char* base = nullptr;
+    if (cudaMalloc(&base, bytes + 256) != cudaSuccess) {
+        delete p;
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "rdf plan: %zu bytes of scratch", bytes);
+    }
+    p->sorted = reinterpret_cast<float4*>(base);
+    p->acell = reinterpret_cast<int32_t*>(p->sorted + std::max<int64_t>(n_max, 1));
+    p->aslot = p->acell + std::max<int64_t>(n_max, 1);
+    p->ccount = p->aslot + std::max<int64_t>(n_max, 1);
+    p->cstart = p->ccount + p->ncell_cap;
+    p->scratch_bytes = (int64_t)bytes;
+    *out = p;
+    return TRJ_OK;
+}
+
+extern "C" int trj_rdf_plan_info(const trj_rdf_plan* p, int* lsmax, int* nit, int cells[3], float* rcrdf_eff,
+                                 float* side2, int64_t* scratch_bytes) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (lsmax) *lsmax = p->lsmax;
+    if (nit) *nit = p->nit;
+    if (cells) for (int d = 0; d < 3; ++d) cells[d] = p->nc[d];
+    if (rcrdf_eff) *rcrdf_eff = p->rcrdf_eff;
+    if (side2) *side2 = p->side2;
+    if (scratch_bytes) *scratch_bytes = p->scratch_bytes;
+    return TRJ_OK;
+}
+
+extern "C" int trj_rdf_kernel_ms(trj_rdf_plan* p, float* ms) {
+    if (!p) return TRJ_ERR_INVALID;
+    return p->timer.elapsed(p->ctx, ms);
+}
+
+extern "C" int trj_rdf_plan_destroy(trj_rdf_plan* p) {
+    if (!p) return TRJ_OK;
+    {
+        trj_device_guard g(p->ctx->device);
+        if (p->sorted) cudaFree(p->sorted);
+        p->timer.release();
+    }
+    delete p;
+    return TRJ_OK;
+}
+
+extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                                  uint64_t* hist_dev, uint64_t* edge_dev, void* stream) {
+    if (!plan) return TRJ_ERR_INVALID;
+    trj_ctx* ctx = plan->ctx;
+    if (!box || !hist_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: null argument");
+    if (n < 0 || n > plan->n_max)
+        return trj_fail(ctx, TRJ_ERR_CAPACITY, "rdf accumulate: n=%lld exceeds plan n_max=%lld", (long long)n,
+                        (long long)plan->n_max);
+    if (n > 0 && (!packed_dev || ((uintptr_t)packed_dev) % 16))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: packed_dev null or not 16-byte aligned");
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: box edges must be positive");
+    if (n < 2) return TRJ_OK;
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    // Per-frame clip, as select_ncdfinput does on every frame (netcdf.f90:610-617).
+    float side = fminf(box[0], fminf(box[1], box[2]));
+    plan->rcrdf_eff = fminf(plan->rcrdf_eff, side / 2.0f);
+    plan->side2 = plan->rcrdf_eff * plan->rcrdf_eff;
+
+    RdfParams P;
+    memset(&P, 0, sizeof(P));
+    for (int d = 0; d < 3; ++d) {
+        P.L[d] = box[d];
+        P.t0[d] = (float)(0.49 * (double)box[d]);
+        P.t1[d] = (float)(0.51 * (double)box[d]);
+        P.t2[d] = (float)(1.49 * (double)box[d]);
+    }
+    P.side2 = plan->side2;
+    P.side2_lo = (float)((double)plan->side2 * (1.0 - 1.0 / 1048576.0));
+    P.side2_hi = (float)((double)plan->side2 * (1.0 + 1.0 / 1048576.0));
+    P.deltar = plan->deltar;
+    P.inv_deltar = 1.0f / plan->deltar;
+    P.lsmax = plan->lsmax;
+    P.nsp = plan->nsp;
+    P.nit = plan->nit;
+    cells_for(box, plan->side2, P.nc);
+    P.ncell = P.nc[0] * P.nc[1] * P.nc[2];
+    if (P.ncell > plan->ncell_cap)
+        return trj_fail(ctx, TRJ_ERR_CAPACITY, "rdf accumulate: %d cells exceed plan capacity %d", P.ncell,
+                        plan->ncell_cap);
+    for (int d = 0; d < 3; ++d) plan->nc[d] = P.nc[d];
+    // Half-shell stencil over the split axes: (0,0,0) first, then offsets > 0 lexicographically.
+    int no = 0;
+    P.off[no][0] = P.off[no][1] = P.off[no][2] = 0;
+    ++no;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                if ((dx && P.nc[0] == 1) || (dy && P.nc[1] == 1) || (dz && P.nc[2] == 1)) continue;
+                bool pos = dx > 0 || (dx == 0 && (dy > 0 || (dy == 0 && dz > 0)));
+                if (!pos) continue;
+                P.off[no][0] = dx;
+                P.off[no][1] = dy;
+                P.off[no][2] = dz;
+                ++no;
+            }
+    P.noff = no;
+    double avg = (double)n / P.ncell;
+    P.hsplit = std::max(1, (int)ceil(avg * 1.25 / kThreads));
+    P.nitems = (int64_t)P.ncell * P.noff * P.hsplit;
+
+    // Shared memory: two staging buffers + histogram replicas.
+    size_t hist_bytes = (size_t)P.nit * P.lsmax * 4;
+    size_t stage = 2 * kJChunk * sizeof(float4);
+    size_t optin = ctx->smem_optin;
+    // Aim for 2 CTAs per SM (16 warps) when the replicas allow it.
+    int ctas_per_sm = 2;
+    size_t per_cta = optin / 2 - 2048;
+    int nrep = (int)std::min<size_t>(8, per_cta > stage ? (per_cta - stage) / hist_bytes : 0);
+    if (nrep < 2) {
+        ctas_per_sm = 1;
+        nrep = (int)std::min<size_t>(8, (optin - 2048 - stage) / hist_bytes);
+    }
+    if (nrep < 1) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf accumulate: histogram too large");
+    P.nrep = nrep;
+    size_t smem = stage + (size_t)nrep * hist_bytes;
+    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(rdf_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+
+    // Cell binning: count, scan, scatter.
+    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->ccount, 0, sizeof(int32_t) * P.ncell, s));
+    unsigned nb = (unsigned)((n + 255) / 256);
+    cell_assign_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, box[0], box[1], box[2], P.nc[0],
+                                          P.nc[1], P.nc[2], plan->ccount, plan->acell, plan->aslot);
+    scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->ccount, plan->cstart, P.ncell);
+    cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->acell, plan->aslot, plan->cstart,
+                                           plan->sorted);
+    int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
+    plan->timer.begin(ctx, s);
+    rdf_pairs_kernel<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount,
+                                                            (unsigned long long*)hist_dev,
+                                                            (unsigned long long*)edge_dev, ctx->status_dev);
+    plan->timer.end(ctx, s);
+    ctx->launches += 4;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}

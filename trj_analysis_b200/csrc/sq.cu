@@ -1,0 +1,472 @@
+// sq.cu -- S_ab(Q) plan, direct-sum kernel, and the FP64 shell reduction.
+//
+// rho_a(k) = sum_{j in species a} exp(i k.r_j) for lattice vectors k = 2*pi*(nx/Lx, ny/Ly, nz/Lz).
+// The phase of every term is reduced exactly: each coordinate becomes the 32-bit fixed-point
+// fraction u = (x/L mod 1) * 2^32 (computed in FP64, once per atom and frame), and
+// n.u mod 2^32 is evaluated in wrapping integer arithmetic, so the angle handed to the FP32
+// sine/cosine is always in [-pi, pi).  The reference (src/modules/sq.cuf:537-581, sqfnD)
+// forms x*kf1 + y*kf2 + z*kf3 in FP32 and calls __cosf/__sinf on arguments up to ~L*q; the
+// exact reduction keeps the per-term error at the FP32 level instead.
+//
+// Output per bin b and species pair (a<=b'): sum_{k in b} w_k Re(rho_a(k) conj(rho_b'(k))),
+// accumulated in FP64 with a fixed reduction order (one CTA per bin), so results do not depend
+// on scheduling.  The reference's sqfp (self partials) and sqf (bsc-weighted total,
+// sq.cuf:583-588) are linear combinations of these rows.
+#include <math.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "sq_plan.cuh"
+
+namespace {
+
+constexpr int kPlainThreads = 256;
+constexpr int kPlainVPT = 4;           // k-vectors per thread
+constexpr int kPlainChunk = 1024;      // atoms staged per pass
+constexpr int kPlainSub = 64;          // FP32 partial-sum length before the FP64 add
+
+// Fixed-point phase coordinates of every atom.
+__global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n, double Lx, double Ly,
+                                    double Lz, uint4* __restrict__ out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = packed[i];
+    double s[3] = {(double)v.x / Lx, (double)v.y / Ly, (double)v.z / Lz};
+    unsigned u[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double f = s[d] - floor(s[d]);             // [0, 1]
+        u[d] = (unsigned)(long long)rint(f * 4294967296.0);  // 2^32 wraps to 0
+    }
+    out[i] = make_uint4(u[0], u[1], u[2], (unsigned)__float_as_int(v.w));
+}
+
+// Direct sum: thread owns kPlainVPT vectors; block y-index selects a slice of every species.
+__global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
+    const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp,
+    const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
+    int nsplit, double2* __restrict__ part) {
+    __shared__ uint4 atoms[kPlainChunk];
+    const int tid = threadIdx.x;
+    const int64_t vbase = (int64_t)blockIdx.x * kPlainThreads * kPlainVPT;
+    unsigned nx[kPlainVPT], ny[kPlainVPT], nz[kPlainVPT];
+    int vidx[kPlainVPT];
+#pragma unroll
+    for (int q = 0; q < kPlainVPT; ++q) {
+        int64_t s = vbase + q * kPlainThreads + tid;
+        vidx[q] = s < nsub ? subset[s] : -1;
+        int4 v = vidx[q] >= 0 ? vecs[vidx[q]] : make_int4(0, 0, 0, 0);
+        nx[q] = (unsigned)v.x;
+        ny[q] = (unsigned)v.y;
+        nz[q] = (unsigned)v.z;
+    }
+    const float kScale = 1.4629180792671596e-09f;  // 2*pi / 2^32
+    for (int a = 0; a < nsp; ++a) {
+        int64_t a0 = sp_off[a], a1 = sp_off[a + 1];
+        int64_t len = a1 - a0;
+        int64_t s0 = a0 + len * blockIdx.y / nsplit, s1 = a0 + len * (blockIdx.y + 1) / nsplit;
+        double accr[kPlainVPT], acci[kPlainVPT];
+#pragma unroll
+        for (int q = 0; q < kPlainVPT; ++q) accr[q] = acci[q] = 0.0;
+        for (int64_t c0 = s0; c0 < s1; c0 += kPlainChunk) {
+            int cnt = (int)((s1 - c0) < (int64_t)kPlainChunk ? (s1 - c0) : (int64_t)kPlainChunk);
+            __syncthreads();
+            for (int k = tid; k < cnt; k += kPlainThreads) atoms[k] = phase[c0 + k];
+            __syncthreads();
+            for (int j0 = 0; j0 < cnt; j0 += kPlainSub) {
+                int j1 = min(cnt, j0 + kPlainSub);
+                float fr[kPlainVPT], fi[kPlainVPT];
+#pragma unroll
+                for (int q = 0; q < kPlainVPT; ++q) fr[q] = fi[q] = 0.f;
+                for (int j = j0; j < j1; ++j) {
+                    uint4 u = atoms[j];
+#pragma unroll
+                    for (int q = 0; q < kPlainVPT; ++q) {
+                        unsigned ph = nx[q] * u.x + ny[q] * u.y + nz[q] * u.z;
+                        float ang = __int2float_rn((int)ph) * kScale;
+                        float sn, cs;
+                        __sincosf(ang, &sn, &cs);
+                        fr[q] += cs;
+                        fi[q] += sn;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kPlainVPT; ++q) {
+                    accr[q] += (double)fr[q];
+                    acci[q] += (double)fi[q];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kPlainVPT; ++q)
+            if (vidx[q] >= 0)
+                part[((int64_t)blockIdx.y * nsp + a) * nvec + vidx[q]] = make_double2(accr[q], acci[q]);
+    }
+}
+
+// rho[a][v] = sum over splits (fixed order) for the subset's vectors.
+__global__ void gather_plain_kernel(const double2* __restrict__ part, const int32_t* __restrict__ subset,
+                                    int nsub, int64_t nvec, int nsp, int nsplit, double2* __restrict__ rho) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)nsub * nsp) return;
+    int a = (int)(t / nsub);
+    int v = subset[t % nsub];
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < nsplit; ++s) {
+        double2 p = part[((int64_t)s * nsp + a) * nvec + v];
+        re += p.x;
+        im += p.y;
+    }
+    rho[(int64_t)a * nvec + v] = make_double2(re, im);
+}
+
+// rho[a][v] for tensor-tile vectors from the FP64 tile blocks.
+__global__ void gather_dense_kernel(const double* __restrict__ tc_out, const int64_t* __restrict__ src,
+                                    int64_t nvec, int nsp, const int64_t* __restrict__ tile_species_stride,
+                                    double2* __restrict__ rho) {
+    int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvec) return;
+    int64_t o = src[v];
+    if (o < 0) return;
+    int64_t stride = tile_species_stride[v];
+    for (int a = 0; a < nsp; ++a) {
+        const double* b = tc_out + o + a * stride;
+        rho[(int64_t)a * nvec + v] = make_double2(b[0], b[kTcRows]);
+    }
+}
+
+// One CTA per bin: out[bin][pair] += sum_v w_v Re(rho_a conj(rho_b)), fixed order.
+__global__ void bin_reduce_kernel(const double2* __restrict__ rho, const double* __restrict__ w,
+                                  const int32_t* __restrict__ bin_start, int64_t nvec, int nsp,
+                                  double* __restrict__ out) {
+    __shared__ double red[32];
+    const int bin = blockIdx.x;
+    const int v0 = bin_start[bin], v1 = bin_start[bin + 1];
+    if (v0 >= v1) return;
+    const int nit = nsp * (nsp + 1) / 2;
+    for (int a = 0; a < nsp; ++a)
+        for (int b = a; b < nsp; ++b) {
+            double s = 0.0;
+            for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+                double2 ra = rho[(int64_t)a * nvec + v], rb = rho[(int64_t)b * nvec + v];
+                s += w[v] * (ra.x * rb.x + ra.y * rb.y);
+            }
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+                out[(int64_t)bin * nit + trj_pair_row(a, b, nsp)] += t;
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void unpermute_rho_kernel(const double2* __restrict__ rho, const int4* __restrict__ vecs,
+                                     int64_t nvec, int nsp, double2* __restrict__ out) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nvec * nsp) return;
+    int64_t a = t / nvec, v = t % nvec;
+    out[a * nvec + vecs[v].w] = rho[t];
+}
+
+__global__ void check_counts_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp,
+                                    int64_t n, unsigned* status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int s = (int)phase[i].w;
+    if (s < 0 || s >= nsp || i < sp_off[s] || i >= sp_off[s + 1]) trj_raise(status, TRJ_DEV_COUNT_MISMATCH);
+}
+
+int plain_nsplit(const trj_ctx* ctx, int64_t nsub, int64_t n_total) {
+    int64_t blocks_v = (nsub + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT);
+    if (blocks_v <= 0) return 1;
+    int64_t target = (int64_t)ctx->sm_count * 8;
+    int64_t ns = (target + blocks_v - 1) / blocks_v;
+    int64_t by_atoms = std::max<int64_t>(1, n_total / (4 * kPlainChunk));
+    ns = std::min<int64_t>(ns, by_atoms);
+    ns = std::max<int64_t>(1, std::min<int64_t>(ns, 128));
+    return (int)ns;
+}
+
+}  // namespace
+
+static void sq_plan_free(trj_sq_plan* p) {
+    trj_device_guard g(p->ctx->device);
+    void* ptrs[] = {p->vec_dev, p->weight_dev, p->bin_start_dev, p->species_off_dev, p->plain_all_dev,
+                    p->plain_sparse_dev, p->tiles_dev, p->dense_src_dev, p->phase_dev, p->part_dev,
+                    p->tc_out_dev, p->rho_dev};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    trj_sq_tc_release(p);
+    p->timer.release();
+}
+
+extern "C" int trj_sq_plan_destroy(trj_sq_plan* p) {
+    if (!p) return TRJ_OK;
+    sq_plan_free(p);
+    delete p;
+    return TRJ_OK;
+}
+
+template <class T>
+static int dev_upload(trj_ctx* ctx, T** dst, const T* src, size_t count, int64_t* acct) {
+    size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: %zu bytes", bytes);
+    *acct += (int64_t)bytes;
+    if (count && src && cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return trj_fail(ctx, TRJ_ERR_CUDA, "sq plan: upload failed");
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int32_t* vec_host,
+                                  const int32_t* bin_host, const double* weight_host, const uint8_t* dense_host,
+                                  int nbins, const int64_t* species_counts, trj_sq_plan** out) {
+    if (!ctx || !out) return TRJ_ERR_INVALID;
+    *out = nullptr;
+    if (nsp < 1 || nsp > 16) return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: nsp=%d (1..16)", nsp);
+    if (nvec < 0 || nvec > (int64_t)INT32_MAX / 2 || nbins < 1)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: nvec=%lld nbins=%d", (long long)nvec, nbins);
+    if (nvec > 0 && (!vec_host || !bin_host || !weight_host))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: null vector arrays");
+    if (!species_counts) return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: null species counts");
+    for (int64_t v = 0; v < nvec; ++v)
+        if (bin_host[v] < 0 || bin_host[v] >= nbins)
+            return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: vector %lld has bin %d outside 0..%d", (long long)v,
+                            bin_host[v], nbins - 1);
+    trj_sq_plan* p = new trj_sq_plan();
+    p->ctx = ctx;
+    p->nsp = nsp;
+    p->nit = nsp * (nsp + 1) / 2;
+    p->nbins = nbins;
+    p->nvec = nvec;
+    p->species_counts.assign(species_counts, species_counts + nsp);
+    p->species_off.assign(nsp + 1, 0);
+    for (int a = 0; a < nsp; ++a) {
+        if (species_counts[a] < 0) {
+            delete p;
+            return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: negative species count");
+        }
+        p->species_off[a + 1] = p->species_off[a] + species_counts[a];
+    }
+    p->n_total = p->species_off[nsp];
+    // Plan order: stable sort by bin.
+    std::vector<int64_t> order(nvec);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return bin_host[x] < bin_host[y]; });
+    std::vector<int4> vecs(nvec);
+    std::vector<double> w(nvec);
+    std::vector<int32_t> bstart(nbins + 1, 0);
+    std::vector<int32_t> all(nvec), sparse;
+    std::vector<int64_t> dense_idx;
+    for (int64_t k = 0; k < nvec; ++k) {
+        int64_t c = order[k];
+        vecs[k] = make_int4(vec_host[3 * c], vec_host[3 * c + 1], vec_host[3 * c + 2], (int)c);
+        w[k] = weight_host[c];
+        bstart[bin_host[c] + 1] += 1;
+        all[k] = (int32_t)k;
+        if (dense_host && dense_host[c]) dense_idx.push_back(k);
+        else sparse.push_back((int32_t)k);
+    }
+    for (int b = 0; b < nbins; ++b) bstart[b + 1] += bstart[b];
+
+    // Tensor tiles over the dense vectors: group by (nx/16, ny/8) blocks, nz span per block,
+    // split into column groups of <= 256 (128 nz values).
+    std::vector<int64_t> dense_src(nvec, -1), dense_stride(nvec, 0);
+    if (!dense_idx.empty()) {
+        struct Key { int bx, by; };
+        std::vector<std::pair<std::pair<int, int>, int64_t>> keyed;
+        keyed.reserve(dense_idx.size());
+        auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+        for (int64_t k : dense_idx)
+            keyed.push_back({{fdiv(vecs[k].x, kTcTileNx), fdiv(vecs[k].y, kTcTileNy)}, k});
+        std::sort(keyed.begin(), keyed.end(), [&](const auto& A, const auto& B) {
+            if (A.first != B.first) return A.first < B.first;
+            return vecs[A.second].z < vecs[B.second].z;
+        });
+        int64_t off = 0;
+        size_t i = 0;
+        while (i < keyed.size()) {
+            size_t j = i;
+            while (j < keyed.size() && keyed[j].first == keyed[i].first) ++j;
+            // nz values of this block, sorted ascending in keyed[i..j)
+            size_t a = i;
+            while (a < j) {
+                int z0 = vecs[keyed[a].second].z;
+                size_t b = a;
+                while (b < j && vecs[keyed[b].second].z - z0 < kTcMaxCols / 2) ++b;
+                int zspan = vecs[keyed[b - 1].second].z - z0 + 1;
+                int ncols = ((2 * zspan + 15) / 16) * 16;
+                SqTile t;
+                t.nx0 = keyed[a].first.first * kTcTileNx;
+                t.ny0 = keyed[a].first.second * kTcTileNy;
+                t.nz0 = z0;
+                t.ncols = ncols;
+                t.out_off = off;
+                for (size_t q = a; q < b; ++q) {
+                    int64_t k = keyed[q].second;
+                    int row = (vecs[k].x - t.nx0) + kTcTileNx * (vecs[k].y - t.ny0);
+                    int col = 2 * (vecs[k].z - t.nz0);
+                    dense_src[k] = off + (int64_t)col * kTcRows + row;
+                    dense_stride[k] = (int64_t)ncols * kTcRows;
+                }
+                p->tile_slots += (int64_t)kTcRows * (ncols / 2);
+                off += (int64_t)nsp * ncols * kTcRows;
+                p->tiles.push_back(t);
+                a = b;
+            }
+            i = j;
+        }
+        p->tc_out_doubles = off;
+        p->n_dense = (int64_t)dense_idx.size();
+    }
+    p->n_sparse = (int64_t)sparse.size();
+
+    trj_device_guard g(ctx->device);
+    int64_t acct = 0;
+    int rc = TRJ_OK;
+    std::vector<int64_t> sp_off = p->species_off;
+    if ((rc = dev_upload(ctx, &p->vec_dev, vecs.data(), vecs.size(), &acct)) ||
+        (rc = dev_upload(ctx, &p->weight_dev, w.data(), w.size(), &acct)) ||
+        (rc = dev_upload(ctx, &p->bin_start_dev, bstart.data(), bstart.size(), &acct)) ||
+        (rc = dev_upload(ctx, &p->species_off_dev, sp_off.data(), sp_off.size(), &acct)) ||
+        (rc = dev_upload(ctx, &p->plain_all_dev, all.data(), all.size(), &acct)) ||
+        (rc = dev_upload(ctx, &p->plain_sparse_dev, sparse.data(), sparse.size(), &acct))) {
+        sq_plan_free(p);
+        delete p;
+        return rc;
+    }
+    if (!p->tiles.empty()) {
+        // dense_src and per-vector species stride packed side by side
+        std::vector<int64_t> both(2 * nvec);
+        for (int64_t k = 0; k < nvec; ++k) {
+            both[k] = dense_src[k];
+            both[nvec + k] = dense_stride[k];
+        }
+        if ((rc = dev_upload(ctx, &p->dense_src_dev, both.data(), both.size(), &acct)) ||
+            (rc = dev_upload(ctx, &p->tiles_dev, p->tiles.data(), p->tiles.size(), &acct))) {
+            sq_plan_free(p);
+            delete p;
+            return rc;
+        }
+        size_t tb = sizeof(double) * (size_t)p->tc_out_doubles;
+        if (cudaMalloc(&p->tc_out_dev, tb) != cudaSuccess) {
+            sq_plan_free(p);
+            delete p;
+            return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: tensor output %zu bytes", tb);
+        }
+        acct += (int64_t)tb;
+    }
+    p->nsplit_all = plain_nsplit(ctx, nvec, p->n_total);
+    p->nsplit_sparse = plain_nsplit(ctx, p->n_sparse, p->n_total);
+    size_t phase_b = sizeof(uint4) * (size_t)std::max<int64_t>(1, p->n_total);
+    size_t part_b = sizeof(double2) * (size_t)std::max(p->nsplit_all, p->nsplit_sparse) * nsp *
+                    (size_t)std::max<int64_t>(1, nvec);
+    size_t rho_b = sizeof(double2) * (size_t)nsp * (size_t)std::max<int64_t>(1, nvec);
+    if (cudaMalloc(&p->phase_dev, phase_b) != cudaSuccess || cudaMalloc(&p->part_dev, part_b) != cudaSuccess ||
+        cudaMalloc(&p->rho_dev, rho_b) != cudaSuccess) {
+        sq_plan_free(p);
+        delete p;
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: scratch allocation failed");
+    }
+    acct += (int64_t)(phase_b + part_b + rho_b);
+    p->scratch_bytes = acct;
+    if (!p->tiles.empty()) {
+        rc = trj_sq_tc_prepare(p);
+        if (rc != TRJ_OK && rc != TRJ_ERR_UNSUPPORTED) {
+            sq_plan_free(p);
+            delete p;
+            return rc;
+        }
+    }
+    *out = p;
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_plan_info(const trj_sq_plan* p, int64_t* n_dense, int64_t* n_tiles, int64_t* tile_slots,
+                                int64_t* scratch_bytes) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (n_dense) *n_dense = p->n_dense;
+    if (n_tiles) *n_tiles = (int64_t)p->tiles.size();
+    if (tile_slots) *tile_slots = p->tile_slots;
+    if (scratch_bytes) *scratch_bytes = p->scratch_bytes;
+    return TRJ_OK;
+}
+
+static int run_plain(trj_sq_plan* p, const int32_t* subset, int64_t nsub, int nsplit, cudaStream_t s,
+                     bool timed) {
+    if (nsub <= 0) return TRJ_OK;
+    dim3 grid((unsigned)((nsub + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT)), (unsigned)nsplit);
+    if (timed) p->timer.begin(p->ctx, s);
+    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->vec_dev, subset,
+                                                   (int)nsub, p->nvec, nsplit, p->part_dev);
+    if (timed) p->timer.end(p->ctx, s);
+    int64_t tot = nsub * p->nsp;
+    gather_plain_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(p->part_dev, subset, (int)nsub, p->nvec,
+                                                                      p->nsp, nsplit, p->rho_dev);
+    p->ctx->launches += 2;
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_accumulate(trj_sq_plan* p, const float* packed_dev, int64_t n, const float box[3], int method,
+                                 double* out_dev, void* stream) {
+    if (!p) return TRJ_ERR_INVALID;
+    trj_ctx* ctx = p->ctx;
+    if (!box || !out_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: null argument");
+    if (n != p->n_total)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: n=%lld but the plan's species counts sum to %lld",
+                        (long long)n, (long long)p->n_total);
+    if (n > 0 && (!packed_dev || ((uintptr_t)packed_dev) % 16))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: packed_dev null or not 16-byte aligned");
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: box edges must be positive");
+    if (method != TRJ_SQ_PLAIN_FP32 && method != TRJ_SQ_SPLIT_BF16X3)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: unknown method %d", method);
+    if (p->nvec == 0) return TRJ_OK;
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (n > 0) {
+        phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
+                                                                       (double)box[1], (double)box[2], p->phase_dev);
+        check_counts_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp,
+                                                                        n, ctx->status_dev);
+        ctx->launches += 2;
+    }
+    if (method == TRJ_SQ_PLAIN_FP32 || p->tiles.empty()) {
+        run_plain(p, p->plain_all_dev, p->nvec, p->nsplit_all, s, true);
+    } else {
+        int rc = trj_sq_tc_run(p, box, s);
+        if (rc != TRJ_OK) return rc;
+        gather_dense_kernel<<<(unsigned)((p->nvec + 255) / 256), 256, 0, s>>>(
+            p->tc_out_dev, p->dense_src_dev, p->nvec, p->nsp, p->dense_src_dev + p->nvec, p->rho_dev);
+        ctx->launches += 1;
+        run_plain(p, p->plain_sparse_dev, p->n_sparse, p->nsplit_sparse, s, false);
+    }
+    bin_reduce_kernel<<<p->nbins, 256, 0, s>>>(p->rho_dev, p->weight_dev, p->bin_start_dev, p->nvec, p->nsp,
+                                              out_dev);
+    ctx->launches += 1;
+    p->last_method = method;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_kernel_ms(trj_sq_plan* p, float* ms) {
+    if (!p) return TRJ_ERR_INVALID;
+    return p->timer.elapsed(p->ctx, ms);
+}
+
+extern "C" int trj_sq_rho(trj_sq_plan* p, double* rho_out, void* stream) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (!rho_out) return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq rho: null output");
+    if (p->last_method < 0) return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq rho: no accumulate call yet");
+    if (p->nvec == 0) return TRJ_OK;
+    trj_device_guard g(p->ctx->device);
+    int64_t tot = p->nvec * p->nsp;
+    unpermute_rho_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        p->rho_dev, p->vec_dev, p->nvec, p->nsp, (double2*)rho_out);
+    TRJ_CUDA_TRY(p->ctx, cudaGetLastError());
+    return TRJ_OK;
+}

@@ -1,0 +1,210 @@
+"""Device layer: contexts, plans and frame buffers over the C ABI.
+
+PyTorch supplies device memory and streams only; every kernel that touches the
+data is in libtrj_sm100.so.  Pointers are passed as integers from
+``tensor.data_ptr()`` and streams as ``torch.cuda.Stream.cuda_stream``.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import box3, check
+from .refsem import KSet
+
+vp = ctypes.c_void_p
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return vp(t.data_ptr()) if t is not None else vp(0)
+
+
+def _stream(stream: Optional[torch.cuda.Stream]):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return vp(s.cuda_stream)
+
+
+class Context:
+    """One device's library context (status word, pack scratch)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("trj_analysis_b200 needs a CUDA device (sm_100); no CPU path exists")
+        self.device = int(device)
+        self.torch_device = torch.device("cuda", self.device)
+        h = vp()
+        rc = self.lib.trj_ctx_create(self.device, ctypes.byref(h))
+        if rc != _lib.TRJ_OK:
+            raise _lib.TrjError(rc, f"trj_ctx_create(device={device}) failed (an sm_100 device is required)")
+        self.h = h
+        self.sm_count = self.lib.trj_ctx_sm_count(h)
+
+    def check(self, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Synchronises ``stream`` and raises on device-side status (bad data, timeouts)."""
+        check(self.lib.trj_ctx_check(self.h, _stream(stream)), self.h, "device status")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.trj_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pack_frame(ctx: Context, xyz: torch.Tensor, species: torch.Tensor, nsp: int, box,
+               packed: torch.Tensor, counts: torch.Tensor, stream=None) -> None:
+    """Device layout step (fold + stable species-contiguous order)."""
+    n = int(xyz.shape[0])
+    assert xyz.dtype == torch.float32 and xyz.is_contiguous() and xyz.is_cuda
+    assert species.dtype == torch.int32 and species.is_contiguous()
+    assert packed.dtype == torch.float32 and packed.shape[0] >= n and packed.shape[1] == 4
+    assert counts.dtype == torch.int64 and counts.numel() >= nsp
+    rc = ctx.lib.trj_frame_pack(ctx.h, _ptr(xyz), _ptr(species), n, nsp, box3(box), _ptr(packed),
+                                _ptr(counts), _stream(stream))
+    check(rc, ctx.h, "trj_frame_pack")
+
+
+class RdfPlan:
+    def __init__(self, ctx: Context, nsp: int, deltar: float, rcrdf: float, box, n_max: int):
+        self.ctx = ctx
+        h = vp()
+        rc = ctx.lib.trj_rdf_plan_create(ctx.h, nsp, float(deltar), float(rcrdf), box3(box), int(n_max),
+                                         ctypes.byref(h))
+        check(rc, ctx.h, "trj_rdf_plan_create")
+        self.h = h
+        self.nsp = nsp
+        self.refresh_info()
+
+    def refresh_info(self) -> None:
+        lsmax, nit = ctypes.c_int(), ctypes.c_int()
+        cells = (ctypes.c_int * 3)()
+        rc_eff, side2 = ctypes.c_float(), ctypes.c_float()
+        sb = ctypes.c_int64()
+        check(self.ctx.lib.trj_rdf_plan_info(self.h, ctypes.byref(lsmax), ctypes.byref(nit), cells,
+                                             ctypes.byref(rc_eff), ctypes.byref(side2), ctypes.byref(sb)),
+              self.ctx.h, "trj_rdf_plan_info")
+        self.lsmax, self.nit = lsmax.value, nit.value
+        self.cells = tuple(cells)
+        self.rcrdf, self.side2 = rc_eff.value, side2.value
+        self.scratch_bytes = sb.value
+
+    def new_hist(self) -> torch.Tensor:
+        return torch.zeros((self.nit, self.lsmax), dtype=torch.int64, device=self.ctx.torch_device)
+
+    def accumulate(self, packed: torch.Tensor, n: int, box, hist: torch.Tensor,
+                   edge: Optional[torch.Tensor] = None, stream=None) -> None:
+        assert hist.dtype == torch.int64 and hist.shape == (self.nit, self.lsmax)
+        rc = self.ctx.lib.trj_rdf_accumulate(self.h, _ptr(packed), int(n), box3(box), _ptr(hist), _ptr(edge),
+                                             _stream(stream))
+        check(rc, self.ctx.h, "trj_rdf_accumulate")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.trj_rdf_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SqPlan:
+    def __init__(self, ctx: Context, nsp: int, kset: KSet, species_counts):
+        self.ctx = ctx
+        self.nsp = nsp
+        self.kset = kset
+        counts = np.ascontiguousarray(np.asarray(species_counts, dtype=np.int64))
+        assert counts.shape == (nsp,)
+        self._vec = np.ascontiguousarray(kset.vectors.astype(np.int32))
+        self._bin = np.ascontiguousarray(kset.bins.astype(np.int32))
+        self._w = np.ascontiguousarray(kset.weights.astype(np.float64))
+        self._dense = np.ascontiguousarray(kset.dense.astype(np.uint8))
+        h = vp()
+        rc = ctx.lib.trj_sq_plan_create(
+            ctx.h, nsp, int(kset.nvec), self._vec.ctypes.data_as(vp), self._bin.ctypes.data_as(vp),
+            self._w.ctypes.data_as(vp), self._dense.ctypes.data_as(vp), int(kset.nbins),
+            counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(h))
+        check(rc, ctx.h, "trj_sq_plan_create")
+        self.h = h
+        self.nit = nsp * (nsp + 1) // 2
+        self.n_total = int(counts.sum())
+        nd, nt, ts, sb = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(ctx.lib.trj_sq_plan_info(h, ctypes.byref(nd), ctypes.byref(nt), ctypes.byref(ts), ctypes.byref(sb)),
+              ctx.h, "trj_sq_plan_info")
+        self.n_dense, self.n_tiles, self.tile_slots, self.scratch_bytes = nd.value, nt.value, ts.value, sb.value
+
+    def new_out(self) -> torch.Tensor:
+        return torch.zeros((self.kset.nbins, self.nit), dtype=torch.float64, device=self.ctx.torch_device)
+
+    def accumulate(self, packed: torch.Tensor, n: int, box, out: torch.Tensor, method: int, stream=None) -> None:
+        assert out.dtype == torch.float64 and out.shape == (self.kset.nbins, self.nit)
+        rc = self.ctx.lib.trj_sq_accumulate(self.h, _ptr(packed), int(n), box3(box), int(method), _ptr(out),
+                                            _stream(stream))
+        check(rc, self.ctx.h, "trj_sq_accumulate")
+
+    def rho(self, stream=None) -> torch.Tensor:
+        """rho_a(k) of the last accumulate, (nsp, nvec) complex128, caller vector order."""
+        t = torch.empty((self.nsp, self.kset.nvec, 2), dtype=torch.float64, device=self.ctx.torch_device)
+        check(self.ctx.lib.trj_sq_rho(self.h, _ptr(t), _stream(stream)), self.ctx.h, "trj_sq_rho")
+        return torch.view_as_complex(t)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.trj_sq_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+METHODS = {"plain": _lib.TRJ_SQ_PLAIN_FP32, "split": _lib.TRJ_SQ_SPLIT_BF16X3,
+           "plain_fp32": _lib.TRJ_SQ_PLAIN_FP32, "split_bf16x3": _lib.TRJ_SQ_SPLIT_BF16X3}
+
+
+class FrameStage:
+    """Pinned host staging + device buffers for frames of up to ``n_max`` atoms."""
+
+    def __init__(self, ctx: Context, n_max: int, nsp: int):
+        dev = ctx.torch_device
+        self.ctx = ctx
+        self.n_max = n_max
+        self.nsp = nsp
+        self.h_xyz = torch.empty((n_max, 3), dtype=torch.float32, pin_memory=True)
+        self.h_sp = torch.empty((n_max,), dtype=torch.int32, pin_memory=True)
+        self.d_xyz = torch.empty((n_max, 3), dtype=torch.float32, device=dev)
+        self.d_sp = torch.empty((n_max,), dtype=torch.int32, device=dev)
+        self.packed = torch.empty((n_max, 4), dtype=torch.float32, device=dev)
+        self.counts = torch.zeros((max(nsp, 1),), dtype=torch.int64, device=dev)
+        self._copied = None  # event after the last host->device copy out of the pinned buffers
+
+    def upload_and_pack(self, xyz: np.ndarray, species: np.ndarray, box, stream=None) -> int:
+        n = int(xyz.shape[0])
+        if n > self.n_max:
+            raise _lib.TrjError(_lib.TRJ_ERR_CAPACITY, f"frame of {n} atoms exceeds stage size {self.n_max}")
+        if self._copied is not None:
+            self._copied.synchronize()  # pinned buffers may still feed the previous copy
+        self.h_xyz[:n].numpy()[:] = xyz
+        self.h_sp[:n].numpy()[:] = species
+        s = stream if stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self.d_xyz[:n].copy_(self.h_xyz[:n], non_blocking=True)
+            self.d_sp[:n].copy_(self.h_sp[:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+            self._copied = ev
+        pack_frame(self.ctx, self.d_xyz[:n], self.d_sp[:n], self.nsp, box, self.packed, self.counts, stream=s)
+        return n

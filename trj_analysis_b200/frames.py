@@ -1,0 +1,192 @@
+"""Frame sources: seeded synthetic FCC frames and file-backed trajectories.
+
+A frame is the raw input of one configuration, before the layout step:
+``xyz`` (N, 3) float32 positions as a trajectory stores them (not folded),
+``types`` (N,) int32 LAMMPS-style type ids (1-based), and ``box`` (3,) float32
+orthorhombic edge lengths.  This is what ``read_nc_cfg`` hands to
+``select_ncdfinput`` in the reference (src/core/netcdf.f90:173-550).
+
+The synthetic generator places 4 atoms per cubic FCC cell of edge
+``a = (4/density)**(1/3)``, displaces each atom by i.i.d. Gaussian noise of
+standard deviation ``sigma * a`` per axis, optionally re-places a fraction of
+atoms uniformly in the box, and assigns types by a seeded shuffle with given
+ratios.  Species identity is fixed per trajectory (seed), displacements differ
+per frame (seed, frame).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Iterator, Sequence
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Frame:
+    xyz: np.ndarray      # (N, 3) float32
+    types: np.ndarray    # (N,) int32, 1-based type ids
+    box: np.ndarray      # (3,) float32
+
+    @property
+    def n(self) -> int:
+        return int(self.xyz.shape[0])
+
+
+@dataclasses.dataclass
+class FCCSpec:
+    """Seeded synthetic trajectory of FCC-derived frames."""
+    cells: tuple = (10, 10, 10)          # FCC cells per axis
+    density: float = 0.8                 # number density
+    sigma: float = 0.12                  # Gaussian displacement, units of the cubic cell edge a
+    fractions: tuple = (1.0,)            # species ratios (normalised), types 1..nsp
+    replace_frac: float = 0.0            # fraction of atoms re-placed uniformly at random
+    remove: int = 0                      # atoms removed by a seeded draw (to hit a target N)
+    seed: int = 1234
+
+    @property
+    def a(self) -> float:
+        return (4.0 / self.density) ** (1.0 / 3.0)
+
+    @property
+    def box(self) -> np.ndarray:
+        return (np.asarray(self.cells, dtype=np.float64) * self.a).astype(np.float32)
+
+    @property
+    def n(self) -> int:
+        c = self.cells
+        return 4 * c[0] * c[1] * c[2] - self.remove
+
+    def _lattice(self) -> np.ndarray:
+        c = self.cells
+        basis = np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0],
+                          [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]])
+        ix, iy, iz = np.meshgrid(np.arange(c[0]), np.arange(c[1]), np.arange(c[2]),
+                                 indexing="ij")
+        origins = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], axis=1).astype(np.float64)
+        pos = (origins[:, None, :] + basis[None, :, :]).reshape(-1, 3) * self.a
+        return pos
+
+    def _identity(self):
+        """Kept-atom index and type per atom; identical for every frame."""
+        rng = np.random.default_rng([self.seed, 0x5eed])
+        ntot = 4 * self.cells[0] * self.cells[1] * self.cells[2]
+        keep = np.arange(ntot)
+        if self.remove:
+            drop = rng.choice(ntot, size=self.remove, replace=False)
+            keep = np.setdiff1d(keep, drop)
+        n = keep.size
+        fr = np.asarray(self.fractions, dtype=np.float64)
+        fr = fr / fr.sum()
+        counts = np.floor(fr * n + 0.5).astype(np.int64)
+        counts[-1] = n - counts[:-1].sum()
+        types = np.repeat(np.arange(1, len(fr) + 1, dtype=np.int32), counts)
+        rng.shuffle(types)
+        return keep, types
+
+    def frame(self, index: int) -> Frame:
+        keep, types = self._identity()
+        pos = self._lattice()[keep]
+        rng = np.random.default_rng([self.seed, 1 + index])
+        pos = pos + rng.normal(0.0, self.sigma * self.a, size=pos.shape)
+        box = self.box.astype(np.float64)
+        if self.replace_frac > 0:
+            m = int(round(self.replace_frac * pos.shape[0]))
+            idx = rng.choice(pos.shape[0], size=m, replace=False)
+            pos[idx] = rng.uniform(0.0, 1.0, size=(m, 3)) * box
+        return Frame(xyz=pos.astype(np.float32), types=types.copy(),
+                     box=self.box.copy())
+
+    def frames(self, count: int, start: int = 0) -> Iterator[Frame]:
+        for i in range(start, start + count):
+            yield self.frame(i)
+
+
+# Named workloads (shapes of the benchmark configurations).
+def c1_spec(seed: int = 1) -> FCCSpec:
+    """N=4000 single species, cubic L=17.0998, sigma=0.12 a."""
+    return FCCSpec(cells=(10, 10, 10), density=0.8, sigma=0.12, fractions=(1.0,), seed=seed)
+
+
+def c2_spec(seed: int = 2) -> FCCSpec:
+    """N=62,500 binary 80:20, L=42.75, sigma=0.1 a."""
+    return FCCSpec(cells=(25, 25, 25), density=0.8, sigma=0.1, fractions=(0.8, 0.2), seed=seed)
+
+
+def c3_spec(seed: int = 3) -> FCCSpec:
+    """N=1,000,188 three species 50:30:20, L=107.73, sigma=0.1 a, 2% re-placed."""
+    return FCCSpec(cells=(63, 63, 63), density=0.8, sigma=0.1, fractions=(0.5, 0.3, 0.2),
+                   replace_frac=0.02, seed=seed)
+
+
+def c4_spec(seed: int = 4) -> FCCSpec:
+    """N=4,000,000 slab 1:1:4 (63x63x252 cells, 752 removed), 50:50."""
+    return FCCSpec(cells=(63, 63, 252), density=0.8, sigma=0.1, fractions=(0.5, 0.5),
+                   remove=752, seed=seed)
+
+
+WORKLOADS = {"c1": c1_spec, "c2": c2_spec, "c3": c3_spec, "c4": c4_spec}
+
+
+class NpzTrajectory:
+    """Frames stored as ``coordinates`` (F, N, 3), ``cell_lengths`` (F, 3), ``type`` (F, N) or (N,)."""
+
+    def __init__(self, path: str):
+        self._z = np.load(path)
+
+    def __len__(self) -> int:
+        return int(self._z["coordinates"].shape[0])
+
+    def __iter__(self) -> Iterator[Frame]:
+        coords = self._z["coordinates"]
+        cells = self._z["cell_lengths"]
+        types = self._z["type"] if "type" in self._z else None
+        for f in range(coords.shape[0]):
+            t = np.ones(coords.shape[1], np.int32) if types is None else (
+                types[f] if types.ndim == 2 else types)
+            yield Frame(xyz=np.asarray(coords[f], np.float32), types=np.asarray(t, np.int32),
+                        box=np.asarray(cells[f], np.float32))
+
+
+class NetCDFTrajectory:
+    """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type``).
+
+    Uses netCDF4 when importable, else scipy's reader for classic CDF-1/2 files.
+    """
+
+    def __init__(self, path: str):
+        self._ds = None
+        try:  # pragma: no cover - netCDF4 is not installed in this image
+            from netCDF4 import Dataset  # type: ignore
+            self._ds = Dataset(path)
+            self._v = self._ds.variables
+        except ImportError:
+            from scipy.io import netcdf_file
+            self._ds = netcdf_file(path, "r", mmap=False)
+            self._v = self._ds.variables
+
+    def __len__(self) -> int:
+        return int(self._v["coordinates"].shape[0])
+
+    def __iter__(self) -> Iterator[Frame]:
+        coords = self._v["coordinates"]
+        cells = self._v["cell_lengths"]
+        has_type = "type" in self._v
+        for f in range(coords.shape[0]):
+            xyz = np.asarray(coords[f], dtype=np.float32)
+            t = (np.asarray(self._v["type"][f], np.int32) if has_type
+                 else np.ones(xyz.shape[0], np.int32))
+            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32))
+
+
+def open_trajectory(path: str):
+    ext = os.path.splitext(path)[1].lower()
+    if ext == ".npz":
+        return NpzTrajectory(path)
+    return NetCDFTrajectory(path)
+
+
+def write_npz_trajectory(path: str, frames: Sequence[Frame]) -> None:
+    np.savez(path, coordinates=np.stack([f.xyz for f in frames]),
+             cell_lengths=np.stack([f.box for f in frames]),
+             type=np.stack([f.types for f in frames]))

@@ -1,0 +1,126 @@
+"""Output files in the reference's formats.
+
+printrdf  -> gmixsim.dat (src/core/log.f90:414-596): header
+             '#       r        ',9x,16('g_',2i1,'(r)',9x:), rows '(16f16.5)'
+             (nsp > 6: one file gmixsim<k>.dat per species k, full rows g_k1..g_knsp).
+printSQ   -> sq.dat  (log.f90:317-412): '(2f15.7,i12)' or, for 2 species with all
+             bsc = 1, '(6f15.7,i12)' with S_NN, S_cc, S_11, S_22, S_12, n(Q);
+             sqmix.dat '(15f16.7)' with S_aa per species.
+freud-style tools -> gr.dat / Sq.dat as numpy.savetxt writes them ('%.18e', header
+             '# r g(r)' / '# k S(k)'); species-resolved columns are appended.
+
+Fortran fixed-point edit descriptors are emulated: values are rounded half away
+from zero from their exact binary value; a record holds at most the repeat count
+of items and continues on the next line (format reversion); a value wider than the
+field prints as asterisks; an i1 field of a value >= 10 prints '*'.
+"""
+from __future__ import annotations
+
+import decimal
+from typing import Iterable, List, Sequence
+
+import numpy as np
+
+
+def fmt_f(value: float, width: int, decimals: int) -> str:
+    d = decimal.Decimal(float(value)).quantize(decimal.Decimal(1).scaleb(-decimals),
+                                               rounding=decimal.ROUND_HALF_UP)
+    s = f"{d:.{decimals}f}"
+    if s.startswith("-") and d == 0:
+        s = s  # keep the sign, as formatted Fortran output does for tiny negatives
+    if len(s) > width:
+        return "*" * width
+    return s.rjust(width)
+
+
+def fmt_i(value: int, width: int) -> str:
+    s = str(int(value))
+    return "*" * width if len(s) > width else s.rjust(width)
+
+
+def _records(values: Sequence[float], per_line: int, width: int, decimals: int) -> List[str]:
+    lines = []
+    for k in range(0, len(values), per_line):
+        lines.append("".join(fmt_f(v, width, decimals) for v in values[k:k + per_line]))
+    return lines or [""]
+
+
+def _i1(v: int) -> str:
+    return str(v) if 0 <= v <= 9 else "*"
+
+
+def _group_header(prefix: str, labels: Sequence[str], per_line: int, sep: str) -> List[str]:
+    """Header with a repeated group ('label', sep) and reversion after per_line groups."""
+    lines = []
+    for k in range(0, len(labels), per_line):
+        chunk = labels[k:k + per_line]
+        body = sep.join(chunk)
+        lines.append((prefix if k == 0 else "") + body)
+    return lines or [prefix.rstrip()]
+
+
+def write_gmixsim(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int) -> List[str]:
+    """g: (nrows, nsp, nsp) symmetric partial g_ab(r).  Returns the files written."""
+    import os
+    files = []
+    if nsp <= 6:
+        labels = [f"g_{_i1(j + 1)}{_i1(k + 1)}(r)" for j in range(nsp) for k in range(j, nsp)]
+        head = _group_header("#       r        " + " " * 9, labels, 16, " " * 9)
+        rows = []
+        for i in range(r.shape[0]):
+            vals = [r[i]] + [g[i, j, k] for j in range(nsp) for k in range(j, nsp)]
+            rows.extend(_records(vals, 16, 16, 5))
+        p = os.path.join(path_dir, "gmixsim.dat")
+        with open(p, "w") as f:
+            f.write("\n".join(head + rows) + "\n")
+        files.append(p)
+    else:
+        for k in range(nsp):
+            labels = [f"g_{_i1(k + 1)}{_i1(j + 1)}(r)" for j in range(nsp)]
+            head = _group_header("#       r        " + " " * 9, labels, 16, " " * 9)
+            rows = []
+            for i in range(r.shape[0]):
+                rows.extend(_records([r[i]] + [g[i, k, j] for j in range(nsp)], 16, 16, 5))
+            p = os.path.join(path_dir, f"gmixsim{k + 1}.dat")
+            with open(p, "w") as f:
+                f.write("\n".join(head + rows) + "\n")
+            files.append(p)
+    return files
+
+
+SQ_HEADER_BINARY = ("#           Q        S_NN(Q)          S_cc(Q)       S_11(Q)        S_22(Q)"
+                    "           S_12(Q)         n(Q)")
+SQ_HEADER = "#           Q       S_NN(Q)          n(Q)"
+
+
+def sqmix_header(nsp: int) -> List[str]:
+    labels = [f"S_{_i1(j + 1)}{_i1(j + 1)}(Q)" for j in range(nsp)]
+    return _group_header("#       Q" + " " * 14, labels, 15, " " * 9)
+
+
+def write_sq(path_dir: str, q: np.ndarray, s_nn: np.ndarray, nq: np.ndarray, s_self: np.ndarray,
+             binary: dict = None) -> List[str]:
+    """q, s_nn, nq: rows 1..nqmax; s_self: (nrows, nsp); binary: scc, s11, s22, s12 arrays."""
+    import os
+    lines = [SQ_HEADER_BINARY if binary is not None else SQ_HEADER]
+    for i in range(q.shape[0]):
+        if binary is not None:
+            vals = [q[i], s_nn[i], binary["scc"][i], binary["s11"][i], binary["s22"][i], binary["s12"][i]]
+            lines.append("".join(fmt_f(v, 15, 7) for v in vals) + fmt_i(nq[i], 12))
+        else:
+            lines.append(fmt_f(q[i], 15, 7) + fmt_f(s_nn[i], 15, 7) + fmt_i(nq[i], 12))
+    p1 = os.path.join(path_dir, "sq.dat")
+    with open(p1, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    nsp = s_self.shape[1]
+    mix = sqmix_header(nsp)
+    for i in range(q.shape[0]):
+        mix.extend(_records([q[i]] + list(s_self[i]), 15, 16, 7))
+    p2 = os.path.join(path_dir, "sqmix.dat")
+    with open(p2, "w") as f:
+        f.write("\n".join(mix) + "\n")
+    return [p1, p2]
+
+
+def savetxt_columns(path: str, columns: Iterable[np.ndarray], header: str) -> None:
+    np.savetxt(path, np.column_stack(list(columns)), header=header)
