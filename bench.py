@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""S(Q)+g(r) frames/s on the N=1,000,188 three-species frame (one step = one frame).
+
+Workload (default ``c3``): FCC 63^3 cells at density 0.8 (L=107.73), species 50:30:20,
+Gaussian displacements 0.1 a plus 2% re-placed atoms, seeded synthetic frames.
+g_ab(r): deltar=0.01, rcrdf=8 (cell lists).  S_ab(Q): qmax=10, qmin=3, bsc=(1,0.8,0.5);
+k-set ``full+axes`` (every lattice vector of every complete shell below qmin, as +-k pairs,
+plus the axis vectors of the shells above), method ``split`` (tcgen05 split-BF16) and, for
+comparison, ``plain`` (FP32 direct sum).
+
+Contract: ``python bench.py --gpus N --steps K --warmup W``; under torchrun each rank runs an
+independent replica on its own frames (weak scaling, no data-path collective); rank 0 prints
+one JSON line.  ``--impl reference`` times the CPU restatement of the reference algorithm on
+the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "S(Q)+g(r) frames/s at N=1M vs plain FP32 kernel (1e-5 rel err); p50/p99 ms"
+
+WORKLOADS = {
+    "c3": dict(spec="c3", deltar=0.01, rcrdf=8.0, qmax=10.0, qmin=3.0, bsc=(1.0, 0.8, 0.5), kset="full+axes"),
+    "c2": dict(spec="c2", deltar=0.01, rcrdf=10.0, qmax=15.0, qmin=5.0, bsc=(1.0, 0.6), kset="full+sampled"),
+    "c1": dict(spec="c1", deltar=0.02, rcrdf=1e9, qmax=20.0, qmin=None, bsc=(1.0,), kset="full"),
+    "c4": dict(spec="c4", deltar=0.02, rcrdf=6.0, qmax=8.0, qmin=2.0, bsc=(1.0, 1.0), kset="full+axes"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--method", default="split", choices=["split", "plain"])
+    ap.add_argument("--kset", default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison pass")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def make_frames(wl, count, start):
+    from trj_analysis_b200 import frames
+    spec = frames.WORKLOADS[wl["spec"]]()
+    return spec, [spec.frame(start + i) for i in range(count)]
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from trj_analysis_b200 import _lib, analysis, engine, refsem
+    from trj_analysis_b200.analysis import Config, Session
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    wl = dict(WORKLOADS[args.workload])
+    if args.kset:
+        wl["kset"] = args.kset
+    nsp = len(wl["bsc"])
+    W, K = args.warmup, args.steps
+    spec, fr = make_frames(wl, W + K, start=1000 * rank)
+    n = fr[0].n
+    box = fr[0].box
+    ctx = engine.Context(local_rank)
+    stream = torch.cuda.current_stream()
+
+    # device-resident inputs: raw coordinates and species of every step's frame
+    d_xyz = [torch.from_numpy(f.xyz).to(dev) for f in fr]
+    d_sp = [torch.from_numpy((f.types - 1).astype(np.int32)).to(dev) for f in fr]
+    packed = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    counts = torch.zeros(nsp, dtype=torch.int64, device=dev)
+    rdf = engine.RdfPlan(ctx, nsp, wl["deltar"], wl["rcrdf"], box, n)
+    hist = rdf.new_hist()
+    edge = torch.zeros(4, dtype=torch.int64, device=dev)
+    ks = refsem.make_kset(wl["kset"], box, wl["qmax"], wl["qmin"], seed=0)
+    sp_counts = np.bincount(fr[0].types - 1, minlength=nsp)
+    sq = engine.SqPlan(ctx, nsp, ks, sp_counts)
+    out = sq.new_out()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    method = args.method
+    if method == "split" and sq.n_tiles == 0:
+        method = "plain"
+
+    def step(i, m):
+        engine.pack_frame(ctx, d_xyz[i], d_sp[i], nsp, box, packed, counts)
+        rdf.accumulate(packed, n, box, hist, edge)
+        sq.accumulate(packed, n, box, out, engine.METHODS[m])
+
+    def timed(m, steps, warm):
+        for i in range(warm):
+            step(i % len(fr), m)
+            flush.zero_()
+        ctx.check()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = ctx.lib.trj_ctx_launches(ctx.h)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.lib.trj_ctx_set_timing(ctx.h, 1)
+        kms = {"rdf": [], "sq": []}
+        per = []
+        ev0.record(stream)
+        for i in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step((warm + i) % len(fr), m)
+            b.record(stream)
+            flush.zero_()
+            per.append((a, b))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        launches = ctx.lib.trj_ctx_launches(ctx.h) - launches0
+        ctx.lib.trj_ctx_set_timing(ctx.h, 0)
+        step_ms = [a.elapsed_time(b) for a, b in per]
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        ctx.check()
+        return ms, step_ms, launches
+
+    # kernel durations: one instrumented pass per kernel (events on the launch stream)
+    def kernel_ms(m, reps):
+        ctx.lib.trj_ctx_set_timing(ctx.h, 1)
+        r_ms, s_ms = [], []
+        import ctypes
+        for i in range(reps):
+            step(i % len(fr), m)
+            v = ctypes.c_float()
+            _lib.check(ctx.lib.trj_rdf_kernel_ms(rdf.h, ctypes.byref(v)), ctx.h)
+            r_ms.append(v.value)
+            _lib.check(ctx.lib.trj_sq_kernel_ms(sq.h, ctypes.byref(v)), ctx.h)
+            s_ms.append(v.value)
+            flush.zero_()
+        ctx.lib.trj_ctx_set_timing(ctx.h, 0)
+        return statistics.mean(r_ms), statistics.mean(s_ms)
+
+    with ClockSampler(local_rank) as clk:
+        total_ms, step_ms, launches = timed(method, K, W)
+    clocks = clk.summary()
+    value = world * K / (total_ms / 1000.0)
+    rdf_ms, sq_ms = kernel_ms(method, max(3, min(K, 5)))
+
+    plain = None
+    if not args.no_plain and method == "split":
+        pk = max(3, K // 3)
+        p_ms, p_step, _ = timed("plain", pk, 1)
+        _, plain_sq_ms = kernel_ms("plain", 2)
+        plain = {"value": world * pk / (p_ms / 1000.0), "unit": "frames/s", "steps": pk,
+                 "sq_kernel_ms": plain_sq_ms, "ms_per_step": p_ms / pk}
+
+    # e2e through the public API: host frames -> Session (pinned copy, H2D, pack, g(r), S(Q)),
+    # then a device->host read of the accumulated results every step.
+    e2e = None
+    if not args.no_e2e:
+        cfg = Config(nsp=nsp, sp_types_selected=list(range(1, nsp + 1)), deltar=wl["deltar"], rcrdf=wl["rcrdf"],
+                     qmax=wl["qmax"], qmin=wl["qmin"], bsc=wl["bsc"], kset=wl["kset"], method=method)
+        sess = Session(cfg, ctx=ctx, n_max=n)
+        for i in range(W):
+            sess.add_frame(fr[i])
+            sess.hist.cpu(), sess.sq_out.cpu()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        lat = []
+        t0 = time.perf_counter()
+        for i in range(K):
+            ts = time.perf_counter()
+            sess.add_frame(fr[W + i])
+            h = sess.hist.cpu()
+            s = sess.sq_out.cpu()
+            lat.append((time.perf_counter() - ts) * 1000.0)
+        torch.cuda.synchronize()
+        e_ms = (time.perf_counter() - t0) * 1000.0
+        if world > 1:
+            t = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        sess.ctx.check()
+        e2e = {"value": world * K / (e_ms / 1000.0), "unit": "frames/s",
+               "h2d_bytes_per_step": int(n * 12 + n * 4), "d2h_bytes_per_step": int(h.numel() * 8 + s.numel() * 8),
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+        sess.rdf.close()
+        sess.sq.close()
+
+    peaks = {}
+    pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    # roofline of the dominant kernel
+    n_dense = sq.n_dense
+    if method == "split" and sq_ms >= rdf_ms:
+        flops = 8.0 * n * n_dense
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        achieved = flops / (sq_ms / 1000.0) / 1e12
+        roof = {"kernel": "sq_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured sustained" if peaks else "fallback",
+                "algorithmic": f"8*N*n_kvec = 8*{n}*{n_dense} flops per launch"}
+    elif sq_ms >= rdf_ms:
+        bytes_ = 16.0 * n * sq.kset.nvec / 1024.0
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = (n * sq.kset.nvec) / (sq_ms / 1000.0) / 1e12
+        roof = {"kernel": "sq_plain (FP32 direct sum)", "bound": "hbm", "achieved": 16.0 * n / (sq_ms / 1e3) / 1e9,
+                "peak": peak, "unit": "GB/s", "frac": 16.0 * n / (sq_ms / 1e3) / 1e9 / peak, "traffic": None,
+                "terms_per_s": achieved * 1e12}
+    else:
+        nit = nsp * (nsp + 1) // 2
+        alg = 16.0 * n + 8.0 * nit * rdf.lsmax
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = alg / (rdf_ms / 1000.0) / 1e9
+        roof = {"kernel": "rdf_pairs (cell list)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "algorithmic": f"16*N + 8*nit*lsmax = {alg:.0f} bytes per launch"}
+    roof["kernels_ms"] = {"rdf_pairs": rdf_ms, "sq_main": sq_ms}
+    edge_h = edge.cpu().numpy()
+    pairs_per_frame = float(edge_h[2]) / max(1, (W + K + 3 * (max(3, min(K, 5)) > 0)))
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+bf16x3" if method == "split" else "f32", "data": "synthetic (seeded FCC frames)",
+        "config": {"workload": f"{args.workload}: N={n} nsp={nsp} L={float(box[0]):.3f}, g(r) deltar={wl['deltar']} "
+                               f"rcrdf={wl['rcrdf']}, S(Q) qmax={wl['qmax']} qmin={wl['qmin']} kset={wl['kset']}",
+                   "method": method, "n_kvec": int(sq.kset.nvec), "n_kvec_tensor": int(n_dense),
+                   "rdf_cells": list(rdf.cells), "parallelism": f"replicas x{world}",
+                   "l2": "256 MB buffer written between steps (inside the timed region)",
+                   "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
+        "clocks": clocks, "gpu_launches": int(launches), "roofline": roof, "e2e": e2e,
+    }
+    if plain is not None:
+        result["plain_fp32"] = plain
+        result["speedup_split_vs_plain"] = value / plain["value"]
+    return result, (spec, fr, wl, ks)
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement (reference algorithm on host cores)
+# ---------------------------------------------------------------------------
+
+def cpu_frame_estimate(wl, fr0, ks, seconds):
+    """Times a bounded sample of one frame on the host cores; returns (s per frame, sample text, cores)."""
+    from oracle import orc
+    from trj_analysis_b200 import refsem
+    nsp = len(wl["bsc"])
+    pos, sp, off = orc.layout(fr0.xyz, fr0.types - 1, fr0.box, nsp)
+    p = refsem.rdf_params(nsp, wl["deltar"], wl["rcrdf"], fr0.box)
+    n = pos.shape[0]
+    budget = seconds / 2.0
+    # g(r): home atoms from the middle of the frame, doubling until the budget is used
+    m = 2000
+    while True:
+        i0 = n // 2 - m // 2
+        t = time.perf_counter()
+        orc.rdf_counts_range(pos, sp, fr0.box, p.side2, p.deltar, p.lsmax, nsp, i0, i0 + m)
+        dt = time.perf_counter() - t
+        if dt > budget / 4 or m >= n:
+            break
+        m = min(n, m * 4)
+    t_rdf = dt * n / m
+    # S(Q): the reference's FP32-phase direct sum over a subset of the k-vectors
+    nv = 16
+    while True:
+        idx = np.linspace(0, ks.nvec - 1, nv).astype(np.int64)
+        t = time.perf_counter()
+        orc.rho_ref32(pos, off, fr0.box, ks.vectors[idx])
+        dt2 = time.perf_counter() - t
+        if dt2 > budget / 4 or nv >= ks.nvec:
+            break
+        nv = min(ks.nvec, nv * 4)
+    t_sq = dt2 * ks.nvec / nv
+    cores = orc.lib().orc_num_threads()
+    sample = (f"g(r): {m} home atoms of {n} (cell list, j>i), S(Q): {nv} of {ks.nvec} k-vectors x {n} atoms; "
+              f"extrapolated to one frame")
+    return t_rdf + t_sq, sample, cores
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from trj_analysis_b200 import refsem
+    wl = dict(WORKLOADS[args.workload])
+    if args.kset:
+        wl["kset"] = args.kset
+    spec, fr = make_frames(wl, 1, 0)
+    ks = refsem.make_kset(wl["kset"], fr[0].box, wl["qmax"], wl["qmin"], seed=0)
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(min(args.warmup, 1)):
+        cpu_frame_estimate(wl, fr[0], ks, per_step / 2)
+    times = []
+    for _ in range(args.steps):
+        t, sample, cores = cpu_frame_estimate(wl, fr[0], ks, per_step)
+        times.append(t)
+    v = 1.0 / statistics.mean(times)
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded FCC frames)",
+            "config": {"workload": f"{args.workload}: N={fr[0].n}, kset={wl['kset']}",
+                       "implementation": "CPU restatement of the reference algorithm (oracle/, C + OpenMP): "
+                                         "linked-cell g(r) with the rdf_sh FP32 binning, FP32-phase direct-sum S(Q)"},
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local_rank))
+    res, (spec, fr, wl, ks) = run_ours(args, rank, world, local_rank)
+    if rank == 0 and not args.no_cpu:
+        t, sample, cores = cpu_frame_estimate(wl, fr[0], ks, args.cpu_seconds)
+        res["cpu_baseline"] = {"value": 1.0 / t, "unit": "frames/s", "cores": cores, "kind": "port",
+                               "sample": sample}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
