@@ -6,20 +6,23 @@
 //   rho(nx, ny, nz) = sum_j A[(nx,ny), j] * Z_j[nz],   A = X*Y,
 // a complex GEMM with the atoms as the contraction dimension.  It runs as a real GEMM:
 //   K index 2j = Re, 2j+1 = Im of atom j;  B columns 2t (Re out) = (zr, -zi), 2t+1 (Im out) = (zi, zr).
-// Each phase value v is split v = hi + lo with hi = bf16(v), lo = bf16(v - hi); the product
-// keeps hi*hi + hi*lo + lo*hi (three tcgen05.mma kind::f16 per K-step into one FP32 TMEM
-// accumulator).  Every F stages the accumulator is drained and added into an FP64 per-CTA
-// block, and the blocks of one species are summed in FP64 in a fixed order.
+// Each factor v is split v = hi + lo with hi = bf16(v), lo = bf16(v - hi); the product keeps
+// hi*hi + hi*lo + lo*hi (three tcgen05.mma kind::f16 per K-step into one FP32 TMEM accumulator).
+// Every F stages (F*32 atoms) the accumulator is drained and added into an FP64 block, and the
+// blocks of one species are summed in FP64 in a fixed order.
 //
-// Phases: every coordinate is the 32-bit fixed-point fraction u = (x/L mod 1) 2^32 (from
-// FP64); n*u mod 2^32 in integer arithmetic is exact, and sincospif of the reduced fraction
-// gives each factor at FP32 accuracy.
+// Phases: every coordinate is the 32-bit fixed-point fraction u = (x/L mod 1) 2^32 (from FP64);
+// n*u mod 2^32 in integer arithmetic is exact, and sincospif of the reduced fraction gives each
+// factor at FP32 accuracy.  A per-frame kernel writes the FP32 X and Y factor tables and the
+// split BF16 Z operand; the contraction kernel reads all three with 2-D TMA loads (no multicast).
 //
-// Roles per CTA (320 threads): warps 0-7 generate the A tile (X*Y products, split) in the
-// 128-byte-swizzled K-major layout and later drain TMEM; warp 8 streams the B tile (Z phases,
-// pre-split in a per-frame table) with 2-D TMA loads (no multicast); warp 9 allocates TMEM
-// and one of its lanes issues the MMAs.  Stages are handed over with mbarriers; every wait
-// is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
+// Work item = (group of up to two tiles that share their nz range, chunk of one species' atoms);
+// the B tile is loaded once per stage for both tiles.  Persistent CTAs walk the items chunk-major
+// so that concurrently running CTAs stream the same atoms (L2 reuse of the tables).
+// Roles per CTA (448 threads): warps 0-7 build the A tiles (X*Y products, split, 128-byte swizzle);
+// warps 8-11 drain the TMEM accumulators (double-buffered) into FP64; warp 12 issues the TMA loads;
+// warp 13 allocates TMEM and one of its lanes issues the MMAs.  Every mbarrier wait is bounded and
+// raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -32,15 +35,26 @@ namespace {
 
 constexpr int kProducerWarps = 8;
 constexpr int kProducers = kProducerWarps * 32;
-constexpr int kTcThreads = kProducers + 64;
+constexpr int kEpiWarps = 4;
+constexpr int kTmaWarp = kProducerWarps + kEpiWarps;  // 12
+constexpr int kMmaWarp = kTmaWarp + 1;                // 13
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;       // 448
 constexpr int kStageSlots = 32;            // atoms per stage: K = 64 bf16 = one 128-byte swizzle row
 constexpr int kATile = 128 * 128;          // bytes of one 128 x 64 bf16 operand tile
-constexpr int kTabEntries = kTcTileNx + kTcTileNy;  // 24 phase factors per atom per stage
+constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // 32 atoms x 16 complex FP32
+constexpr int kYBytes = kStageSlots * kTcTileNy * 8;  // 32 atoms x 8 complex FP32
 constexpr int kMaxStages = 4;
 
 struct TcTile {
-    int nx0, ny0, ncols, brow;  // brow: first table row (2*(nz0 - nz_min))
+    int nx0, ny0, ncols, brow;  // brow: first Z-table row (2*(nz0 - nz_min))
+    int xcol, ycol;             // first float of the tile's 16 X / 8 Y factors in a table row
     int64_t acc_off;            // doubles: offset of this tile's [ncols][128] block in a chunk's slice
+};
+
+struct TcGroup {
+    int t0, t1;    // tile indices; t1 = -1 for a single tile
+    int bcols;     // B rows loaded per stage (max ncols of the group)
+    int brow;
 };
 
 struct TcChunk {
@@ -50,41 +64,43 @@ struct TcChunk {
 
 struct TcParams {
     const TcTile* tiles;
+    const TcGroup* groups;
     const TcChunk* chunks;
-    const uint2* slot_uv;   // (ux, uy) per padded atom slot
     double* part;           // [chunk][acc_stride]
     int64_t acc_stride;
+    int ngroups, nchunks;
     int nstages;
     int flush_stages;
     int stage_bytes;
+    int tpc;                // tiles per CTA slot layout (1 or 2)
     unsigned* status;
 };
 
 struct TcState {
-    int nz_min = 0, table_rows = 0;
+    int nz_min = 0, table_rows = 0, nx_min = 0, nxr = 0, ny_min = 0, nyr = 0;
     int64_t total_slots = 0;
     std::vector<int64_t> pad_off;  // nsp+1 padded slot offsets
     std::vector<TcChunk> chunks;
+    std::vector<TcGroup> groups;
     std::vector<int> chunk_of_species_begin;  // nsp+1
     TcTile* tiles_dev = nullptr;
+    TcGroup* groups_dev = nullptr;
     TcChunk* chunks_dev = nullptr;
     int64_t* pad_off_dev = nullptr;
     int32_t* chunk_begin_dev = nullptr;
     __nv_bfloat16* tab_hi = nullptr;
     __nv_bfloat16* tab_lo = nullptr;
-    uint2* slot_uv = nullptr;
+    float2* tab_x = nullptr;
+    float2* tab_y = nullptr;
     double* part = nullptr;
     int64_t acc_stride = 0;
-    CUtensorMap map_hi, map_lo;
-    int nstages = 2, stage_bytes = 0, smem_bytes = 0, max_cols = 0;
-    int flush_stages = 32;
+    CUtensorMap map_hi, map_lo, map_x, map_y;
+    int nstages = 2, stage_bytes = 0, smem_bytes = 0, max_cols = 0, tpc = 2;
+    int flush_stages = 16;
+    int grid = 0;
 };
 
 // ---- PTX wrappers ----------------------------------------------------------
-
-__device__ __forceinline__ void named_bar(int id, int n) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
 
 // Barrier `id` over n threads that also returns whether any participant passed pred = true,
 // so a group leaves a loop together (a plain named barrier has no timeout).
@@ -148,11 +164,13 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                   "=r"(r[7])
-                 : "r"(taddr));
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
@@ -174,31 +192,44 @@ __device__ __forceinline__ float2 phase_factor(unsigned ph) {
     return make_float2(c, s);
 }
 
-// ---- per-frame table: Z phases split into the B operand rows, slot (ux, uy) ----
+__device__ __forceinline__ bool timed_wait(uint64_t* bar, unsigned parity, unsigned* status) {
+    if (trj_mbar_wait(bar, parity)) return true;
+    trj_raise(status, TRJ_DEV_TIMEOUT);
+    return false;
+}
 
-__global__ void tc_table_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
-                                const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nz_min,
-                                int nz_count, int table_rows, int64_t kdim, __nv_bfloat16* __restrict__ tab_hi,
-                                __nv_bfloat16* __restrict__ tab_lo, uint2* __restrict__ slot_uv) {
-    int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= total_slots) return;
+// ---- per-frame tables --------------------------------------------------------
+// slot -> atom of the species-padded layout; padding slots carry zero factors.
+__device__ __forceinline__ bool slot_atom(int64_t slot, const int64_t* pad_off, const int64_t* sp_off, int nsp,
+                                          int64_t& atom) {
     int a = 0;
     while (a + 1 < nsp && slot >= pad_off[a + 1]) ++a;
     int64_t local = slot - pad_off[a];
-    bool real = local < sp_off[a + 1] - sp_off[a];
-    uint4 u = real ? phase[sp_off[a] + local] : make_uint4(0u, 0u, 0u, 0u);
-    if (blockIdx.y == 0) slot_uv[slot] = make_uint2(u.x, u.y);
+    atom = sp_off[a] + local;
+    return local < sp_off[a + 1] - sp_off[a];
+}
+
+// Z factors split into the B operand rows (row 2t: (zr, -zi), row 2t+1: (zi, zr) along K).
+__global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
+                                 const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nz_min,
+                                 int nz_count, int64_t kdim, __nv_bfloat16* __restrict__ tab_hi,
+                                 __nv_bfloat16* __restrict__ tab_lo) {
+    int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= total_slots) return;
+    int64_t atom;
+    const bool real = slot_atom(slot, pad_off, sp_off, nsp, atom);
+    const unsigned uz = real ? phase[atom].z : 0u;
     uint32_t* hi = reinterpret_cast<uint32_t*>(tab_hi);
     uint32_t* lo = reinterpret_cast<uint32_t*>(tab_lo);
-    for (int t = blockIdx.y; t < table_rows / 2; t += gridDim.y) {
+    for (int t = blockIdx.y; t < nz_count; t += gridDim.y) {
         uint32_t h0 = 0u, l0 = 0u, h1 = 0u, l1 = 0u;
-        if (real && t < nz_count) {
-            float2 z = phase_factor((unsigned)(nz_min + t) * u.z);
-            split2(z.x, -z.y, h0, l0);  // row 2t   (Re out): K(2j) = zr, K(2j+1) = -zi
-            split2(z.y, z.x, h1, l1);   // row 2t+1 (Im out): K(2j) = zi, K(2j+1) = zr
+        if (real) {
+            const float2 z = phase_factor((unsigned)(nz_min + t) * uz);
+            split2(z.x, -z.y, h0, l0);
+            split2(z.y, z.x, h1, l1);
         }
-        int64_t w0 = (int64_t)(2 * t) * (kdim / 2) + slot;
-        int64_t w1 = (int64_t)(2 * t + 1) * (kdim / 2) + slot;
+        const int64_t w0 = (int64_t)(2 * t) * (kdim / 2) + slot;
+        const int64_t w1 = w0 + kdim / 2;
         hi[w0] = h0;
         lo[w0] = l0;
         hi[w1] = h1;
@@ -206,45 +237,64 @@ __global__ void tc_table_kernel(const uint4* __restrict__ phase, const int64_t* 
     }
 }
 
+// FP32 X and Y factor tables: [slot][n - n_min].
+__global__ void tc_xytable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
+                                  const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nx_min,
+                                  int nxr, int ny_min, int nyr, float2* __restrict__ tab_x,
+                                  float2* __restrict__ tab_y) {
+    const int64_t slot = blockIdx.x;
+    int64_t atom;
+    const bool real = slot_atom(slot, pad_off, sp_off, nsp, atom);
+    uint4 u = real ? phase[atom] : make_uint4(0u, 0u, 0u, 0u);
+    for (int t = threadIdx.x; t < nxr + nyr; t += blockDim.x) {
+        if (t < nxr) {
+            tab_x[slot * nxr + t] = real ? phase_factor((unsigned)(nx_min + t) * u.x) : make_float2(0.f, 0.f);
+        } else {
+            const int k = t - nxr;
+            tab_y[slot * nyr + k] = real ? phase_factor((unsigned)(ny_min + k) * u.y) : make_float2(0.f, 0.f);
+        }
+    }
+}
+
 // ---- the contraction kernel ------------------------------------------------
 
 __global__ void __launch_bounds__(kTcThreads, 1)
     sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-                 TcParams p) {
+                 const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_y, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full_a[kMaxStages], full_b[kMaxStages], empty[kMaxStages];
-    __shared__ __align__(8) uint64_t acc_full, acc_empty;
+    __shared__ __align__(8) uint64_t full_tma[kMaxStages], full_a[kMaxStages], empty[kMaxStages];
+    __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const TcTile T = p.tiles[blockIdx.x];
-    const TcChunk C = p.chunks[blockIdx.y];
-    const int ncols = T.ncols;
     const int NS = p.nstages;
-    const int nst = (C.slot1 - C.slot0) / kStageSlots;
     const int F = p.flush_stages;
-    const int nflush = (nst + F - 1) / F;
-    float2* tab = reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes);  // [32][24]
-    const uint32_t tmem_cols = ncols <= 32 ? 32u : ncols <= 64 ? 64u : ncols <= 128 ? 128u : 256u;
+    const int nitems = p.ngroups * p.nchunks;
+    // stage layout: A hi/lo per tile slot, B hi/lo, X/Y per tile slot
+    const int a_bytes = p.tpc * 2 * kATile;
+    const int bmax = (p.stage_bytes - a_bytes - p.tpc * (kXBytes + kYBytes)) / 256;  // max B rows
+    auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
 
     if (tid == 0) {
         abort_flag = 0;
         for (int s = 0; s < NS; ++s) {
+            trj_mbar_init(&full_tma[s], 1);
             trj_mbar_init(&full_a[s], kProducerWarps);
-            trj_mbar_init(&full_b[s], 1);
             trj_mbar_init(&empty[s], 1);
         }
-        trj_mbar_init(&acc_full, 1);
-        trj_mbar_init(&acc_empty, kProducerWarps);
+        for (int b = 0; b < 2; ++b) {
+            trj_mbar_init(&acc_full[b], 1);
+            trj_mbar_init(&acc_empty[b], kEpiWarps);
+        }
         trj_fence_mbar_init();
     }
-    if (warp == 9) {
+    if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          trj_smem_addr(&tmem_slot)),
-                     "r"(tmem_cols)
+                     "r"(512)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -252,155 +302,203 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
+    // accumulator column of (tile slot i, buffer b)
+    auto acc_col = [&](int i, int b) -> uint32_t {
+        return p.tpc == 2 ? (uint32_t)((2 * i + b) * 128) : (uint32_t)(b * 256);
+    };
 
-    if (warp == 8) {
-        // ---- B operand: TMA loads of the Z-phase table (hi and lo), 16 rows per load ----
-        if (lane == 0 && nst > 0) {
-            const unsigned bytes = (unsigned)(2 * ncols * 128);
-            for (int s = 0; s < nst; ++s) {
-                const int slot = s % NS;
-                if (!trj_mbar_wait(&empty[slot], ((s / NS) & 1) ^ 1)) {
-                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                    abort_flag = 1;
-                    break;
-                }
-                uint8_t* bh = smem + (size_t)slot * p.stage_bytes + 2 * kATile;
-                uint8_t* bl = bh + ncols * 128;
-                trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
-                const int k0 = 2 * (C.slot0 + s * kStageSlots);
-                for (int r = 0; r < ncols / 16; ++r) {
-                    tma_load_2d(bh + r * 2048, &map_hi, k0, T.brow + 16 * r, &full_b[slot]);
-                    tma_load_2d(bl + r * 2048, &map_lo, k0, T.brow + 16 * r, &full_b[slot]);
-                }
-            }
-        }
-    } else if (warp == 9) {
-        // ---- MMA issue: one lane ----
-        if (lane == 0 && nst > 0) {
-            const uint32_t idesc = (1u << 4)                    // D: F32
-                                   | (1u << 7) | (1u << 10)     // A, B: BF16
-                                   | ((uint32_t)(ncols >> 3) << 17)
-                                   | ((uint32_t)(128 >> 4) << 24);
-            int f = 0;
-            for (int s = 0; s < nst && !abort_flag; ++s) {
-                const int slot = s % NS;
-                const unsigned par = (s / NS) & 1;
-                const bool first = (s % F) == 0;
-                if (first && s > 0) {
-                    if (!trj_mbar_wait(&acc_empty, (f - 1) & 1)) {
-                        trj_raise(p.status, TRJ_DEV_TIMEOUT);
+    if (warp == kTmaWarp) {
+        if (lane == 0) {
+            int sg = 0;
+            for (int it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x) {
+                const TcGroup G = p.groups[it % p.ngroups];
+                const TcChunk C = p.chunks[it / p.ngroups];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const int ntile = G.t1 >= 0 ? 2 : 1;
+                const TcTile T0 = p.tiles[G.t0];
+                const TcTile T1 = p.tiles[G.t1 >= 0 ? G.t1 : G.t0];
+                const unsigned bytes = (unsigned)(2 * G.bcols * 128 + ntile * (kXBytes + kYBytes));
+                for (int s = 0; s < nst; ++s, ++sg) {
+                    const int slot = sg % NS;
+                    if (!timed_wait(&empty[slot], ((sg / NS) & 1) ^ 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                }
-                if (!trj_mbar_wait(&full_a[slot], par) || !trj_mbar_wait(&full_b[slot], par)) {
-                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                    abort_flag = 1;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t base = trj_smem_addr(smem + (size_t)slot * p.stage_bytes);
-                const uint32_t ahi = base, alo = base + kATile, bhi = base + 2 * kATile,
-                               blo = bhi + ncols * 128;
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const uint32_t o = kk * 32;  // 16 bf16 along K
-                    mma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc, (first && kk == 0) ? 0u : 1u);
-                    mma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(blo + o), idesc, 1u);
-                    mma_bf16(tmem, sw128_desc(alo + o), sw128_desc(bhi + o), idesc, 1u);
-                }
-                mma_commit(&empty[slot]);
-                if ((s + 1) % F == 0 || s == nst - 1) {
-                    mma_commit(&acc_full);
-                    ++f;
+                    uint8_t* st = stage_ptr(slot);
+                    uint8_t* bh = st + a_bytes;
+                    uint8_t* bl = bh + bmax * 128;
+                    uint8_t* xy = bl + bmax * 128;
+                    trj_mbar_arrive_expect_tx(&full_tma[slot], bytes);
+                    const int slot0 = C.slot0 + s * kStageSlots;
+                    const int k0 = 2 * slot0;
+                    for (int r = 0; r < G.bcols / 16; ++r) {
+                        tma_load_2d(bh + r * 2048, &map_hi, k0, G.brow + 16 * r, &full_tma[slot]);
+                        tma_load_2d(bl + r * 2048, &map_lo, k0, G.brow + 16 * r, &full_tma[slot]);
+                    }
+                    tma_load_2d(xy, &map_x, T0.xcol, slot0, &full_tma[slot]);
+                    tma_load_2d(xy + kXBytes, &map_y, T0.ycol, slot0, &full_tma[slot]);
+                    if (ntile == 2) {
+                        tma_load_2d(xy + kXBytes + kYBytes, &map_x, T1.xcol, slot0, &full_tma[slot]);
+                        tma_load_2d(xy + 2 * kXBytes + kYBytes, &map_y, T1.ycol, slot0, &full_tma[slot]);
+                    }
                 }
             }
         }
-    } else {
-        // ---- A operand producers (warps 0-7), then TMEM drain ----
-        const int ptid = tid;  // 0..255
-        const int m = ptid & 127, half = ptid >> 7;
-        const int nxl = m & 15, nyl = m >> 4;
-        const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
-        int f = 0;
-        for (int s = 0; s < nst; ++s) {
-            const int slot = s % NS;
-            const int sbase = C.slot0 + s * kStageSlots;
-            named_bar(1, kProducers);  // previous stage's table reads are done
-            for (int q = ptid; q < kStageSlots * kTabEntries; q += kProducers) {
-                const int j = q / kTabEntries, e = q % kTabEntries;
-                const uint2 uv = p.slot_uv[sbase + j];
-                const unsigned ph = e < kTcTileNx ? (unsigned)(T.nx0 + e) * uv.x
-                                                  : (unsigned)(T.ny0 + e - kTcTileNx) * uv.y;
-                tab[q] = phase_factor(ph);
-            }
-            named_bar(1, kProducers);
-            const bool ok = trj_mbar_wait(&empty[slot], ((s / NS) & 1) ^ 1);
-            if (bar_any(1, kProducers, !ok || abort_flag)) {
-                trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                abort_flag = 1;
-                break;
-            }
-            uint8_t* ahi = smem + (size_t)slot * p.stage_bytes;
-            uint8_t* alo = ahi + kATile;
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const int c = half * 4 + cc;  // 16-byte chunk = 4 atoms along K
-                uint32_t hw[4], lw[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = c * 4 + q;
-                    const float2 x = tab[j * kTabEntries + nxl];
-                    const float2 y = tab[j * kTabEntries + kTcTileNx + nyl];
-                    const float ar = x.x * y.x - x.y * y.y;
-                    const float ai = x.x * y.y + x.y * y.x;
-                    split2(ar, ai, hw[q], lw[q]);
+    } else if (warp == kMmaWarp) {
+        if (lane == 0) {
+            int sg = 0, fg = 0;
+            for (int it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x) {
+                const TcGroup G = p.groups[it % p.ngroups];
+                const TcChunk C = p.chunks[it / p.ngroups];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const int ntile = G.t1 >= 0 ? 2 : 1;
+                uint32_t idesc[2];
+                for (int i = 0; i < 2; ++i) {
+                    const int nc = p.tiles[i == 0 ? G.t0 : (G.t1 >= 0 ? G.t1 : G.t0)].ncols;
+                    idesc[i] = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nc >> 3) << 17) |
+                               ((uint32_t)(128 >> 4) << 24);
                 }
-                const uint32_t off = rowoff + (uint32_t)((c ^ (m & 7)) << 4);
-                *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                *reinterpret_cast<uint4*>(alo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                for (int s = 0; s < nst; ++s, ++sg) {
+                    const int slot = sg % NS;
+                    const unsigned par = (sg / NS) & 1;
+                    const bool first = (s % F) == 0;
+                    const int b = fg & 1;
+                    if (first && fg >= 2 && !timed_wait(&acc_empty[b], ((fg >> 1) - 1) & 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    if (!timed_wait(&full_tma[slot], par, p.status) || !timed_wait(&full_a[slot], par, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = trj_smem_addr(stage_ptr(slot));
+                    const uint32_t bhi = base + a_bytes, blo = bhi + bmax * 128;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        const uint32_t o = kk * 32;  // 16 bf16 along K
+                        for (int i = 0; i < ntile; ++i) {
+                            const uint32_t ahi = base + i * 2 * kATile, alo = ahi + kATile;
+                            const uint32_t d = tmem + acc_col(i, b);
+                            mma_bf16(d, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc[i],
+                                     (first && kk == 0) ? 0u : 1u);
+                            mma_bf16(d, sw128_desc(ahi + o), sw128_desc(blo + o), idesc[i], 1u);
+                            mma_bf16(d, sw128_desc(alo + o), sw128_desc(bhi + o), idesc[i], 1u);
+                        }
+                    }
+                    mma_commit(&empty[slot]);
+                    if ((s + 1) % F == 0 || s == nst - 1) {
+                        mma_commit(&acc_full[b]);
+                        ++fg;
+                    }
+                }
             }
-            fence_proxy_async();
-            __syncwarp();
-            if (lane == 0) trj_mbar_arrive(&full_a[slot]);
-            if ((s + 1) % F == 0 || s == nst - 1) {
-                // drain the FP32 accumulator into this CTA's FP64 block
-                const bool okf = trj_mbar_wait(&acc_full, f & 1);
-                if (bar_any(1, kProducers, !okf)) {
-                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
+        }
+    } else if (warp >= kProducerWarps) {
+        // ---- epilogue: drain the FP32 accumulators into the FP64 blocks ----
+        const int q4 = warp & 3;
+        const int row = 32 * q4 + lane;
+        int fg = 0;
+        bool stop = false;
+        for (int it = blockIdx.x; it < nitems && !stop; it += gridDim.x) {
+            const TcGroup G = p.groups[it % p.ngroups];
+            const int chunk = it / p.ngroups;
+            const TcChunk C = p.chunks[chunk];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const int nflush = (nst + F - 1) / F;
+            const int ntile = G.t1 >= 0 ? 2 : 1;
+            for (int f = 0; f < nflush; ++f, ++fg) {
+                const int b = fg & 1;
+                const bool ok = trj_mbar_wait(&acc_full[b], (fg >> 1) & 1);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
+                    stop = true;
                     break;
                 }
                 tc_fence_after();
-                const int q4 = warp & 3, h2 = warp >> 2;
-                const int row = 32 * q4 + lane;
-                const int c0 = h2 * (ncols / 2), c1 = c0 + ncols / 2;
-                double* dst = p.part + (int64_t)blockIdx.y * p.acc_stride + T.acc_off;
-                for (int c = c0; c < c1; c += 8) {
-                    uint32_t r[8];
-                    tmem_ld8(tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)c, r);
+                for (int i = 0; i < ntile; ++i) {
+                    const TcTile T = p.tiles[i == 0 ? G.t0 : G.t1];
+                    double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
+                    const uint32_t tb = tmem + ((uint32_t)(32 * q4) << 16) + acc_col(i, b);
+                    for (int c = 0; c < T.ncols; c += 16) {
+                        uint32_t r[16];
+                        tmem_ld16(tb + (uint32_t)c, r);
+                        if (f == 0) {
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        double* d = dst + (int64_t)(c + i) * 128 + row;
-                        const double v = (double)__uint_as_float(r[i]);
-                        if (f == 0) *d = v;
-                        else *d += v;
+                            for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(r[k]);
+                        } else {
+                            double old[16];
+#pragma unroll
+                            for (int k = 0; k < 16; ++k) old[k] = dst[(int64_t)(c + k) * 128];
+#pragma unroll
+                            for (int k = 0; k < 16; ++k)
+                                dst[(int64_t)(c + k) * 128] = old[k] + (double)__uint_as_float(r[k]);
+                        }
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&acc_empty);
-                ++f;
+                if (lane == 0) trj_mbar_arrive(&acc_empty[b]);
             }
         }
-        (void)nflush;
+    } else {
+        // ---- A producers (warps 0-7): one A row per thread for tile slot i = tid / 128 ----
+        const int i = tid >> 7;
+        const int m = tid & 127;
+        const int nxl = m & 15, nyl = m >> 4;
+        const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
+        int sg = 0;
+        bool stop = false;
+        for (int it = blockIdx.x; it < nitems && !stop; it += gridDim.x) {
+            const TcGroup G = p.groups[it % p.ngroups];
+            const TcChunk C = p.chunks[it / p.ngroups];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const bool active = i == 0 || G.t1 >= 0;
+            for (int s = 0; s < nst; ++s, ++sg) {
+                const int slot = sg % NS;
+                const bool ok = trj_mbar_wait(&full_tma[slot], (sg / NS) & 1);
+                if (bar_any(1, kProducers, !ok || abort_flag)) {
+                    if (tid == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                if (active) {
+                    uint8_t* st = stage_ptr(slot);
+                    uint8_t* ahi = st + i * 2 * kATile;
+                    uint8_t* alo = ahi + kATile;
+                    const uint8_t* xy = st + a_bytes + 2 * bmax * 128 + i * (kXBytes + kYBytes);
+                    const float2* X = reinterpret_cast<const float2*>(xy);
+                    const float2* Y = reinterpret_cast<const float2*>(xy + kXBytes);
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {  // 16-byte chunk = 4 atoms along K
+                        uint32_t hw[4], lw[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int j = c * 4 + q;
+                            const float2 x = X[j * kTcTileNx + nxl];
+                            const float2 y = Y[j * kTcTileNy + nyl];
+                            const float ar = x.x * y.x - x.y * y.y;
+                            const float ai = x.x * y.y + x.y * y.x;
+                            split2(ar, ai, hw[q], lw[q]);
+                        }
+                        const uint32_t off = rowoff + (uint32_t)((c ^ (m & 7)) << 4);
+                        *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                        *reinterpret_cast<uint4*>(alo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                    }
+                    fence_proxy_async();
+                }
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&full_a[slot]);
+            }
+        }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 9) {
+    if (warp == kMmaWarp) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols)
-                     : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
     }
 }
 
@@ -437,16 +535,17 @@ EncodeTiledFn get_encode() {
     return fn;
 }
 
-int encode_map(trj_ctx* ctx, CUtensorMap* map, void* base, int64_t kdim, int rows) {
+// 2-D map over a row-major [rows][inner] array; inner extent and box inner in elements.
+int encode_map(trj_ctx* ctx, CUtensorMap* map, void* base, CUtensorMapDataType dt, int esize, int64_t inner,
+               int64_t rows, int box_inner, int box_rows, CUtensorMapSwizzle sw) {
     EncodeTiledFn enc = get_encode();
     if (!enc) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
-    cuuint32_t box[2] = {64, 16};
+    cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)inner * esize};
+    cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = enc(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return trj_fail(ctx, TRJ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return TRJ_OK;
 }
@@ -456,8 +555,8 @@ int encode_map(trj_ctx* ctx, CUtensorMap* map, void* base, int64_t kdim, int row
 void trj_sq_tc_release(trj_sq_plan* plan) {
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (!st) return;
-    void* ptrs[] = {st->tiles_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
-                    st->tab_hi, st->tab_lo, st->slot_uv, st->part};
+    void* ptrs[] = {st->tiles_dev, st->groups_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
+                    st->tab_hi, st->tab_lo, st->tab_x, st->tab_y, st->part};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete st;
@@ -476,28 +575,55 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         st->pad_off[a + 1] = st->pad_off[a] + (plan->species_counts[a] + kStageSlots - 1) / kStageSlots * kStageSlots;
     st->total_slots = std::max<int64_t>(st->pad_off[nsp], kStageSlots);
     if (2 * st->total_slots > (int64_t)INT32_MAX) return trj_fail(ctx, TRJ_ERR_CAPACITY, "tensor path: frame too large");
-    // table rows and tiles
+    // table extents
     int nz_min = plan->tiles[0].nz0, nz_max = nz_min;
+    int nx_min = plan->tiles[0].nx0, nx_max = nx_min, ny_min = plan->tiles[0].ny0, ny_max = ny_min;
     for (const SqTile& t : plan->tiles) {
         nz_min = std::min(nz_min, t.nz0);
         nz_max = std::max(nz_max, t.nz0 + t.ncols / 2 - 1);
+        nx_min = std::min(nx_min, t.nx0);
+        nx_max = std::max(nx_max, t.nx0 + kTcTileNx);
+        ny_min = std::min(ny_min, t.ny0);
+        ny_max = std::max(ny_max, t.ny0 + kTcTileNy);
+        st->max_cols = std::max(st->max_cols, t.ncols);
     }
     st->nz_min = nz_min;
     st->table_rows = 2 * (nz_max - nz_min + 1);
+    st->nx_min = nx_min;
+    st->nxr = nx_max - nx_min;
+    st->ny_min = ny_min;
+    st->nyr = ny_max - ny_min;
     std::vector<TcTile> tt(plan->tiles.size());
     int64_t acc = 0;
     for (size_t i = 0; i < plan->tiles.size(); ++i) {
         const SqTile& s = plan->tiles[i];
-        tt[i] = TcTile{s.nx0, s.ny0, s.ncols, 2 * (s.nz0 - nz_min), acc};
+        tt[i] = TcTile{s.nx0, s.ny0, s.ncols, 2 * (s.nz0 - nz_min), 2 * (s.nx0 - nx_min), 2 * (s.ny0 - ny_min), acc};
         acc += (int64_t)s.ncols * 128;
-        st->max_cols = std::max(st->max_cols, s.ncols);
     }
     st->acc_stride = acc;
-    // chunks: each species' slots split so that tiles x chunks covers the GPU about twice
-    const int64_t ntiles = (int64_t)tt.size();
-    const int64_t target_chunks = std::max<int64_t>(nsp, (2 * ctx->sm_count + ntiles - 1) / ntiles);
+    // groups: pair tiles of equal nz0 (sorted by width) when every tile fits two accumulators
+    st->tpc = st->max_cols <= 128 ? 2 : 1;
+    {
+        std::vector<int> order(tt.size());
+        for (size_t i = 0; i < tt.size(); ++i) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            if (plan->tiles[x].nz0 != plan->tiles[y].nz0) return plan->tiles[x].nz0 < plan->tiles[y].nz0;
+            return tt[x].ncols > tt[y].ncols;
+        });
+        size_t k = 0;
+        while (k < order.size()) {
+            const int a = order[k];
+            int b = -1;
+            if (st->tpc == 2 && k + 1 < order.size() && plan->tiles[order[k + 1]].nz0 == plan->tiles[a].nz0)
+                b = order[k + 1];
+            st->groups.push_back(TcGroup{a, b, std::max(tt[a].ncols, b >= 0 ? tt[b].ncols : 0), tt[a].brow});
+            k += b >= 0 ? 2 : 1;
+        }
+    }
+    // chunks: each species' slots split so that groups x chunks covers the GPU a few times
+    const int64_t ngroups = (int64_t)st->groups.size();
+    const int64_t target_chunks = std::max<int64_t>(nsp, (3 * ctx->sm_count + ngroups - 1) / ngroups);
     const int64_t total_real = std::max<int64_t>(1, plan->n_total);
-    st->chunk_begin_dev = nullptr;
     st->chunk_of_species_begin.assign(nsp + 1, 0);
     for (int a = 0; a < nsp; ++a) {
         st->chunk_of_species_begin[a] = (int)st->chunks.size();
@@ -515,33 +641,48 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     }
     st->chunk_of_species_begin[nsp] = (int)st->chunks.size();
     if (st->chunks.empty()) return TRJ_OK;
-    // shared memory: stages of (A hi, A lo, B hi, B lo) + the X/Y phase table
-    st->stage_bytes = 2 * kATile + 2 * st->max_cols * 128;
-    const int table_bytes = kStageSlots * kTabEntries * (int)sizeof(float2);
-    const int avail = (int)ctx->smem_optin - 1024 - table_bytes - 512;
+    // shared memory stage: A hi/lo per tile slot, B hi/lo (max width), X/Y per tile slot
+    st->stage_bytes = st->tpc * 2 * kATile + 2 * st->max_cols * 128 + st->tpc * (kXBytes + kYBytes);
+    const int avail = (int)ctx->smem_optin - 1024 - 512;
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
-    st->smem_bytes = st->nstages * st->stage_bytes + table_bytes + 1024;
+    st->smem_bytes = st->nstages * st->stage_bytes + 1024;
+    const int64_t nitems = ngroups * (int64_t)st->chunks.size();
+    st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
 
     const int64_t kdim = 2 * st->total_slots;
     size_t tab_bytes = (size_t)st->table_rows * (size_t)kdim * sizeof(__nv_bfloat16);
+    size_t x_bytes = sizeof(float2) * (size_t)st->total_slots * st->nxr;
+    size_t y_bytes = sizeof(float2) * (size_t)st->total_slots * st->nyr;
     size_t part_bytes = sizeof(double) * (size_t)st->acc_stride * st->chunks.size();
     std::vector<int32_t> cb(st->chunk_of_species_begin.begin(), st->chunk_of_species_begin.end());
     if (cudaMalloc(&st->tab_hi, tab_bytes) != cudaSuccess || cudaMalloc(&st->tab_lo, tab_bytes) != cudaSuccess ||
-        cudaMalloc(&st->slot_uv, sizeof(uint2) * st->total_slots) != cudaSuccess ||
+        cudaMalloc(&st->tab_x, x_bytes) != cudaSuccess || cudaMalloc(&st->tab_y, y_bytes) != cudaSuccess ||
         cudaMalloc(&st->part, part_bytes) != cudaSuccess ||
         cudaMalloc(&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
+        cudaMalloc(&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
         cudaMalloc(&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
         cudaMalloc(&st->pad_off_dev, sizeof(int64_t) * (nsp + 1)) != cudaSuccess ||
         cudaMalloc(&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess)
-        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables", 2 * tab_bytes + part_bytes);
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
+                        2 * tab_bytes + x_bytes + y_bytes + part_bytes);
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(st->groups_dev, st->groups.data(), sizeof(TcGroup) * st->groups.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunks_dev, st->chunks.data(), sizeof(TcChunk) * st->chunks.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->pad_off_dev, st->pad_off.data(), sizeof(int64_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
-    plan->scratch_bytes += (int64_t)(2 * tab_bytes + part_bytes + sizeof(uint2) * st->total_slots);
-    int rc = encode_map(ctx, &st->map_hi, st->tab_hi, kdim, st->table_rows);
-    if (rc == TRJ_OK) rc = encode_map(ctx, &st->map_lo, st->tab_lo, kdim, st->table_rows);
+    plan->scratch_bytes += (int64_t)(2 * tab_bytes + x_bytes + y_bytes + part_bytes);
+    int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
+                        16, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc == TRJ_OK)
+        rc = encode_map(ctx, &st->map_lo, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
+                        16, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc == TRJ_OK)
+        rc = encode_map(ctx, &st->map_x, st->tab_x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, 2 * (int64_t)st->nxr,
+                        st->total_slots, 2 * kTcTileNx, kStageSlots, CU_TENSOR_MAP_SWIZZLE_NONE);
+    if (rc == TRJ_OK)
+        rc = encode_map(ctx, &st->map_y, st->tab_y, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, 2 * (int64_t)st->nyr,
+                        st->total_slots, 2 * kTcTileNy, kStageSlots, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
@@ -556,28 +697,33 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor-core S(Q) path was not prepared for this plan");
     const int64_t kdim = 2 * st->total_slots;
     const int nz_count = st->table_rows / 2;
-    dim3 tg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 64));
-    tc_table_kernel<<<tg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
-                                       st->total_slots, st->nz_min, nz_count, st->table_rows, kdim, st->tab_hi,
-                                       st->tab_lo, st->slot_uv);
+    dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 32));
+    tc_ztable_kernel<<<zg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
+                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo);
+    tc_xytable_kernel<<<(unsigned)st->total_slots, 128, 0, s>>>(plan->phase_dev, plan->species_off_dev,
+                                                                st->pad_off_dev, plan->nsp, st->total_slots,
+                                                                st->nx_min, st->nxr, st->ny_min, st->nyr, st->tab_x,
+                                                                st->tab_y);
     TcParams P;
     P.tiles = st->tiles_dev;
+    P.groups = st->groups_dev;
     P.chunks = st->chunks_dev;
-    P.slot_uv = st->slot_uv;
     P.part = st->part;
     P.acc_stride = st->acc_stride;
+    P.ngroups = (int)st->groups.size();
+    P.nchunks = (int)st->chunks.size();
     P.nstages = st->nstages;
     P.flush_stages = st->flush_stages;
     P.stage_bytes = st->stage_bytes;
+    P.tpc = st->tpc;
     P.status = ctx->status_dev;
-    dim3 grid((unsigned)plan->tiles.size(), (unsigned)st->chunks.size());
     plan->timer.begin(ctx, s);
-    sq_tc_kernel<<<grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, P);
+    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_x, st->map_y, P);
     plan->timer.end(ctx, s);
     tc_reduce_kernel<<<(unsigned)plan->tiles.size(), 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev,
                                                                   plan->tiles_dev, st->chunk_begin_dev, plan->nsp,
                                                                   plan->tc_out_dev);
-    ctx->launches += 3;
+    ctx->launches += 4;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
 }
