@@ -25,7 +25,9 @@
 
 namespace {
 
-constexpr int kThreads = 256;       // threads per CTA = home atoms per task
+constexpr int kThreads = 256;       // threads per CTA
+constexpr int kHome = 2;            // home atoms per thread
+constexpr int kHomeChunk = kThreads * kHome;
 constexpr int kJChunk = 1024;       // neighbour atoms per staged buffer (16 KB)
 constexpr int kMaxOffsets = 14;
 
@@ -38,8 +40,9 @@ struct RdfParams {
     int nc[3];
     int ncell;
     int noff;
-    int hsplit;
+    int hsplit, jsplit;
     int nrep;
+    int fast_ok;                // every axis split into >= 5 cells
     int off[kMaxOffsets][3];
     int64_t nitems;
 };
@@ -51,6 +54,7 @@ struct TaskInfo {
     int jlocal0;       // index within the neighbour cell of the first staged atom
     int hc;            // home chunk
     int self;          // home cell == neighbour cell
+    int fast;          // no minimum image needed for any pair of the task
     int valid;         // 0 = no more tasks
 };
 
@@ -59,7 +63,7 @@ __device__ __forceinline__ float min_image_exact(float d, float L) {
     return __fsub_rn(d, __fmul_rn(L, n));
 }
 
-// Minimum image of the reference; fast exact branches for |d| far from L/2 and 3L/2.
+// Minimum image of the reference; exact shortcuts for |d| far from L/2 and 3L/2.
 __device__ __forceinline__ float min_image(float d, float L, float t0, float t1, float t2) {
     float a = fabsf(d);
     if (a < t0) return d;
@@ -75,8 +79,8 @@ __device__ __forceinline__ int outcome(float rr2, const RdfParams& p) {
     return (ind <= p.lsmax && ind > 0) ? ind : 0;
 }
 
-// Task iterator run by thread 0: items w = blockIdx.x + k*gridDim.x; item = (cell, offset,
-// home split); tasks = (home chunk, neighbour chunk) of the item.
+// Task iterator run by thread 0: items are taken from a global counter (dynamic balance);
+// item = (cell, offset, home split, neighbour segment); tasks = (home chunk, neighbour chunk).
 struct TaskGen {
     int64_t w;
     int hc, jc;
@@ -86,11 +90,12 @@ struct TaskGen {
 __device__ __forceinline__ int wrapc(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
 
 __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restrict__ cstart,
-                          const int32_t* __restrict__ ccount, TaskInfo& t) {
+                          const int32_t* __restrict__ ccount, const int32_t* __restrict__ cflag,
+                          unsigned long long* work, TaskInfo& t) {
     for (;;) {
         if (!g.started) {
             g.started = 1;
-            g.w = blockIdx.x;
+            g.w = (int64_t)atomicAdd(work, 1ull);
             g.hc = -1;
             g.jc = 0;
         }
@@ -99,51 +104,131 @@ __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restr
             return false;
         }
         int64_t w = g.w;
-        int h = (int)(w % p.hsplit);
-        int64_t r = w / p.hsplit;
-        int o = (int)(r % p.noff);
-        int c = (int)(r / p.noff);
-        int cz = c % p.nc[2];
-        int cy = (c / p.nc[2]) % p.nc[1];
-        int cx = c / (p.nc[2] * p.nc[1]);
-        int c2 = (wrapc(cx + p.off[o][0], p.nc[0]) * p.nc[1] + wrapc(cy + p.off[o][1], p.nc[1])) * p.nc[2] +
-                 wrapc(cz + p.off[o][2], p.nc[2]);
-        int na = ccount[c], nb = ccount[c2];
-        int self = (o == 0);
+        const int seg = (int)(w % p.jsplit);
+        w /= p.jsplit;
+        const int h = (int)(w % p.hsplit);
+        w /= p.hsplit;
+        const int o = (int)(w % p.noff);
+        const int c = (int)(w / p.noff);
+        const int cz = c % p.nc[2];
+        const int cy = (c / p.nc[2]) % p.nc[1];
+        const int cx = c / (p.nc[2] * p.nc[1]);
+        const int ex = cx + p.off[o][0], ey = cy + p.off[o][1], ez = cz + p.off[o][2];
+        const int c2 = (wrapc(ex, p.nc[0]) * p.nc[1] + wrapc(ey, p.nc[1])) * p.nc[2] + wrapc(ez, p.nc[2]);
+        const int na = ccount[c], nb = ccount[c2];
+        const int self = (o == 0);
         if (g.hc < 0) {
             g.hc = h;
             g.jc = 0;
         }
-        // advance within the item
         while (true) {
-            if (g.hc * kThreads >= na) break;  // item done
-            int jfirst = self ? g.hc * kThreads : 0;
-            int jtot = nb - jfirst;
-            int jstart = jfirst + g.jc * kJChunk;
-            if (jtot <= 0 || jstart >= nb) {
+            if (g.hc * kHomeChunk >= na) break;  // item done
+            const int jfirst = self ? g.hc * kHomeChunk : 0;
+            const int jtot = nb - jfirst;
+            const int s0 = jfirst + (int)((int64_t)jtot * seg / p.jsplit);
+            const int s1 = jfirst + (int)((int64_t)jtot * (seg + 1) / p.jsplit);
+            const int jstart = s0 + g.jc * kJChunk;
+            if (jtot <= 0 || jstart >= s1) {
                 g.hc += p.hsplit;
                 g.jc = 0;
                 continue;
             }
+            const bool wraps = ex < 0 || ex >= p.nc[0] || ey < 0 || ey >= p.nc[1] || ez < 0 || ez >= p.nc[2];
             t.sa = cstart[c];
             t.na = na;
             t.sb = cstart[c2] + jstart;
-            t.jcount = min(kJChunk, nb - jstart);
+            t.jcount = min(kJChunk, s1 - jstart);
             t.jlocal0 = jstart;
             t.hc = g.hc;
             t.self = self;
+            t.fast = p.fast_ok && !wraps && !cflag[c] && !cflag[c2];
             t.valid = 1;
             g.jc += 1;
             return true;
         }
-        g.w += gridDim.x;
+        g.w = (int64_t)atomicAdd(work, 1ull);
         g.hc = -1;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
+struct PairCounters {
+    unsigned long long ulp = 0, fma = 0, counted = 0;
+};
+
+// Bin of one candidate pair (rr2 < side2_hi): approximate bin from rsqrt, exact reference
+// arithmetic (and edge statistics) whenever the approximation is within a window of a bin edge
+// or of the cutoff, so the result always equals outcome(rr2).
+// Exact reference outcome of a pair near a bin edge or the cutoff, with its edge statistics.
+__device__ __noinline__ int exact_bin(float rr2, float x2, float dy, float dz, const RdfParams& p,
+                                      PairCounters& pc) {
+    const int ind = outcome(rr2, p);
+    const int olo = outcome(nextafterf(rr2, -INFINITY), p);
+    const int ohi = outcome(nextafterf(rr2, INFINITY), p);
+    pc.ulp += (olo != ind || ohi != ind);
+    const float rr2f = fmaf(dz, dz, fmaf(dy, dy, x2));
+    pc.fma += (outcome(rr2f, p) != ind);
+    return ind;
+}
+
+__device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz, int row, const RdfParams& p,
+                                         unsigned* myhist, PairCounters& pc) {
+    const float q = rr2 * rsqrtf(rr2) * p.inv_deltar;
+    const float fq = q - floorf(q);
+    const float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
+    int ind;
+    if (rr2 >= p.side2_lo || !(fabsf(fq - 0.5f) > win)) {  // NaN (rr2 == 0) takes this path too
+        ind = exact_bin(rr2, x2, dy, dz, p, pc);
+    } else {
+        ind = __float2int_rn(q);
+        if (ind > p.lsmax) ind = 0;
+    }
+    if (ind > 0) {
+        atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
+        ++pc.counted;
+    }
+}
+
+template <bool FAST>
+__device__ __forceinline__ void pair(const float4& a, const float4& b, bool valid, int si, const RdfParams& p,
+                                     const int* rowtab, unsigned* myhist, PairCounters& pc) {
+    float dx = __fsub_rn(b.x, a.x);
+    float dy = __fsub_rn(b.y, a.y);
+    float dz = __fsub_rn(b.z, a.z);
+    if (!FAST) {
+        dx = min_image(dx, p.L[0], p.t0[0], p.t1[0], p.t2[0]);
+        dy = min_image(dy, p.L[1], p.t0[1], p.t1[1], p.t2[1]);
+        dz = min_image(dz, p.L[2], p.t0[2], p.t1[2], p.t2[2]);
+    }
+    const float x2 = __fmul_rn(dx, dx);
+    const float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (valid && rr2 < p.side2_hi) {
+        const int sj = __float_as_int(b.w);
+        if ((unsigned)sj < (unsigned)p.nsp) bin_pair(rr2, x2, dy, dz, rowtab[si * p.nsp + sj], p, myhist, pc);
+    }
+}
+
+template <bool FAST>
+__device__ __forceinline__ void run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
+                                         const float4& a1, bool h0, bool h1, int il0, int il1, int s0, int s1,
+                                         const RdfParams& p, const int* rowtab, unsigned* myhist, PairCounters& pc) {
+    int jbeg = 0;
+    if (ti.self) jbeg = max(0, il0 + 1 - ti.jlocal0);  // il0 < il1: a0 starts earlier
+    if (!h0 && !h1) jbeg = ti.jcount;
+    if (!h0 && h1) jbeg = ti.self ? max(0, il1 + 1 - ti.jlocal0) : 0;
+    const int lim1 = ti.self ? il1 - ti.jlocal0 : -1;  // a1 pairs need jj > lim1
+#pragma unroll 2
+    for (int jj = jbeg; jj < ti.jcount; ++jj) {
+        const float4 b = bj[jj];
+        pair<FAST>(a0, b, h0, s0, p, rowtab, myhist, pc);
+        pair<FAST>(a1, b, h1 && jj > lim1, s1, p, rowtab, myhist, pc);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
                                                              const int32_t* __restrict__ cstart,
                                                              const int32_t* __restrict__ ccount,
+                                                             const int32_t* __restrict__ cflag,
+                                                             unsigned long long* __restrict__ work,
                                                              unsigned long long* __restrict__ hist_g,
                                                              unsigned long long* __restrict__ edge_g,
                                                              unsigned* __restrict__ status) {
@@ -168,13 +253,14 @@ __global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const 
         trj_mbar_init(&bars[0], 1);
         trj_mbar_init(&bars[1], 1);
         trj_fence_mbar_init();
-        if (next_task(gen, p, cstart, ccount, tinfo[0])) {
+        if (next_task(gen, p, cstart, ccount, cflag, work, tinfo[0])) {
             trj_mbar_arrive_expect_tx(&bars[0], tinfo[0].jcount * 16u);
             trj_bulk_g2s(buf, sorted + tinfo[0].sb, tinfo[0].jcount * 16u, &bars[0]);
             issued[0] = 1;
         }
     }
-    unsigned long long n_ulp = 0, n_fma = 0, n_counted = 0, n_tested = 0;
+    PairCounters pc;
+    unsigned long long n_tested = 0;
     for (int t = 0;; ++t) {
         __syncthreads();
         const int slot = t & 1;
@@ -182,61 +268,36 @@ __global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const 
         if (!ti.valid || abort_flag) break;
         if (tid == 0) {
             TaskInfo nx;
-            if (next_task(gen, p, cstart, ccount, nx)) {
+            if (next_task(gen, p, cstart, ccount, cflag, work, nx)) {
                 trj_mbar_arrive_expect_tx(&bars[slot ^ 1], nx.jcount * 16u);
                 trj_bulk_g2s(buf + (slot ^ 1) * kJChunk, sorted + nx.sb, nx.jcount * 16u, &bars[slot ^ 1]);
                 issued[slot ^ 1] += 1;
             }
             tinfo[slot ^ 1] = nx;
         }
+        // home atoms of this task (loaded before the wait to overlap the copy)
+        const int il0 = ti.hc * kHomeChunk + tid, il1 = il0 + kThreads;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a0 = il0 < ti.na ? sorted[ti.sa + il0] : z4;
+        const float4 a1 = il1 < ti.na ? sorted[ti.sa + il1] : z4;
+        const int s0 = __float_as_int(a0.w), s1 = __float_as_int(a1.w);
+        // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
+        const bool h0 = il0 < ti.na && (unsigned)s0 < (unsigned)p.nsp;
+        const bool h1 = il1 < ti.na && (unsigned)s1 < (unsigned)p.nsp;
         if (!trj_mbar_wait(&bars[slot], (t >> 1) & 1)) {
             trj_raise(status, TRJ_DEV_TIMEOUT);
             abort_flag = 1;
             continue;  // the barrier at the loop head sees the flag
         }
-        const int il = ti.hc * kThreads + tid;
-        float4 ai = il < ti.na ? sorted[ti.sa + il] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const int si = __float_as_int(ai.w);
-        // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
-        const bool has_i = il < ti.na && (unsigned)si < (unsigned)p.nsp;
         const float4* bj = buf + slot * kJChunk;
-        // For a self task, only j > i (indices within the same cell).
-        int jbeg = 0;
-        if (ti.self) jbeg = max(0, il + 1 - ti.jlocal0);
-        if (!has_i) jbeg = ti.jcount;
-        n_tested += (unsigned long long)max(0, ti.jcount - jbeg);
-        for (int jj = jbeg; jj < ti.jcount; ++jj) {
-            const float4 b = bj[jj];
-            float dx = min_image(__fsub_rn(b.x, ai.x), p.L[0], p.t0[0], p.t1[0], p.t2[0]);
-            float dy = min_image(__fsub_rn(b.y, ai.y), p.L[1], p.t0[1], p.t1[1], p.t2[1]);
-            float dz = min_image(__fsub_rn(b.z, ai.z), p.L[2], p.t0[2], p.t1[2], p.t2[2]);
-            float x2 = __fmul_rn(dx, dx);
-            float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-            if (rr2 < p.side2_hi) {
-                float rr = __fsqrt_rn(rr2);
-                float q = __fmul_rn(rr, p.inv_deltar);
-                float fq = q - floorf(q);
-                float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
-                int ind;
-                if (rr2 >= p.side2_lo || fabsf(fq - 0.5f) <= win) {
-                    ind = outcome(rr2, p);
-                    int olo = outcome(nextafterf(rr2, -INFINITY), p);
-                    int ohi = outcome(nextafterf(rr2, INFINITY), p);
-                    n_ulp += (olo != ind || ohi != ind);
-                    float rr2f = fmaf(dz, dz, fmaf(dy, dy, x2));
-                    n_fma += (outcome(rr2f, p) != ind);
-                } else {
-                    ind = __float2int_rn(q);
-                    if (ind > p.lsmax) ind = 0;
-                }
-                const int sj = __float_as_int(b.w);
-                if (ind > 0 && (unsigned)sj < (unsigned)p.nsp) {
-                    int row = rowtab[si * p.nsp + sj];
-                    atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
-                    ++n_counted;
-                }
-            }
+        if (ti.self) {
+            n_tested += (unsigned long long)(h0 ? max(0, ti.jcount - max(0, il0 + 1 - ti.jlocal0)) : 0);
+            n_tested += (unsigned long long)(h1 ? max(0, ti.jcount - max(0, il1 + 1 - ti.jlocal0)) : 0);
+        } else {
+            n_tested += (unsigned long long)((h0 ? ti.jcount : 0) + (h1 ? ti.jcount : 0));
         }
+        if (ti.fast) run_task<true>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc);
+        else run_task<false>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc);
     }
     if (tid == 0 && abort_flag) {
         // Let copies still in flight land before the CTA exits (bounded).
@@ -251,6 +312,7 @@ __global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const 
         if (s) atomicAdd(&hist_g[k], s);
     }
     if (edge_g) {
+        unsigned long long n_ulp = pc.ulp, n_fma = pc.fma, n_counted = pc.counted;
         for (int off = 16; off > 0; off >>= 1) {
             n_ulp += __shfl_down_sync(0xffffffffu, n_ulp, off);
             n_fma += __shfl_down_sync(0xffffffffu, n_fma, off);
@@ -269,7 +331,8 @@ __global__ void __launch_bounds__(kThreads) rdf_pairs_kernel(RdfParams p, const 
 // Cell of each atom from its wrapped coordinate; per-cell counts and slots.
 __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n, float Lx, float Ly,
                                    float Lz, int ncx, int ncy, int ncz, int32_t* __restrict__ ccount,
-                                   int32_t* __restrict__ acell, int32_t* __restrict__ aslot) {
+                                   int32_t* __restrict__ cflag, int32_t* __restrict__ acell,
+                                   int32_t* __restrict__ aslot) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 v = packed[i];
@@ -277,8 +340,10 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     int nc[3] = {ncx, ncy, ncz};
     float r[3] = {v.x, v.y, v.z};
     int k[3];
+    bool outside = false;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        outside |= !(r[d] >= 0.0f && r[d] < L[d]);
         float w = r[d] - L[d] * floorf(r[d] / L[d]);
         int c = (int)(w * ((float)nc[d] / L[d]));
         c = c < 0 ? 0 : (c >= nc[d] ? nc[d] - 1 : c);
@@ -287,6 +352,7 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     int c = (k[0] * ncy + k[1]) * ncz + k[2];
     acell[i] = c;
     aslot[i] = atomicAdd(&ccount[c], 1);
+    if (outside) cflag[c] = 1;
 }
 
 __global__ void cell_scatter_kernel(const float4* __restrict__ packed, int64_t n,
@@ -330,6 +396,8 @@ struct trj_rdf_plan {
     int ncell_cap = 0;
     int nc[3] = {1, 1, 1};
     int32_t* ccount = nullptr;  // ncell_cap
+    int32_t* cflag = nullptr;   // ncell_cap: cell holds a coordinate outside [0, L)
+    unsigned long long* work = nullptr;  // item counter of the pair kernel
     int32_t* cstart = nullptr;  // ncell_cap + 1
     int32_t* acell = nullptr;   // n_max
     int32_t* aslot = nullptr;   // n_max
@@ -392,7 +460,7 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     // Room for a box up to 25% smaller per axis (more cells) without re-planning.
     p->ncell_cap = std::max(ncell * 2 + 64, 64);
     trj_device_guard g(ctx->device);
-    size_t bytes = sizeof(int32_t) * (size_t)(2 * p->ncell_cap + 1) +
+    size_t bytes = 64 + sizeof(int32_t) * (size_t)(3 * p->ncell_cap + 1) +
                    (sizeof(int32_t) * 2 + sizeof(float4)) * (size_t)std::max<int64_t>(n_max, 1);
     char* base = nullptr;
     if (cudaMalloc(&base, bytes + 256) != cudaSuccess) {
@@ -404,6 +472,9 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     p->aslot = p->acell + std::max<int64_t>(n_max, 1);
     p->ccount = p->aslot + std::max<int64_t>(n_max, 1);
     p->cstart = p->ccount + p->ncell_cap;
+    p->cflag = p->cstart + p->ncell_cap + 1;
+    p->work = reinterpret_cast<unsigned long long*>(
+        (reinterpret_cast<uintptr_t>(p->cflag + p->ncell_cap) + 15) & ~(uintptr_t)15);
     p->scratch_bytes = (int64_t)bytes;
     *out = p;
     return TRJ_OK;
@@ -496,8 +567,13 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
             }
     P.noff = no;
     double avg = (double)n / P.ncell;
-    P.hsplit = std::max(1, (int)ceil(avg * 1.25 / kThreads));
-    P.nitems = (int64_t)P.ncell * P.noff * P.hsplit;
+    P.hsplit = std::max(1, (int)ceil(avg / kHomeChunk));
+    P.fast_ok = P.nc[0] >= 5 && P.nc[1] >= 5 && P.nc[2] >= 5;
+    // Split neighbour ranges when there are too few (cell, offset, home chunk) items to fill the GPU.
+    int64_t base_items = (int64_t)P.ncell * P.noff * P.hsplit;
+    int64_t want = (int64_t)ctx->sm_count * 4;
+    P.jsplit = (int)std::max<int64_t>(1, std::min<int64_t>(64, (want + base_items - 1) / base_items));
+    P.nitems = base_items * P.jsplit;
 
     // Shared memory: two staging buffers + histogram replicas.
     size_t hist_bytes = (size_t)P.nit * P.lsmax * 4;
@@ -519,16 +595,18 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
 
     // Cell binning: count, scan, scatter.
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->ccount, 0, sizeof(int32_t) * P.ncell, s));
+    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->cflag, 0, sizeof(int32_t) * P.ncell, s));
+    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->work, 0, sizeof(unsigned long long), s));
     unsigned nb = (unsigned)((n + 255) / 256);
     cell_assign_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, box[0], box[1], box[2], P.nc[0],
-                                          P.nc[1], P.nc[2], plan->ccount, plan->acell, plan->aslot);
+                                          P.nc[1], P.nc[2], plan->ccount, plan->cflag, plan->acell, plan->aslot);
     scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->ccount, plan->cstart, P.ncell);
     cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->acell, plan->aslot, plan->cstart,
                                            plan->sorted);
     int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
     plan->timer.begin(ctx, s);
     rdf_pairs_kernel<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount,
-                                                            (unsigned long long*)hist_dev,
+                                                            plan->cflag, plan->work, (unsigned long long*)hist_dev,
                                                             (unsigned long long*)edge_dev, ctx->status_dev);
     plan->timer.end(ctx, s);
     ctx->launches += 4;
