@@ -28,7 +28,7 @@ namespace {
 constexpr int kThreads = 256;       // threads per CTA
 constexpr int kHome = 2;            // home atoms per thread
 constexpr int kHomeChunk = kThreads * kHome;
-constexpr int kJChunk = 1024;       // neighbour atoms per staged buffer (16 KB)
+constexpr int kJChunk = 512;        // neighbour atoms per staged buffer (8 KB)
 constexpr int kMaxOffsets = 14;
 
 struct RdfParams {
@@ -182,10 +182,7 @@ __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz
         ind = __float2int_rn(q);
         if (ind > p.lsmax) ind = 0;
     }
-    if (ind > 0) {
-        atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
-        ++pc.counted;
-    }
+    if (ind > 0) atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
 }
 
 template <bool FAST>
@@ -224,7 +221,7 @@ __device__ __forceinline__ void run_task(const TaskInfo& ti, const float4* __res
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 2) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
+__global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
                                                              const int32_t* __restrict__ cstart,
                                                              const int32_t* __restrict__ ccount,
                                                              const int32_t* __restrict__ cflag,
@@ -305,11 +302,12 @@ __global__ void __launch_bounds__(kThreads, 2) rdf_pairs_kernel(RdfParams p, con
             if (issued[sl]) trj_mbar_wait(&bars[sl], (issued[sl] - 1) & 1);
     }
     __syncthreads();
-    // Merge replicas into the global uint64 histogram.
+    // Merge replicas into the global uint64 histogram (their total is the counted pairs).
     for (int k = tid; k < hsz; k += blockDim.x) {
         unsigned long long s = 0;
         for (int r = 0; r < p.nrep; ++r) s += hist[(size_t)r * hsz + k];
         if (s) atomicAdd(&hist_g[k], s);
+        pc.counted += s;
     }
     if (edge_g) {
         unsigned long long n_ulp = pc.ulp, n_fma = pc.fma, n_counted = pc.counted;
@@ -579,14 +577,20 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
     size_t hist_bytes = (size_t)P.nit * P.lsmax * 4;
     size_t stage = 2 * kJChunk * sizeof(float4);
     size_t optin = ctx->smem_optin;
-    // Aim for 2 CTAs per SM (16 warps) when the replicas allow it.
-    int ctas_per_sm = 2;
-    size_t per_cta = optin / 2 - 2048;
-    int nrep = (int)std::min<size_t>(8, per_cta > stage ? (per_cta - stage) / hist_bytes : 0);
-    if (nrep < 2) {
-        ctas_per_sm = 1;
-        nrep = (int)std::min<size_t>(8, (optin - 2048 - stage) / hist_bytes);
+    // Most CTAs per SM (up to 4, i.e. 32 warps) that still hold >= 2 histogram replicas each;
+    // a single CTA per SM otherwise.
+    const size_t sm_smem = optin + 1024;  // per-SM shared memory (the opt-in limit plus the driver's block reserve)
+    int ctas_per_sm = 1, nrep = 0;
+    for (int k = 4; k >= 2; --k) {
+        size_t per_cta = sm_smem / k - 1024 - 1280;  // driver reserve + static shared memory
+        int r = per_cta > stage ? (int)std::min<size_t>(8, (per_cta - stage) / hist_bytes) : 0;
+        if (r >= 2) {
+            ctas_per_sm = k;
+            nrep = r;
+            break;
+        }
     }
+    if (nrep < 2) nrep = (int)std::min<size_t>(8, (optin - 2048 - stage) / hist_bytes);
     if (nrep < 1) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf accumulate: histogram too large");
     P.nrep = nrep;
     size_t smem = stage + (size_t)nrep * hist_bytes;
