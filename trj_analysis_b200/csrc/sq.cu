@@ -131,9 +131,11 @@ __global__ void gather_dense_kernel(const double* __restrict__ tc_out, const int
     int64_t o = src[v];
     if (o < 0) return;
     int64_t stride = tile_species_stride[v];
+    const bool conj = stride < 0;  // evaluated through -k: rho(k) = conj(rho(-k))
+    if (conj) stride = -stride;
     for (int a = 0; a < nsp; ++a) {
         const double* b = tc_out + o + a * stride;
-        rho[(int64_t)a * nvec + v] = make_double2(b[0], b[kTcRows]);
+        rho[(int64_t)a * nvec + v] = make_double2(b[0], conj ? -b[kTcRows] : b[kTcRows]);
     }
 }
 
@@ -273,19 +275,27 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     }
     for (int b = 0; b < nbins; ++b) bstart[b + 1] += bstart[b];
 
-    // Tensor tiles over the dense vectors: group by (nx/16, ny/8) blocks, nz span per block,
-    // split into column groups of <= 256 (128 nz values).
+    // Tensor tiles over the dense vectors.  rho(-k) = conj(rho(k)), so every vector is evaluated
+    // through its representative with (nx, ny) in the half plane {ny > 0, or ny == 0 and nx >= 0}
+    // (the negated vector, conjugated, when its own (nx, ny) is outside).  Representatives are
+    // grouped by (nx/16, ny/8) blocks; a block's nz span (both signs) becomes the tile's columns,
+    // split into column groups of <= 256 (128 nz values).  A negative stride marks a conjugate.
     std::vector<int64_t> dense_src(nvec, -1), dense_stride(nvec, 0);
     if (!dense_idx.empty()) {
-        struct Key { int bx, by; };
+        struct Rep { int x, y, z; bool conj; };
+        std::vector<Rep> rep(nvec);
         std::vector<std::pair<std::pair<int, int>, int64_t>> keyed;
         keyed.reserve(dense_idx.size());
         auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
-        for (int64_t k : dense_idx)
-            keyed.push_back({{fdiv(vecs[k].x, kTcTileNx), fdiv(vecs[k].y, kTcTileNy)}, k});
+        for (int64_t k : dense_idx) {
+            const int x = vecs[k].x, y = vecs[k].y, z = vecs[k].z;
+            const bool in_half = y > 0 || (y == 0 && x >= 0);
+            rep[k] = in_half ? Rep{x, y, z, false} : Rep{-x, -y, -z, true};
+            keyed.push_back({{fdiv(rep[k].x, kTcTileNx), fdiv(rep[k].y, kTcTileNy)}, k});
+        }
         std::sort(keyed.begin(), keyed.end(), [&](const auto& A, const auto& B) {
             if (A.first != B.first) return A.first < B.first;
-            return vecs[A.second].z < vecs[B.second].z;
+            return rep[A.second].z < rep[B.second].z;
         });
         int64_t off = 0;
         size_t i = 0;
@@ -295,10 +305,10 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
             // nz values of this block, sorted ascending in keyed[i..j)
             size_t a = i;
             while (a < j) {
-                int z0 = vecs[keyed[a].second].z;
+                int z0 = rep[keyed[a].second].z;
                 size_t b = a;
-                while (b < j && vecs[keyed[b].second].z - z0 < kTcMaxCols / 2) ++b;
-                int zspan = vecs[keyed[b - 1].second].z - z0 + 1;
+                while (b < j && rep[keyed[b].second].z - z0 < kTcMaxCols / 2) ++b;
+                int zspan = rep[keyed[b - 1].second].z - z0 + 1;
                 int ncols = ((2 * zspan + 15) / 16) * 16;
                 SqTile t;
                 t.nx0 = keyed[a].first.first * kTcTileNx;
@@ -308,10 +318,10 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
                 t.out_off = off;
                 for (size_t q = a; q < b; ++q) {
                     int64_t k = keyed[q].second;
-                    int row = (vecs[k].x - t.nx0) + kTcTileNx * (vecs[k].y - t.ny0);
-                    int col = 2 * (vecs[k].z - t.nz0);
+                    int row = (rep[k].x - t.nx0) + kTcTileNx * (rep[k].y - t.ny0);
+                    int col = 2 * (rep[k].z - t.nz0);
                     dense_src[k] = off + (int64_t)col * kTcRows + row;
-                    dense_stride[k] = (int64_t)ncols * kTcRows;
+                    dense_stride[k] = (rep[k].conj ? -1 : 1) * (int64_t)ncols * kTcRows;
                 }
                 p->tile_slots += (int64_t)kTcRows * (ncols / 2);
                 off += (int64_t)nsp * ncols * kTcRows;

@@ -66,6 +66,8 @@ struct TcParams {
     const TcTile* tiles;
     const TcGroup* groups;
     const TcChunk* chunks;
+    const int32_t* cta_items;   // item ids (chunk * ngroups + group) of every CTA, concatenated
+    const int32_t* cta_off;     // gridDim.x + 1 offsets into cta_items
     double* part;           // [chunk][acc_stride]
     int64_t acc_stride;
     int ngroups, nchunks;
@@ -85,6 +87,7 @@ struct TcState {
     std::vector<int> chunk_of_species_begin;  // nsp+1
     TcTile* tiles_dev = nullptr;
     TcGroup* groups_dev = nullptr;
+    int32_t* sched_dev = nullptr;   // [grid + 1 offsets][items]
     TcChunk* chunks_dev = nullptr;
     int64_t* pad_off_dev = nullptr;
     int32_t* chunk_begin_dev = nullptr;
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NS = p.nstages;
     const int F = p.flush_stages;
-    const int nitems = p.ngroups * p.nchunks;
+    const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
     // stage layout: A hi/lo per tile slot, B hi/lo, X/Y per tile slot
     const int a_bytes = p.tpc * 2 * kATile;
     const int bmax = (p.stage_bytes - a_bytes - p.tpc * (kXBytes + kYBytes)) / 256;  // max B rows
@@ -310,7 +313,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (warp == kTmaWarp) {
         if (lane == 0) {
             int sg = 0;
-            for (int it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x) {
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cta_items[li];
                 const TcGroup G = p.groups[it % p.ngroups];
                 const TcChunk C = p.chunks[it / p.ngroups];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
@@ -346,8 +350,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == kMmaWarp) {
         if (lane == 0) {
+            // Descriptors of every stage slot, built once; a K-step of 16 bf16 (32 bytes) adds 2
+            // to the start-address field, the lo operand of A sits kATile bytes after the hi one.
+            uint64_t adesc[kMaxStages][2], bdesc[kMaxStages];
+            for (int sl = 0; sl < NS; ++sl) {
+                const uint32_t base = trj_smem_addr(stage_ptr(sl));
+                adesc[sl][0] = sw128_desc(base);
+                adesc[sl][1] = sw128_desc(base + 2 * kATile);
+                bdesc[sl] = sw128_desc(base + a_bytes);
+            }
+            const uint64_t a_lo = (uint64_t)(kATile >> 4), b_lo = (uint64_t)((bmax * 128) >> 4);
             int sg = 0, fg = 0;
-            for (int it = blockIdx.x; it < nitems && !abort_flag; it += gridDim.x) {
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cta_items[li];
                 const TcGroup G = p.groups[it % p.ngroups];
                 const TcChunk C = p.chunks[it / p.ngroups];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
@@ -372,18 +387,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t base = trj_smem_addr(stage_ptr(slot));
-                    const uint32_t bhi = base + a_bytes, blo = bhi + bmax * 128;
+                    const uint64_t bh = bdesc[slot], bl = bh + b_lo;
+                    const uint32_t d0 = tmem + acc_col(0, b), d1 = tmem + acc_col(1, b);
+                    const uint64_t a0h = adesc[slot][0], a0l = a0h + a_lo;
+                    const uint64_t a1h = adesc[slot][1], a1l = a1h + a_lo;
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
-                        const uint32_t o = kk * 32;  // 16 bf16 along K
-                        for (int i = 0; i < ntile; ++i) {
-                            const uint32_t ahi = base + i * 2 * kATile, alo = ahi + kATile;
-                            const uint32_t d = tmem + acc_col(i, b);
-                            mma_bf16(d, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc[i],
-                                     (first && kk == 0) ? 0u : 1u);
-                            mma_bf16(d, sw128_desc(ahi + o), sw128_desc(blo + o), idesc[i], 1u);
-                            mma_bf16(d, sw128_desc(alo + o), sw128_desc(bhi + o), idesc[i], 1u);
+                        const uint64_t o = 2 * kk;
+                        mma_bf16(d0, a0h + o, bh + o, idesc[0], (first && kk == 0) ? 0u : 1u);
+                        mma_bf16(d0, a0h + o, bl + o, idesc[0], 1u);
+                        mma_bf16(d0, a0l + o, bh + o, idesc[0], 1u);
+                        if (ntile == 2) {
+                            mma_bf16(d1, a1h + o, bh + o, idesc[1], (first && kk == 0) ? 0u : 1u);
+                            mma_bf16(d1, a1h + o, bl + o, idesc[1], 1u);
+                            mma_bf16(d1, a1l + o, bh + o, idesc[1], 1u);
                         }
                     }
                     mma_commit(&empty[slot]);
@@ -400,7 +417,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int row = 32 * q4 + lane;
         int fg = 0;
         bool stop = false;
-        for (int it = blockIdx.x; it < nitems && !stop; it += gridDim.x) {
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cta_items[li];
             const TcGroup G = p.groups[it % p.ngroups];
             const int chunk = it / p.ngroups;
             const TcChunk C = p.chunks[chunk];
@@ -450,7 +468,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
         int sg = 0;
         bool stop = false;
-        for (int it = blockIdx.x; it < nitems && !stop; it += gridDim.x) {
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cta_items[li];
             const TcGroup G = p.groups[it % p.ngroups];
             const TcChunk C = p.chunks[it / p.ngroups];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
@@ -555,7 +574,7 @@ int encode_map(trj_ctx* ctx, CUtensorMap* map, void* base, CUtensorMapDataType d
 void trj_sq_tc_release(trj_sq_plan* plan) {
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (!st) return;
-    void* ptrs[] = {st->tiles_dev, st->groups_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
+    void* ptrs[] = {st->sched_dev, st->tiles_dev, st->groups_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
                     st->tab_hi, st->tab_lo, st->tab_x, st->tab_y, st->part};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -622,7 +641,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     }
     // chunks: each species' slots split so that groups x chunks covers the GPU a few times
     const int64_t ngroups = (int64_t)st->groups.size();
-    const int64_t target_chunks = std::max<int64_t>(nsp, (3 * ctx->sm_count + ngroups - 1) / ngroups);
+    const int64_t target_chunks = std::max<int64_t>(nsp, (6 * ctx->sm_count + ngroups - 1) / ngroups);
     const int64_t total_real = std::max<int64_t>(1, plan->n_total);
     st->chunk_of_species_begin.assign(nsp + 1, 0);
     for (int a = 0; a < nsp; ++a) {
@@ -649,6 +668,40 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     st->smem_bytes = st->nstages * st->stage_bytes + 1024;
     const int64_t nitems = ngroups * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
+    // Longest-processing-time-first schedule: items costed by (columns + producer work) x stages,
+    // each assigned to the least-loaded CTA; every CTA then walks its items in chunk order.
+    std::vector<int32_t> sched;
+    {
+        std::vector<std::pair<double, int32_t>> items;
+        items.reserve(nitems);
+        for (int64_t c = 0; c < (int64_t)st->chunks.size(); ++c) {
+            const double stages = (double)(st->chunks[c].slot1 - st->chunks[c].slot0) / kStageSlots;
+            for (int64_t g = 0; g < ngroups; ++g) {
+                const TcGroup& G = st->groups[g];
+                const double cols = tt[G.t0].ncols + (G.t1 >= 0 ? tt[G.t1].ncols : 0);
+                const double rows = G.t1 >= 0 ? 256.0 : 128.0;
+                items.push_back({stages * (cols + 0.5 * rows), (int32_t)(c * ngroups + g)});
+            }
+        }
+        std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        std::vector<std::vector<int32_t>> lists(st->grid);
+        std::vector<std::pair<double, int>> heap;  // (load, cta), min-heap
+        for (int b = 0; b < st->grid; ++b) heap.push_back({0.0, b});
+        auto cmp = [](const std::pair<double, int>& a, const std::pair<double, int>& b) { return a > b; };
+        std::make_heap(heap.begin(), heap.end(), cmp);
+        for (const auto& it : items) {
+            std::pop_heap(heap.begin(), heap.end(), cmp);
+            heap.back().first += it.first;
+            lists[heap.back().second].push_back(it.second);
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+        sched.assign(st->grid + 1, 0);
+        for (int b = 0; b < st->grid; ++b) {
+            std::sort(lists[b].begin(), lists[b].end());
+            sched[b + 1] = sched[b] + (int32_t)lists[b].size();
+        }
+        for (int b = 0; b < st->grid; ++b) sched.insert(sched.end(), lists[b].begin(), lists[b].end());
+    }
 
     const int64_t kdim = 2 * st->total_slots;
     size_t tab_bytes = (size_t)st->table_rows * (size_t)kdim * sizeof(__nv_bfloat16);
@@ -663,7 +716,8 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         cudaMalloc(&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
         cudaMalloc(&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
         cudaMalloc(&st->pad_off_dev, sizeof(int64_t) * (nsp + 1)) != cudaSuccess ||
-        cudaMalloc(&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess)
+        cudaMalloc(&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
+        cudaMalloc(&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
         return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
                         2 * tab_bytes + x_bytes + y_bytes + part_bytes);
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
@@ -671,6 +725,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     cudaMemcpy(st->chunks_dev, st->chunks.data(), sizeof(TcChunk) * st->chunks.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->pad_off_dev, st->pad_off.data(), sizeof(int64_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(st->sched_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
     plan->scratch_bytes += (int64_t)(2 * tab_bytes + x_bytes + y_bytes + part_bytes);
     int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
                         16, CU_TENSOR_MAP_SWIZZLE_128B);
@@ -708,6 +763,8 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.tiles = st->tiles_dev;
     P.groups = st->groups_dev;
     P.chunks = st->chunks_dev;
+    P.cta_off = st->sched_dev;
+    P.cta_items = st->sched_dev + st->grid + 1;
     P.part = st->part;
     P.acc_stride = st->acc_stride;
     P.ngroups = (int)st->groups.size();
