@@ -94,6 +94,23 @@ TRJ_API int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* sp
                    int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
                    void* stream);
 
+/* trj_frame_pack without any device allocation (this entry point has no
+ * counterpart in the reference).  It is for callers that may not have the
+ * library allocate device memory: applications whose device memory belongs to
+ * another allocator (a framework's caching allocator, a pre-sized arena) and
+ * frame loops that cannot take the implicit synchronisation of cudaMalloc.
+ * The per-block scratch is a fixed 1 MiB device array inside the library:
+ * ceil(n/1024) * nsp must be <= 87381, larger frames get TRJ_ERR_CAPACITY.
+ * Every GPU that loads the library keeps that array until the process exits.
+ * The first call on a device resolves the array's address on that device
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array and overwrite what they use: calls whose work
+ * overlaps on the GPU (other streams or host threads) race on it.
+ * Arguments and results are those of trj_frame_pack. */
+TRJ_API int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
+                                  int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
+                                  void* stream);
+
 /* ---- g_ab(r) --------------------------------------------------------- */
 /* Replaces RDF_init (src/modules/rdf.cuf:51-122) with the rcrdf clip of
  * select_ncdfinput (src/core/netcdf.f90:610-617): rcrdf_eff = min(rcrdf, min(box)/2),

@@ -5,6 +5,8 @@
 // periodic fold r = r - L*int(r/L) (netcdf.f90:681), both on the device.
 #include <stdarg.h>
 
+#include <mutex>
+
 #include "trj_common.cuh"
 
 int trj_fail(trj_ctx* ctx, int code, const char* fmt, ...) {
@@ -275,6 +277,92 @@ extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t*
     pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
     pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(
         xyz_dev, species_dev, n, nsp, box[0], box[1], box[2], block_base, (float4*)packed_dev);
+    ctx->launches += 3;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Frame layout without allocation.
+//
+// trj_frame_pack_static runs the same three layout kernels as trj_frame_pack, but its
+// per-block species counts and block offsets live in the fixed device array below instead of
+// context scratch grown with cudaMalloc.  It serves callers that may not allocate device memory
+// from inside the library: applications whose device memory is owned by another allocator (a
+// framework's caching allocator, a pre-sized arena) and that forbid foreign allocations, and
+// frame loops that cannot take the implicit device synchronisation of cudaMalloc/cudaFree.
+//
+// Limit: ceil(n / 1024) * nsp * 12 bytes must fit in kPackStaticBytes (1 MiB), i.e.
+// ceil(n / 1024) * nsp <= 87381 (about 29.8 million atoms for 3 species, 5.5 million for 16).
+// Every GPU that loads this library holds the 1 MiB array until the process exits.  All calls
+// share it: each call overwrites every word it reads (nothing has to start at zero), and calls
+// whose kernels overlap on the GPU (different streams, other host threads) race on it.
+// ---------------------------------------------------------------------------
+
+constexpr size_t kPackStaticBytes = (size_t)1 << 20;
+static __device__ __align__(256) unsigned char g_pack_static[kPackStaticBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_pack_static_mu;
+void* g_pack_static_addr[kMaxDevices] = {};
+
+// Device address of g_pack_static on the current device, resolved once per device.
+int pack_static_address(trj_ctx* ctx, void** out) {
+    if (ctx->device < 0 || ctx->device >= kMaxDevices)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "trj_frame_pack_static: device ordinal %d >= %d", ctx->device,
+                        kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_pack_static_mu);
+    if (!g_pack_static_addr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_pack_static);
+        if (e != cudaSuccess || !p)
+            return trj_fail(ctx, TRJ_ERR_CUDA, "trj_frame_pack_static: cudaGetSymbolAddress failed: %s",
+                            cudaGetErrorString(e));
+        g_pack_static_addr[ctx->device] = p;
+    }
+    *out = g_pack_static_addr[ctx->device];
+    return TRJ_OK;
+}
+}  // namespace
+
+extern "C" int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
+                                     int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
+                                     void* stream) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    if (n < 0 || nsp < 1 || nsp > kMaxSpecies || !box)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_static: n=%lld nsp=%d (1..%d)", (long long)n, nsp,
+                        kMaxSpecies);
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_static: box edges must be positive");
+    if (n > 0 && (!xyz_dev || !species_dev || !packed_dev))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_static: null pointer");
+    if (!counts_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_static: null counts");
+    if (((uintptr_t)packed_dev) % 16 != 0)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_static: packed_dev must be 16-byte aligned");
+    const int64_t nblocks = (n + kPackChunk - 1) / kPackChunk;
+    const size_t need = (size_t)nblocks * nsp * (sizeof(int64_t) + sizeof(int32_t));
+    if (need > kPackStaticBytes)
+        return trj_fail(ctx, TRJ_ERR_CAPACITY,
+                        "trj_frame_pack_static: n=%lld with nsp=%d needs %zu bytes of scratch; the fixed array holds "
+                        "%zu (ceil(n/1024)*nsp must be <= %zu)",
+                        (long long)n, nsp, need, kPackStaticBytes, kPackStaticBytes / 12);
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (nblocks == 0) {
+        TRJ_CUDA_TRY(ctx, cudaMemsetAsync(counts_dev, 0, sizeof(int64_t) * nsp, s));
+        return TRJ_OK;
+    }
+    void* scratch = nullptr;
+    int rc = pack_static_address(ctx, &scratch);
+    if (rc != TRJ_OK) return rc;
+    int64_t* block_base = (int64_t*)scratch;
+    int32_t* block_counts = (int32_t*)(block_base + nblocks * nsp);
+    pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, block_counts,
+                                                                 ctx->status_dev);
+    pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
+    pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, box[0], box[1],
+                                                                   box[2], block_base, (float4*)packed_dev);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
