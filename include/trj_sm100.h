@@ -118,6 +118,13 @@ TRJ_API int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const int3
  * n_max: largest frame the plan will accept. */
 TRJ_API int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
                         int64_t n_max, trj_rdf_plan** out);
+/* Plan with nbins bins of width r_max/nbins covering [0, r_max): bin k (1-based)
+ * holds r in [(k-1) dr, k dr), i.e. index floor(r/dr)+1, pairs counted for
+ * rr2 < r_max^2 (FP32).  This is the binning of the freud RDF used by the
+ * reference's tools/fast_grfreud_netcdf.py (bins on [0, r_max)); r_max must be
+ * below half the smallest box edge. */
+TRJ_API int trj_rdf_plan_create_floor(trj_ctx* ctx, int nsp, float r_max, int nbins, const float box[3],
+                                      int64_t n_max, trj_rdf_plan** out);
 /* lsmax, nit = nsp(nsp+1)/2, cells per axis (1 = no cell split on that axis),
  * effective cutoff, side2, device scratch bytes held by the plan. */
 TRJ_API int trj_rdf_plan_info(const trj_rdf_plan* plan, int* lsmax, int* nit, int cells[3],

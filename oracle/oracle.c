@@ -39,7 +39,12 @@ typedef struct {
     float deltar;
     int lsmax;
     int nsp;
+    int floor_bins;  /* 0: nint(r/deltar) as rdf_sh; 1: floor(r/deltar)+1 (bins [k dr, (k+1) dr)) */
 } orc_rdf_params;
+
+static int g_floor_bins = 0;  /* binning of the next orc_rdf_* call (set by orc_set_binning) */
+
+ORC_EXPORT void orc_set_binning(int floor_bins) { g_floor_bins = floor_bins; }
 
 /* ind_ij (rdf.cuf:741-753), 0-based species a,b -> 0-based pair row. */
 static inline int pair_row(int a, int b, int nsp) {
@@ -60,7 +65,7 @@ static inline int pair_outcome(float rr2, const orc_rdf_params* p) {
     if (!(rr2 < p->side2)) return 0;
     float rr = sqrtf(rr2);
     float q = rr / p->deltar;
-    int ind = (int)roundf(q);
+    int ind = p->floor_bins ? (int)floorf(q) + 1 : (int)roundf(q);
     if (ind <= p->lsmax && ind > 0) return ind;
     return 0;
 }
@@ -105,7 +110,7 @@ static inline void do_pair(const float* pi, int si, const float* pj, int sj,
 ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
                                  const float box[3], float side2, float deltar,
                                  int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
-    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp};
+    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp, g_floor_bins};
     int nit = nsp * (nsp + 1) / 2;
     int nthr = 1;
 #ifdef _OPENMP
@@ -187,7 +192,7 @@ ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t
         next[i] = head[c];
         head[c] = i;
     }
-    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp};
+    orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp, g_floor_bins};
     int nit = nsp * (nsp + 1) / 2;
     int nthr = 1;
 #ifdef _OPENMP

@@ -58,6 +58,8 @@ def lib():
             fn.restype = None
             fn.argtypes = [vp, i64, vp, i32, vp, i64, vp, vp]
         L.orc_num_threads.restype = i32
+        L.orc_set_binning.restype = None
+        L.orc_set_binning.argtypes = [i32]
         _lib = L
     return _lib
 
@@ -80,8 +82,9 @@ def layout(xyz: np.ndarray, species: np.ndarray, box, nsp: int):
 
 
 def rdf_counts(pos: np.ndarray, species: np.ndarray, box, side2: float, deltar: float, lsmax: int, nsp: int,
-               cells: bool = False):
-    """uint64 [nit][lsmax] pair counts and (edge_ulp, edge_fma, counted) of one frame."""
+               cells: bool = False, floor_bins: bool = False):
+    """uint64 [nit][lsmax] pair counts and (edge_ulp, edge_fma, counted) of one frame.
+    floor_bins: bin floor(r/deltar)+1 instead of the reference's nint(r/deltar)."""
     pos = np.ascontiguousarray(pos, F32)
     sp = np.ascontiguousarray(species, np.int32)
     nit = nsp * (nsp + 1) // 2
@@ -89,8 +92,12 @@ def rdf_counts(pos: np.ndarray, species: np.ndarray, box, side2: float, deltar: 
     edge = np.zeros(3, np.uint64)
     b = np.asarray(box, F32)
     fn = lib().orc_rdf_cells if cells else lib().orc_rdf_allpairs
-    fn(_p(pos), _p(sp), pos.shape[0], _p(b), float(F32(side2)), float(F32(deltar)), int(lsmax), int(nsp),
-       _p(hist), _p(edge))
+    lib().orc_set_binning(1 if floor_bins else 0)
+    try:
+        fn(_p(pos), _p(sp), pos.shape[0], _p(b), float(F32(side2)), float(F32(deltar)), int(lsmax), int(nsp),
+           _p(hist), _p(edge))
+    finally:
+        lib().orc_set_binning(0)
     return hist, edge
 
 

@@ -139,3 +139,58 @@ def test_synthetic_frames_shape_and_determinism():
     counts = np.bincount(a.types)[1:]
     assert list(counts) == [250, 150, 100]
     assert frames.c4_spec().n == 4000000
+
+
+def test_namelist_reader():
+    from trj_analysis_b200 import namelist
+    text = """&INPUT
+  trj_input_file='run.nc'   ! a comment
+  nsp=2
+  ncfs_from_to=1000 1 1000
+  rdf_sq_cl_dyn_sqw_conf_ord=T T F F F  F T
+  rcl=1.5
+/
+&INPUT_SP
+  sp_types_selected=3 1
+  mat=1.0 2.0
+/
+&INPUT_RDF
+  deltar=0.25
+  rcrdf=15.0
+/
+&INPUT_SQ
+  qmax=25.0
+  qmin=6.4
+  bsc=1.0 0.6d0
+/
+"""
+    g = namelist.parse(text)
+    assert g["INPUT"]["trj_input_file"] == "run.nc" and g["INPUT"]["nsp"] == 2
+    assert g["INPUT"]["rdf_sq_cl_dyn_sqw_conf_ord"] == [True, True, False, False, False, False, True]
+    cfg = namelist.config_from_namelist(g)
+    assert cfg.sp_types_selected == [3, 1] and cfg.deltar == 0.25 and cfg.rcrdf == 15.0
+    assert cfg.qmax == 25.0 and cfg.qmin == 6.4 and cfg.bsc == [1.0, 0.6]
+    assert namelist.parse("&A x=3*0 /\n")["A"]["x"] == [0, 0, 0]
+
+
+def test_netcdf_roundtrip(tmp_path):
+    spec = frames.FCCSpec(cells=(3, 3, 3), fractions=(0.5, 0.5), seed=5)
+    frs = [spec.frame(i) for i in range(3)]
+    p = str(tmp_path / "t.nc")
+    frames.write_netcdf_trajectory(p, frs)
+    got = list(frames.open_trajectory(p))
+    assert len(got) == 3
+    for a, b in zip(got, frs):
+        assert np.array_equal(a.xyz, b.xyz) and np.array_equal(a.types, b.types)
+        assert np.array_equal(a.box, b.box)
+
+
+def test_linear_kset_counts():
+    box = np.array([20.0, 20.0, 20.0], F32)
+    ks = refsem.linear_kset(box, 2 * np.pi / 20.0, 2.0, 10)
+    fk = 2 * np.pi / 20.0
+    m = 8
+    g = np.stack(np.meshgrid(*[np.arange(-m, m + 1)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    q = np.sqrt(((g * fk) ** 2).sum(1))
+    sel = (q >= fk) & (q < 2.0)
+    assert ks.nq.sum() == sel.sum()

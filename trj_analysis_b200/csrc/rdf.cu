@@ -37,6 +37,7 @@ struct RdfParams {
     float side2, side2_lo, side2_hi;
     float deltar, inv_deltar;
     int lsmax, nsp, nit;
+    int floor_bins;             // 0: bin nint(r/deltar) (reference); 1: bin floor(r/deltar)+1
     int nc[3];
     int ncell;
     int noff;
@@ -75,7 +76,7 @@ __device__ __forceinline__ int outcome(float rr2, const RdfParams& p) {
     if (!(rr2 < p.side2)) return 0;
     float rr = __fsqrt_rn(rr2);
     float q = __fdiv_rn(rr, p.deltar);
-    int ind = (int)roundf(q);
+    int ind = p.floor_bins ? (int)floorf(q) + 1 : (int)roundf(q);
     return (ind <= p.lsmax && ind > 0) ? ind : 0;
 }
 
@@ -175,11 +176,13 @@ __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz
     const float q = rr2 * rsqrtf(rr2) * p.inv_deltar;
     const float fq = q - floorf(q);
     const float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
+    // distance of q from the nearest bin edge: half-integers (nint bins) or integers (floor bins)
+    const float edge = p.floor_bins ? fminf(fq, 1.0f - fq) : fabsf(fq - 0.5f);
     int ind;
-    if (rr2 >= p.side2_lo || !(fabsf(fq - 0.5f) > win)) {  // NaN (rr2 == 0) takes this path too
+    if (rr2 >= p.side2_lo || !(edge > win)) {  // NaN (rr2 == 0) takes this path too
         ind = exact_bin(rr2, x2, dy, dz, p, pc);
     } else {
-        ind = __float2int_rn(q);
+        ind = p.floor_bins ? (int)floorf(q) + 1 : __float2int_rn(q);
         if (ind > p.lsmax) ind = 0;
     }
     if (ind > 0) atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
@@ -389,6 +392,7 @@ __global__ void scan_exclusive_kernel(const int32_t* __restrict__ in, int32_t* _
 struct trj_rdf_plan {
     trj_ctx* ctx = nullptr;
     int nsp = 0, nit = 0, lsmax = 0;
+    int floor_bins = 0;
     float deltar = 0.f, rcrdf_eff = 0.f, side2 = 0.f;
     int64_t n_max = 0;
     int ncell_cap = 0;
@@ -478,6 +482,27 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     return TRJ_OK;
 }
 
+extern "C" int trj_rdf_plan_create_floor(trj_ctx* ctx, int nsp, float r_max, int nbins, const float box[3],
+                                         int64_t n_max, trj_rdf_plan** out) {
+    if (!ctx || !out || !box) return TRJ_ERR_INVALID;
+    *out = nullptr;
+    if (nbins < 1 || !(r_max > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan (floor bins): nbins=%d r_max=%g", nbins, (double)r_max);
+    const float side = fminf(box[0], fminf(box[1], box[2]));
+    if (!(r_max < side / 2.0f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan (floor bins): r_max=%g must be below half the box (%g)",
+                        (double)r_max, (double)(side / 2.0f));
+    const float deltar = r_max / (float)nbins;
+    int rc = trj_rdf_plan_create(ctx, nsp, deltar, r_max, box, n_max, out);
+    if (rc != TRJ_OK) return rc;
+    trj_rdf_plan* p = *out;
+    p->floor_bins = 1;
+    p->lsmax = nbins;
+    p->rcrdf_eff = r_max;
+    p->side2 = r_max * r_max;
+    return TRJ_OK;
+}
+
 extern "C" int trj_rdf_plan_info(const trj_rdf_plan* p, int* lsmax, int* nit, int cells[3], float* rcrdf_eff,
                                  float* side2, int64_t* scratch_bytes) {
     if (!p) return TRJ_ERR_INVALID;
@@ -540,6 +565,7 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
     P.deltar = plan->deltar;
     P.inv_deltar = 1.0f / plan->deltar;
     P.lsmax = plan->lsmax;
+    P.floor_bins = plan->floor_bins;
     P.nsp = plan->nsp;
     P.nit = plan->nit;
     cells_for(box, plan->side2, P.nc);

@@ -74,11 +74,19 @@ def pack_frame(ctx: Context, xyz: torch.Tensor, species: torch.Tensor, nsp: int,
 
 
 class RdfPlan:
-    def __init__(self, ctx: Context, nsp: int, deltar: float, rcrdf: float, box, n_max: int):
+    """g_ab(r) plan.  Reference bins (nint(r/deltar), rcrdf clipped to half the box) by default;
+    ``floor_bins=nbins`` gives nbins bins [k dr, (k+1) dr) on [0, rcrdf) instead."""
+
+    def __init__(self, ctx: Context, nsp: int, deltar: float, rcrdf: float, box, n_max: int,
+                 floor_bins: Optional[int] = None):
         self.ctx = ctx
         h = vp()
-        rc = ctx.lib.trj_rdf_plan_create(ctx.h, nsp, float(deltar), float(rcrdf), box3(box), int(n_max),
-                                         ctypes.byref(h))
+        if floor_bins:
+            rc = ctx.lib.trj_rdf_plan_create_floor(ctx.h, nsp, float(rcrdf), int(floor_bins), box3(box), int(n_max),
+                                                   ctypes.byref(h))
+        else:
+            rc = ctx.lib.trj_rdf_plan_create(ctx.h, nsp, float(deltar), float(rcrdf), box3(box), int(n_max),
+                                             ctypes.byref(h))
         check(rc, ctx.h, "trj_rdf_plan_create")
         self.h = h
         self.nsp = nsp

@@ -190,3 +190,25 @@ def write_npz_trajectory(path: str, frames: Sequence[Frame]) -> None:
     np.savez(path, coordinates=np.stack([f.xyz for f in frames]),
              cell_lengths=np.stack([f.box for f in frames]),
              type=np.stack([f.types for f in frames]))
+
+
+def write_netcdf_trajectory(path: str, frames: Sequence[Frame]) -> None:
+    """Classic NetCDF (CDF-2) file with the AMBER-convention variables the reference reads:
+    coordinates (frame, atom, spatial), cell_lengths (frame, cell_spatial), type (frame, atom)."""
+    from scipy.io import netcdf_file
+    nf = len(frames)
+    n = frames[0].n
+    with netcdf_file(path, "w", version=2) as nc:
+        nc.Conventions = b"AMBER"
+        nc.ConventionVersion = b"1.0"
+        nc.createDimension("frame", nf)
+        nc.createDimension("atom", n)
+        nc.createDimension("spatial", 3)
+        nc.createDimension("cell_spatial", 3)
+        c = nc.createVariable("coordinates", "f4", ("frame", "atom", "spatial"))
+        L = nc.createVariable("cell_lengths", "f4", ("frame", "cell_spatial"))
+        t = nc.createVariable("type", "i4", ("frame", "atom"))
+        for k, f in enumerate(frames):
+            c[k] = f.xyz
+            L[k] = f.box
+            t[k] = f.types

@@ -402,3 +402,27 @@ def make_kset(mode: str, box, qmax: float, qmin: Optional[float] = None, seed: i
     if mode == "full+sampled":
         return full_kset(box, qmax, qmin, above="sampled", per_shell=per_shell, seed=seed)
     raise ValueError(f"unknown k-set mode {mode!r}")
+
+
+def linear_kset(box, k_min: float, k_max: float, nbins: int) -> KSet:
+    """Every lattice vector with k_min <= |k| < k_max in nbins linear bins of (k_max-k_min)/nbins.
+
+    The binning of the freud StaticStructureFactorDirect used by the reference's
+    tools/fast_sq_freud_netcdf.py (bins=60, k_min=2 pi / max(L), k_max=0.5).  Vectors are
+    evaluated as +-k pairs (weight 2); nq[b] = number of vectors in bin b.  ``dq`` holds the
+    bin width and the bin centres are k_min + (b + 1/2) dq.
+    """
+    box = np.asarray(box, F32)
+    sph = _sphere(box, k_max, strict=True)
+    fk = 2.0 * np.pi / np.asarray(box, np.float64)
+    q = np.sqrt(((sph * fk[None, :]) ** 2).sum(axis=1))
+    keep = (q >= k_min) & _half_space(sph)
+    v = sph[keep]
+    dk = (k_max - k_min) / nbins
+    b = np.floor((q[keep] - k_min) / dk).astype(np.int64)
+    b = np.clip(b, 0, nbins - 1)
+    w = np.full(v.shape[0], 2.0)
+    nq = np.zeros(nbins, np.int64)
+    np.add.at(nq, b, 2)
+    return KSet(mode="linear", dq=float(dk), nqmax=nbins - 1, vectors=v.astype(np.int32), bins=b.astype(np.int32),
+                weights=w, dense=np.zeros(v.shape[0], np.uint8), nq=nq, qmin_eff=float(k_min))
