@@ -14,11 +14,14 @@
  * globals (CUDA Fortran, src/modules/rdf.cuf and src/modules/sq.cuf).  Each
  * entry point below names the reference routine whose role it takes.
  * Threading: a context and its plans may be used from one host thread at a
- * time; use one context per thread, or distinct streams.
+ * time (use one context per thread).  Work of one context may run on several
+ * streams at once: frame-layout scratch is kept per stream, plans own theirs
+ * (one plan must not run on two streams at the same time).
  */
 #ifndef TRJ_SM100_H
 #define TRJ_SM100_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -71,6 +74,18 @@ TRJ_API const char* trj_ctx_last_error(const trj_ctx* ctx);
  * (TRJ_ERR_DATA / TRJ_ERR_TIMEOUT / TRJ_ERR_CAPACITY), then clear it. */
 TRJ_API int trj_ctx_check(trj_ctx* ctx, void* stream);
 TRJ_API int trj_ctx_sm_count(const trj_ctx* ctx);
+/* Device memory of plans and scratch.  By default the library calls cudaMalloc
+ * and cudaFree (and cudaFree synchronises the device).  A caller that owns
+ * device memory through its own allocator (for example a caching allocator, so
+ * that plans can be created and destroyed while other streams keep running)
+ * installs alloc/free callbacks here: alloc(bytes, user) returns a device
+ * pointer (256-byte aligned) or NULL; free(ptr, user) releases it.  Install
+ * them right after trj_ctx_create, before any plan exists; pass NULLs to return
+ * to cudaMalloc/cudaFree.  The callbacks are called from the thread that
+ * creates or destroys a plan. */
+typedef void* (*trj_alloc_fn)(size_t bytes, void* user);
+typedef void (*trj_free_fn)(void* ptr, void* user);
+TRJ_API int trj_ctx_set_allocator(trj_ctx* ctx, trj_alloc_fn alloc, trj_free_fn free_fn, void* user);
 /* Kernel timing: when enabled, each accumulate call records CUDA events on its
  * stream around the plan's main kernel (the cell-pair kernel, the tcgen05 S(Q)
  * kernel, or the direct-sum kernel); trj_*_kernel_ms reads the last duration
@@ -88,8 +103,9 @@ TRJ_API int64_t trj_ctx_launches(const trj_ctx* ctx);
  *   species_dev  n int32 species index 0..nsp-1 (device)
  *   packed_dev   n x 4 float out: x, y, z, species (int bits in w)
  *   counts_dev   nsp int64 out: atoms per species
- * The context keeps the per-block counting scratch; it grows (one cudaMalloc)
- * the first time a larger frame or species count is seen. */
+ * The context keeps the per-block counting scratch, one buffer per stream; it
+ * grows (one allocation) the first time a larger frame or species count is
+ * seen on that stream. */
 TRJ_API int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
                    int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
                    void* stream);

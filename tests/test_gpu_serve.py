@@ -1,0 +1,62 @@
+"""The request loop: isolation (same bits alone and in a mix), admission, graphs, parity."""
+import numpy as np
+import pytest
+
+from oracle import orc
+from trj_analysis_b200 import refsem
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def workload():
+    from trj_analysis_b200.serve import serving_workload
+    reqs = serving_workload(12, seed=7, n_lo=500, n_hi=6000)
+    return reqs
+
+
+def _run(reqs, **kw):
+    from trj_analysis_b200.serve import Server
+    srv = Server(slots=kw.pop("slots", 6), n_max=1 << 14, **kw)
+    res = srv.run(reqs, realtime=False)
+    return srv, {r.rid: r for r in res}
+
+
+def test_results_identical_alone_and_in_mix(workload):
+    _, mixed = _run(workload, method="split")
+    assert len(mixed) == len(workload)
+    for req in workload[:6]:
+        _, alone = _run([req], slots=1, method="split")
+        a, b = alone[req.rid], mixed[req.rid]
+        assert np.array_equal(a.hist, b.hist)
+        assert np.array_equal(a.sq_sums, b.sq_sums)
+
+
+def test_graph_replay_matches_eager(workload):
+    multi = [r for r in workload if len(r.frames) >= 4][:3]
+    assert multi
+    _, g = _run(multi, method="plain", use_graphs=True)
+    _, e = _run(multi, method="plain", use_graphs=False)
+    for r in multi:
+        assert np.array_equal(g[r.rid].hist, e[r.rid].hist)
+        assert np.array_equal(g[r.rid].sq_sums, e[r.rid].sq_sums)
+
+
+def test_admission_under_small_budget(workload):
+    srv, res = _run(workload, hbm_budget=1)
+    assert len(res) == len(workload)
+    assert srv.admission_waits > 0
+
+
+def test_served_counts_match_oracle(workload):
+    _, res = _run(workload[:4], method="split")
+    for req in workload[:4]:
+        H = 0
+        sel = sorted(set(int(t) for t in np.unique(req.frames[0].types)))[: req.nsp]
+        sp = refsem.species_by_first_appearance(req.frames[0].types, sel)[0]
+        p = refsem.rdf_params(req.nsp, req.deltar, req.rcrdf, req.frames[0].box)
+        for fr in req.frames:
+            pos, sps, off = orc.layout(fr.xyz, sp, fr.box, req.nsp)
+            h, _ = orc.rdf_counts(pos, sps, fr.box, p.side2, p.deltar, p.lsmax, req.nsp, cells=True)
+            H = H + h
+        assert np.array_equal(res[req.rid].hist, H)

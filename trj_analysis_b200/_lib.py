@@ -44,6 +44,7 @@ SIGNATURES = {
     "trj_ctx_check": (c_int, [vp, vp]),
     "trj_ctx_sm_count": (c_int, [vp]),
     "trj_ctx_set_timing": (c_int, [vp, c_int]),
+    "trj_ctx_set_allocator": (c_int, [vp, vp, vp, vp]),
     "trj_ctx_launches": (c_int64, [vp]),
     "trj_rdf_kernel_ms": (c_int, [vp, P(c_float)]),
     "trj_sq_kernel_ms": (c_int, [vp, P(c_float)]),

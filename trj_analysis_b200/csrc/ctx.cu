@@ -65,7 +65,8 @@ extern "C" int trj_ctx_destroy(trj_ctx* ctx) {
         trj_device_guard g(ctx->device);
         if (ctx->status_dev) cudaFree(ctx->status_dev);
         if (ctx->status_host) cudaFreeHost(ctx->status_host);
-        if (ctx->pack_scratch) cudaFree(ctx->pack_scratch);
+        for (auto& kv : ctx->pack_scratch) trj_dev_free(ctx, kv.second.ptr);
+        ctx->pack_scratch.clear();
     }
     delete ctx;
     return TRJ_OK;
@@ -76,6 +77,18 @@ extern "C" const char* trj_ctx_last_error(const trj_ctx* ctx) {
 }
 
 extern "C" int trj_ctx_sm_count(const trj_ctx* ctx) { return ctx ? ctx->sm_count : 0; }
+
+extern "C" int trj_ctx_set_allocator(trj_ctx* ctx, trj_alloc_fn alloc, trj_free_fn free_fn, void* user) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    if ((alloc == nullptr) != (free_fn == nullptr))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_ctx_set_allocator: give both callbacks or neither");
+    for (auto& kv : ctx->pack_scratch) trj_dev_free(ctx, kv.second.ptr);  // with the allocator that made it
+    ctx->pack_scratch.clear();
+    ctx->alloc = alloc;
+    ctx->free_fn = free_fn;
+    ctx->alloc_user = user;
+    return TRJ_OK;
+}
 
 extern "C" int64_t trj_ctx_launches(const trj_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
@@ -262,15 +275,19 @@ extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t*
     }
     if (nblocks > (int64_t)INT32_MAX) return trj_fail(ctx, TRJ_ERR_INVALID, "frame too large");
     size_t need = (size_t)nblocks * nsp * (sizeof(int32_t) + sizeof(int64_t)) + 256;
-    if (need > ctx->pack_scratch_bytes) {
-        if (ctx->pack_scratch) cudaFree(ctx->pack_scratch);
-        ctx->pack_scratch = nullptr;
-        ctx->pack_scratch_bytes = 0;
-        if (cudaMalloc(&ctx->pack_scratch, need) != cudaSuccess)
+    trj_ctx::PackScratch& ps = ctx->pack_scratch[stream];
+    if (need > ps.bytes) {
+        // Earlier work of this stream may still read the old buffer; cudaFree waits for it, and a
+        // caller allocator receives the release from the thread that issued that work.
+        if (ps.ptr && !ctx->alloc) TRJ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        trj_dev_free(ctx, ps.ptr);
+        ps.ptr = nullptr;
+        ps.bytes = 0;
+        if (trj_dev_alloc(ctx, &ps.ptr, need) != cudaSuccess)
             return trj_fail(ctx, TRJ_ERR_NOMEM, "trj_frame_pack: scratch of %zu bytes", need);
-        ctx->pack_scratch_bytes = need;
+        ps.bytes = need;
     }
-    int64_t* block_base = (int64_t*)ctx->pack_scratch;
+    int64_t* block_base = (int64_t*)ps.ptr;
     int32_t* block_counts = (int32_t*)(block_base + nblocks * nsp);
     pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp,
                                                                  block_counts, ctx->status_dev);

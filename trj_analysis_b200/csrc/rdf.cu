@@ -465,7 +465,7 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     size_t bytes = 64 + sizeof(int32_t) * (size_t)(3 * p->ncell_cap + 1) +
                    (sizeof(int32_t) * 2 + sizeof(float4)) * (size_t)std::max<int64_t>(n_max, 1);
     char* base = nullptr;
-    if (cudaMalloc(&base, bytes + 256) != cudaSuccess) {
+    if (trj_dev_alloc(ctx, (void**)&base, bytes + 256) != cudaSuccess) {
         delete p;
         return trj_fail(ctx, TRJ_ERR_NOMEM, "rdf plan: %zu bytes of scratch", bytes);
     }
@@ -524,7 +524,7 @@ extern "C" int trj_rdf_plan_destroy(trj_rdf_plan* p) {
     if (!p) return TRJ_OK;
     {
         trj_device_guard g(p->ctx->device);
-        if (p->sorted) cudaFree(p->sorted);
+        trj_dev_free(p->ctx, p->sorted);
         p->timer.release();
     }
     delete p;

@@ -201,8 +201,7 @@ static void sq_plan_free(trj_sq_plan* p) {
     void* ptrs[] = {p->vec_dev, p->weight_dev, p->bin_start_dev, p->species_off_dev, p->plain_all_dev,
                     p->plain_sparse_dev, p->tiles_dev, p->dense_src_dev, p->phase_dev, p->part_dev,
                     p->tc_out_dev, p->rho_dev};
-    for (void* q : ptrs)
-        if (q) cudaFree(q);
+    for (void* q : ptrs) trj_dev_free(p->ctx, q);
     trj_sq_tc_release(p);
     p->timer.release();
 }
@@ -217,7 +216,8 @@ extern "C" int trj_sq_plan_destroy(trj_sq_plan* p) {
 template <class T>
 static int dev_upload(trj_ctx* ctx, T** dst, const T* src, size_t count, int64_t* acct) {
     size_t bytes = std::max<size_t>(1, count) * sizeof(T);
-    if (cudaMalloc(dst, bytes) != cudaSuccess) return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: %zu bytes", bytes);
+    if (trj_dev_alloc(ctx, (void**)dst, bytes) != cudaSuccess)
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: %zu bytes", bytes);
     *acct += (int64_t)bytes;
     if (count && src && cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
         return trj_fail(ctx, TRJ_ERR_CUDA, "sq plan: upload failed");
@@ -363,7 +363,7 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
             return rc;
         }
         size_t tb = sizeof(double) * (size_t)p->tc_out_doubles;
-        if (cudaMalloc(&p->tc_out_dev, tb) != cudaSuccess) {
+        if (trj_dev_alloc(ctx, (void**)&p->tc_out_dev, tb) != cudaSuccess) {
             sq_plan_free(p);
             delete p;
             return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: tensor output %zu bytes", tb);
@@ -376,8 +376,9 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     size_t part_b = sizeof(double2) * (size_t)std::max(p->nsplit_all, p->nsplit_sparse) * nsp *
                     (size_t)std::max<int64_t>(1, nvec);
     size_t rho_b = sizeof(double2) * (size_t)nsp * (size_t)std::max<int64_t>(1, nvec);
-    if (cudaMalloc(&p->phase_dev, phase_b) != cudaSuccess || cudaMalloc(&p->part_dev, part_b) != cudaSuccess ||
-        cudaMalloc(&p->rho_dev, rho_b) != cudaSuccess) {
+    if (trj_dev_alloc(ctx, (void**)&p->phase_dev, phase_b) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&p->part_dev, part_b) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&p->rho_dev, rho_b) != cudaSuccess) {
         sq_plan_free(p);
         delete p;
         return trj_fail(ctx, TRJ_ERR_NOMEM, "sq plan: scratch allocation failed");

@@ -576,8 +576,7 @@ void trj_sq_tc_release(trj_sq_plan* plan) {
     if (!st) return;
     void* ptrs[] = {st->sched_dev, st->tiles_dev, st->groups_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
                     st->tab_hi, st->tab_lo, st->tab_x, st->tab_y, st->part};
-    for (void* q : ptrs)
-        if (q) cudaFree(q);
+    for (void* q : ptrs) trj_dev_free(plan->ctx, q);
     delete st;
     plan->tc_state = nullptr;
 }
@@ -709,15 +708,15 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     size_t y_bytes = sizeof(float2) * (size_t)st->total_slots * st->nyr;
     size_t part_bytes = sizeof(double) * (size_t)st->acc_stride * st->chunks.size();
     std::vector<int32_t> cb(st->chunk_of_species_begin.begin(), st->chunk_of_species_begin.end());
-    if (cudaMalloc(&st->tab_hi, tab_bytes) != cudaSuccess || cudaMalloc(&st->tab_lo, tab_bytes) != cudaSuccess ||
-        cudaMalloc(&st->tab_x, x_bytes) != cudaSuccess || cudaMalloc(&st->tab_y, y_bytes) != cudaSuccess ||
-        cudaMalloc(&st->part, part_bytes) != cudaSuccess ||
-        cudaMalloc(&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
-        cudaMalloc(&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
-        cudaMalloc(&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
-        cudaMalloc(&st->pad_off_dev, sizeof(int64_t) * (nsp + 1)) != cudaSuccess ||
-        cudaMalloc(&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
-        cudaMalloc(&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
+    if (trj_dev_alloc(ctx, (void**)&st->tab_hi, tab_bytes) != cudaSuccess || trj_dev_alloc(ctx, (void**)&st->tab_lo, tab_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->tab_x, x_bytes) != cudaSuccess || trj_dev_alloc(ctx, (void**)&st->tab_y, y_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->part, part_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->pad_off_dev, sizeof(int64_t) * (nsp + 1)) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
         return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
                         2 * tab_bytes + x_bytes + y_bytes + part_bytes);
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
@@ -774,6 +773,9 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.stage_bytes = st->stage_bytes;
     P.tpc = st->tpc;
     P.status = ctx->status_dev;
+    // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
+    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           st->smem_bytes));
     plan->timer.begin(ctx, s);
     sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_x, st->map_y, P);
     plan->timer.end(ctx, s);

@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <string>
+#include <unordered_map>
 
 #include "../../include/trj_sm100.h"
 
@@ -23,10 +24,18 @@ struct trj_ctx {
     size_t smem_optin = 0;
     unsigned* status_dev = nullptr;     // [0] status bits, [1..7] diagnostics
     unsigned* status_host = nullptr;    // pinned mirror
-    void* pack_scratch = nullptr;       // per-block species counts of trj_frame_pack
-    size_t pack_scratch_bytes = 0;
+    struct PackScratch {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+    };
+    // per-block species counts of trj_frame_pack, one buffer per stream so that packs on
+    // different streams never share scratch
+    std::unordered_map<void*, PackScratch> pack_scratch;
     bool timing = false;
     long long launches = 0;             // kernels this library launched on the context
+    trj_alloc_fn alloc = nullptr;       // caller-provided device allocator (NULL: cudaMalloc)
+    trj_free_fn free_fn = nullptr;
+    void* alloc_user = nullptr;
     std::string last_error;
 };
 
@@ -54,6 +63,20 @@ struct trj_kernel_timer {
         start = stop = nullptr;
     }
 };
+
+// Device allocation through the context's allocator (cudaMalloc/cudaFree unless one is installed).
+inline cudaError_t trj_dev_alloc(trj_ctx* ctx, void** p, size_t bytes) {
+    if (ctx->alloc) {
+        *p = ctx->alloc(bytes, ctx->alloc_user);
+        return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+inline void trj_dev_free(trj_ctx* ctx, void* p) {
+    if (!p) return;
+    if (ctx->alloc) ctx->free_fn(p, ctx->alloc_user);
+    else cudaFree(p);
+}
 
 // Records an error message on the context and returns the status code.
 int trj_fail(trj_ctx* ctx, int code, const char* fmt, ...);
