@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-FP32 comparison pass")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--serving", type=int, default=200, help="requests in the serving run (0: skip)")
     return ap.parse_args()
 
 
@@ -311,6 +312,44 @@ def run_ours(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
+# serving: continuous batching vs offline vs the plain per-request path
+# ---------------------------------------------------------------------------
+
+def run_serving(n_req, seed=5):
+    import copy
+    from trj_analysis_b200.serve import Server, serving_workload, summarize
+    reqs = serving_workload(n_req, seed=seed)
+
+    def timed(srv, rq, realtime):
+        t0 = time.perf_counter()
+        res = srv.run(rq, realtime=realtime)
+        return summarize(res, time.perf_counter() - t0)
+
+    srv = Server(slots=8)
+    timed(srv, copy.copy(reqs)[: max(8, n_req // 4)], False)          # tunes the buckets, warms caches
+    offline = timed(srv, copy.copy(reqs), False)
+    rng = np.random.default_rng(seed + 1)
+    rate = 0.8 * offline["requests_per_s"]
+    t = 0.0
+    online_reqs = []
+    for r in reqs:
+        t += rng.exponential(1.0 / rate)
+        q = copy.copy(r)
+        q.arrival = t
+        online_reqs.append(q)
+    online = timed(srv, online_reqs, True)
+    base_srv = Server(slots=1, use_graphs=False, method="plain")
+    baseline = timed(base_srv, copy.copy(reqs), False)
+    return {"workload": f"{n_req} requests, N log-uniform [1e3, 2e5], 1-3 species, cubic or 1:1:2, 1-8 frames, "
+                        "deltar 0.02, rcrdf min(L/2, 8), S(Q) reference k-set qmax 12 qmin 3; Poisson arrivals at "
+                        "80% of the offline request rate",
+            "offline": offline, "online": online, "per_request_plain_path": baseline,
+            "online_vs_offline_throughput": online["frames_per_s"] / offline["frames_per_s"],
+            "offline_vs_plain_path": offline["frames_per_s"] / baseline["frames_per_s"],
+            "peak_hbm_in_use_bytes": srv.peak_in_use, "admission_waits": srv.admission_waits}
+
+
+# ---------------------------------------------------------------------------
 # CPU restatement (reference algorithm on host cores)
 # ---------------------------------------------------------------------------
 
@@ -395,6 +434,8 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", local_rank))
     res, (spec, fr, wl, ks) = run_ours(args, rank, world, local_rank)
+    if rank == 0 and args.serving > 0:
+        res["serving"] = run_serving(args.serving)
     if rank == 0 and not args.no_cpu:
         t, sample, cores = cpu_frame_estimate(wl, fr[0], ks, args.cpu_seconds)
         res["cpu_baseline"] = {"value": 1.0 / t, "unit": "frames/s", "cores": cores, "kind": "port",

@@ -172,6 +172,12 @@ TRJ_API int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int32_
  * device scratch bytes held by the plan. */
 TRJ_API int trj_sq_plan_info(const trj_sq_plan* plan, int64_t* n_dense, int64_t* n_tiles,
                      int64_t* tile_slots, int64_t* scratch_bytes);
+/* Tensor-core tuning: atoms accumulated by the tensor cores in one FP32 run before
+ * the run is added (round-to-nearest) into the running sum, rounded down to a
+ * multiple of 32 (>= 32).  The tensor-core accumulation error grows linearly with
+ * the run length, so longer runs trade accuracy for fewer drains; the default,
+ * 256 atoms, keeps the per-shell error of an N = 1e6 frame below 1e-5. */
+TRJ_API int trj_sq_plan_set_flush(trj_sq_plan* plan, int atoms);
 /* Replaces SQcalc (src/modules/sq.cuf:58-126; kernels sqfnD 523-591, sqfact
  * 372-454): adds, for every bin and species pair (a<=b, row ind_ij(a,b)-1),
  * sum over the bin's vectors of weight * Re(rho_a(k) conj(rho_b(k))) to

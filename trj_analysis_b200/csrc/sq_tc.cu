@@ -8,8 +8,11 @@
 //   K index 2j = Re, 2j+1 = Im of atom j;  B columns 2t (Re out) = (zr, -zi), 2t+1 (Im out) = (zi, zr).
 // Each factor v is split v = hi + lo with hi = bf16(v), lo = bf16(v - hi); the product keeps
 // hi*hi + hi*lo + lo*hi (three tcgen05.mma kind::f16 per K-step into one FP32 TMEM accumulator).
-// Every F stages (F*32 atoms) the accumulator is drained and added into an FP64 block, and the
-// blocks of one species are summed in FP64 in a fixed order.
+// The tensor core's FP32 accumulation is biased (the error of a run grows linearly with its
+// length), so every F stages (F*32 atoms, 256 by default) the accumulator is drained: the
+// epilogue warps add it with round-to-nearest CUDA-core adds into an FP32 running sum kept in
+// TMEM, and the last drain of a work item stores that sum once, in FP64, to global memory.
+// The blocks of one species are then summed in FP64 in a fixed order.
 //
 // Phases: every coordinate is the 32-bit fixed-point fraction u = (x/L mod 1) 2^32 (from FP64);
 // n*u mod 2^32 in integer arithmetic is exact, and sincospif of the reduced fraction gives each
@@ -19,9 +22,10 @@
 // Work item = (group of up to two tiles that share their nz range, chunk of one species' atoms);
 // the B tile is loaded once per stage for both tiles.  Persistent CTAs walk the items chunk-major
 // so that concurrently running CTAs stream the same atoms (L2 reuse of the tables).
-// Roles per CTA (448 threads): warps 0-7 build the A tiles (X*Y products, split, 128-byte swizzle);
-// warps 8-11 drain the TMEM accumulators (double-buffered) into FP64; warp 12 issues the TMA loads;
-// warp 13 allocates TMEM and one of its lanes issues the MMAs.  Every mbarrier wait is bounded and
+// Roles per CTA (704 threads): warps 0-15 build the A tiles (X*Y products, split, 128-byte swizzle;
+// 4 threads per A row for a single tile, 2 per row for a pair of tiles); warps 16-19 drain the TMEM
+// accumulator into the running sum; warp 20 issues the TMA loads; warp 21 allocates TMEM and one
+// of its lanes issues the MMAs.  Every mbarrier wait is bounded and
 // raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -33,12 +37,12 @@
 
 namespace {
 
-constexpr int kProducerWarps = 8;
+constexpr int kProducerWarps = 16;
 constexpr int kProducers = kProducerWarps * 32;
 constexpr int kEpiWarps = 4;
-constexpr int kTmaWarp = kProducerWarps + kEpiWarps;  // 12
+constexpr int kTmaWarp = kProducerWarps + kEpiWarps;  // 20
 constexpr int kMmaWarp = kTmaWarp + 1;                // 13
-constexpr int kTcThreads = (kMmaWarp + 1) * 32;       // 448
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;       // 704
 constexpr int kStageSlots = 32;            // atoms per stage: K = 64 bf16 = one 128-byte swizzle row
 constexpr int kATile = 128 * 128;          // bytes of one 128 x 64 bf16 operand tile
 constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // 32 atoms x 16 complex FP32
@@ -99,7 +103,7 @@ struct TcState {
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_x, map_y;
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, max_cols = 0, tpc = 2;
-    int flush_stages = 16;
+    int flush_stages = 8;   // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
 };
 
@@ -167,15 +171,28 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+// tcgen05.ld without the wait, so that several loads are in flight before one tmem_wait_ld.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
@@ -202,14 +219,21 @@ __device__ __forceinline__ bool timed_wait(uint64_t* bar, unsigned parity, unsig
 }
 
 // ---- per-frame tables --------------------------------------------------------
-// slot -> atom of the species-padded layout; padding slots carry zero factors.
+// slot -> atom of the species-padded layout; padding slots carry zero factors.  Within a species
+// the slots visit the atoms in the order local * mul[a] mod n_a (mul coprime with n_a, near the
+// golden ratio of n_a; mul = pad_off + nsp + 1): packed frames are cell-sorted, so consecutive atoms
+// are close in space and, at small k, their phase factors nearly equal.  Scattered, a run of slots
+// samples the whole box and its partial sums stay small, which keeps the FP32 accumulation error of
+// the tensor cores and of the running sums small compared with rho.
 __device__ __forceinline__ bool slot_atom(int64_t slot, const int64_t* pad_off, const int64_t* sp_off, int nsp,
                                           int64_t& atom) {
     int a = 0;
     while (a + 1 < nsp && slot >= pad_off[a + 1]) ++a;
-    int64_t local = slot - pad_off[a];
-    atom = sp_off[a] + local;
-    return local < sp_off[a + 1] - sp_off[a];
+    const int64_t local = slot - pad_off[a];
+    const int64_t na = sp_off[a + 1] - sp_off[a];
+    if (local >= na) return false;
+    atom = sp_off[a] + (int64_t)(((uint64_t)local * (uint64_t)pad_off[nsp + 1 + a]) % (uint64_t)na);  // < 2^62
+    return true;
 }
 
 // Z factors split into the B operand rows (row 2t: (zr, -zi), row 2t+1: (zi, zr) along K).
@@ -261,13 +285,41 @@ __global__ void tc_xytable_kernel(const uint4* __restrict__ phase, const int64_t
 
 // ---- the contraction kernel ------------------------------------------------
 
+// CPT 16-byte K-chunks (4 atoms each, starting at chunk c0) of A row m = (nx, ny) = (m % 16, m / 16):
+// A = X[nx] * Y[ny] per atom, split hi/lo, written into the 128-byte-swizzled hi tile at ahi and
+// the lo tile kATile bytes after it.
+template <int CPT>
+__device__ __forceinline__ void build_a_rows(uint8_t* ahi, const uint8_t* xy, int m, int c0) {
+    const float2* X = reinterpret_cast<const float2*>(xy);
+    const float2* Y = reinterpret_cast<const float2*>(xy + kXBytes);
+    const int nxl = m & 15, nyl = m >> 4;
+    const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
+#pragma unroll
+    for (int cc = 0; cc < CPT; ++cc) {
+        const int c = c0 + cc;
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = c * 4 + q;
+            const float2 x = X[j * kTcTileNx + nxl];
+            const float2 y = Y[j * kTcTileNy + nyl];
+            const float ar = x.x * y.x - x.y * y.y;
+            const float ai = x.x * y.y + x.y * y.x;
+            split2(ar, ai, hw[q], lw[q]);
+        }
+        const uint32_t off = rowoff + (uint32_t)((c ^ (m & 7)) << 4);
+        *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(ahi + kATile + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
     sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
                  const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_y, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_tma[kMaxStages], full_a[kMaxStages], empty[kMaxStages];
-    __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2];
+    __shared__ __align__(8) uint64_t acc_full, acc_empty;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -288,10 +340,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             trj_mbar_init(&full_a[s], kProducerWarps);
             trj_mbar_init(&empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            trj_mbar_init(&acc_full[b], 1);
-            trj_mbar_init(&acc_empty[b], kEpiWarps);
-        }
+        trj_mbar_init(&acc_full, 1);
+        trj_mbar_init(&acc_empty, kEpiWarps);
         trj_fence_mbar_init();
     }
     if (warp == kMmaWarp) {
@@ -305,10 +355,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    // accumulator column of (tile slot i, buffer b)
-    auto acc_col = [&](int i, int b) -> uint32_t {
-        return p.tpc == 2 ? (uint32_t)((2 * i + b) * 128) : (uint32_t)(b * 256);
-    };
+    // TMEM columns of tile slot i: FP32 accumulator (written by the MMAs) and FP32 running sum.
+    auto acc_col = [&](int i) -> uint32_t { return p.tpc == 2 ? (uint32_t)(i * 256) : 0u; };
+    auto sum_col = [&](int i) -> uint32_t { return p.tpc == 2 ? (uint32_t)(i * 256 + 128) : 256u; };
 
     if (warp == kTmaWarp) {
         if (lane == 0) {
@@ -350,15 +399,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else if (warp == kMmaWarp) {
         if (lane == 0) {
-            // Descriptors of every stage slot, built once; a K-step of 16 bf16 (32 bytes) adds 2
-            // to the start-address field, the lo operand of A sits kATile bytes after the hi one.
-            uint64_t adesc[kMaxStages][2], bdesc[kMaxStages];
-            for (int sl = 0; sl < NS; ++sl) {
-                const uint32_t base = trj_smem_addr(stage_ptr(sl));
-                adesc[sl][0] = sw128_desc(base);
-                adesc[sl][1] = sw128_desc(base + 2 * kATile);
-                bdesc[sl] = sw128_desc(base + a_bytes);
-            }
+            // Descriptors of stage slot 0; slot k sits k * stage_bytes further (the start-address field
+            // holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds without
+            // carry).  A K-step of 16 bf16 (32 bytes) adds 2; the lo operand of A sits kATile bytes after
+            // the hi one.
+            const uint32_t base0 = trj_smem_addr(stage_ptr(0));
+            const uint64_t a0desc = sw128_desc(base0), a1desc = sw128_desc(base0 + 2 * kATile);
+            const uint64_t b0desc = sw128_desc(base0 + a_bytes);
             const uint64_t a_lo = (uint64_t)(kATile >> 4), b_lo = (uint64_t)((bmax * 128) >> 4);
             int sg = 0, fg = 0;
             for (int li = item0; li < item1 && !abort_flag; ++li) {
@@ -377,8 +424,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const int slot = sg % NS;
                     const unsigned par = (sg / NS) & 1;
                     const bool first = (s % F) == 0;
-                    const int b = fg & 1;
-                    if (first && fg >= 2 && !timed_wait(&acc_empty[b], ((fg >> 1) - 1) & 1, p.status)) {
+                    // the epilogue must have read the previous run out of the accumulator
+                    if (first && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
@@ -387,10 +434,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t bh = bdesc[slot], bl = bh + b_lo;
-                    const uint32_t d0 = tmem + acc_col(0, b), d1 = tmem + acc_col(1, b);
-                    const uint64_t a0h = adesc[slot][0], a0l = a0h + a_lo;
-                    const uint64_t a1h = adesc[slot][1], a1l = a1h + a_lo;
+                    const uint64_t so = (uint64_t)(((uint32_t)slot * (uint32_t)p.stage_bytes) >> 4);
+                    const uint64_t bh = b0desc + so, bl = bh + b_lo;
+                    const uint32_t d0 = tmem + acc_col(0), d1 = tmem + acc_col(1);
+                    const uint64_t a0h = a0desc + so, a0l = a0h + a_lo;
+                    const uint64_t a1h = a1desc + so, a1l = a1h + a_lo;
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) {
                         const uint64_t o = 2 * kk;
@@ -405,16 +453,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     }
                     mma_commit(&empty[slot]);
                     if ((s + 1) % F == 0 || s == nst - 1) {
-                        mma_commit(&acc_full[b]);
+                        mma_commit(&acc_full);
                         ++fg;
                     }
                 }
             }
         }
     } else if (warp >= kProducerWarps) {
-        // ---- epilogue: drain the FP32 accumulators into the FP64 blocks ----
+        // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
+        //      last run writes (sum + run) to this CTA's FP64 block once ----
         const int q4 = warp & 3;
         const int row = 32 * q4 + lane;
+        const uint32_t lanes = (uint32_t)(32 * q4) << 16;
         int fg = 0;
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
@@ -426,8 +476,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const int nflush = (nst + F - 1) / F;
             const int ntile = G.t1 >= 0 ? 2 : 1;
             for (int f = 0; f < nflush; ++f, ++fg) {
-                const int b = fg & 1;
-                const bool ok = trj_mbar_wait(&acc_full[b], (fg >> 1) & 1);
+                const bool ok = trj_mbar_wait(&acc_full, fg & 1);
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
@@ -435,37 +484,41 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 tc_fence_after();
+                const bool last = f == nflush - 1;
                 for (int i = 0; i < ntile; ++i) {
                     const TcTile T = p.tiles[i == 0 ? G.t0 : G.t1];
                     double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
-                    const uint32_t tb = tmem + ((uint32_t)(32 * q4) << 16) + acc_col(i, b);
-                    for (int c = 0; c < T.ncols; c += 16) {
-                        uint32_t r[16];
-                        tmem_ld16(tb + (uint32_t)c, r);
-                        if (f == 0) {
+                    const uint32_t ta = tmem + lanes + acc_col(i), ts = tmem + lanes + sum_col(i);
+                    for (int c = 0; c < T.ncols; c += 16) {  // ncols is a multiple of 16
+                        uint32_t a0[16], s0[16];
+                        tmem_ld16_nowait(ta + (uint32_t)c, a0);
+                        if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
+                        tmem_wait_ld();
 #pragma unroll
-                            for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(r[k]);
+                        for (int k = 0; k < 16; ++k) {
+                            const float v = __uint_as_float(a0[k]);
+                            s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
+                        }
+                        if (last) {
+#pragma unroll
+                            for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
                         } else {
-                            double old[16];
-#pragma unroll
-                            for (int k = 0; k < 16; ++k) old[k] = dst[(int64_t)(c + k) * 128];
-#pragma unroll
-                            for (int k = 0; k < 16; ++k)
-                                dst[(int64_t)(c + k) * 128] = old[k] + (double)__uint_as_float(r[k]);
+                            tmem_st16(ts + (uint32_t)c, s0);
                         }
                     }
                 }
+                if (!last) tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&acc_empty[b]);
+                if (lane == 0) trj_mbar_arrive(&acc_empty);
             }
         }
     } else {
-        // ---- A producers (warps 0-7): one A row per thread for tile slot i = tid / 128 ----
-        const int i = tid >> 7;
+        // ---- A producers (warps 0-15): row m of tile slot i, K-chunks [h*cpt, (h+1)*cpt) ----
+        const int R = kProducers / (p.tpc * 128);  // threads per A row: 4 (one tile) or 2 (two)
+        const int i = tid / (128 * R);
+        const int h = (tid >> 7) % R;
         const int m = tid & 127;
-        const int nxl = m & 15, nyl = m >> 4;
-        const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
         int sg = 0;
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
@@ -486,26 +539,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (active) {
                     uint8_t* st = stage_ptr(slot);
                     uint8_t* ahi = st + i * 2 * kATile;
-                    uint8_t* alo = ahi + kATile;
                     const uint8_t* xy = st + a_bytes + 2 * bmax * 128 + i * (kXBytes + kYBytes);
-                    const float2* X = reinterpret_cast<const float2*>(xy);
-                    const float2* Y = reinterpret_cast<const float2*>(xy + kXBytes);
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) {  // 16-byte chunk = 4 atoms along K
-                        uint32_t hw[4], lw[4];
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const int j = c * 4 + q;
-                            const float2 x = X[j * kTcTileNx + nxl];
-                            const float2 y = Y[j * kTcTileNy + nyl];
-                            const float ar = x.x * y.x - x.y * y.y;
-                            const float ai = x.x * y.y + x.y * y.x;
-                            split2(ar, ai, hw[q], lw[q]);
-                        }
-                        const uint32_t off = rowoff + (uint32_t)((c ^ (m & 7)) << 4);
-                        *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                        *reinterpret_cast<uint4*>(alo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-                    }
+                    if (R == 4)
+                        build_a_rows<2>(ahi, xy, m, 2 * h);
+                    else
+                        build_a_rows<4>(ahi, xy, m, 4 * h);
                     fence_proxy_async();
                 }
                 __syncwarp();
@@ -714,7 +752,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         trj_dev_alloc(ctx, (void**)&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
-        trj_dev_alloc(ctx, (void**)&st->pad_off_dev, sizeof(int64_t) * (nsp + 1)) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->pad_off_dev, sizeof(int64_t) * (2 * nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
         return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
@@ -722,7 +760,16 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->groups_dev, st->groups.data(), sizeof(TcGroup) * st->groups.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunks_dev, st->chunks.data(), sizeof(TcChunk) * st->chunks.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(st->pad_off_dev, st->pad_off.data(), sizeof(int64_t) * (nsp + 1), cudaMemcpyHostToDevice);
+    // pad offsets, then the per-species slot -> atom multipliers
+    std::vector<int64_t> pad_mul(st->pad_off.begin(), st->pad_off.end());
+    for (int a = 0; a < nsp; ++a) {
+        const int64_t na = plan->species_counts[a];
+        int64_t m = na > 1 ? std::max<int64_t>(1, (int64_t)(0.6180339887498949 * (double)na + 0.5)) % na : 1;
+        auto gcd = [](int64_t x, int64_t y) { while (y) { int64_t t = x % y; x = y; y = t; } return x; };
+        while (na > 1 && (m == 0 || gcd(m, na) != 1)) m = (m + 1) % na;
+        pad_mul.push_back(m);
+    }
+    cudaMemcpy(st->pad_off_dev, pad_mul.data(), sizeof(int64_t) * (2 * nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->sched_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
     plan->scratch_bytes += (int64_t)(2 * tab_bytes + x_bytes + y_bytes + part_bytes);
@@ -784,5 +831,13 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
                                                                   plan->tc_out_dev);
     ctx->launches += 4;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_plan_set_flush(trj_sq_plan* plan, int atoms) {
+    if (!plan) return TRJ_ERR_INVALID;
+    if (atoms < kStageSlots) return trj_fail(plan->ctx, TRJ_ERR_INVALID, "flush interval %d < %d atoms", atoms, kStageSlots);
+    TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
+    if (st) st->flush_stages = atoms / kStageSlots;
     return TRJ_OK;
 }

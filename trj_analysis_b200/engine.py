@@ -155,6 +155,10 @@ class SqPlan:
     def new_out(self) -> torch.Tensor:
         return torch.zeros((self.kset.nbins, self.nit), dtype=torch.float64, device=self.ctx.torch_device)
 
+    def set_flush(self, atoms: int) -> None:
+        """Atoms accumulated in FP32 by the tensor-core path between FP64 drains."""
+        check(self.ctx.lib.trj_sq_plan_set_flush(self.h, int(atoms)), self.ctx.h, "trj_sq_plan_set_flush")
+
     def accumulate(self, packed: torch.Tensor, n: int, box, out: torch.Tensor, method: int, stream=None) -> None:
         assert out.dtype == torch.float64 and out.shape == (self.kset.nbins, self.nit)
         rc = self.ctx.lib.trj_sq_accumulate(self.h, _ptr(packed), int(n), box3(box), int(method), _ptr(out),
