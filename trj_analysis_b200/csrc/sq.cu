@@ -279,7 +279,7 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     // through its representative with (nx, ny) in the half plane {ny > 0, or ny == 0 and nx >= 0}
     // (the negated vector, conjugated, when its own (nx, ny) is outside).  Representatives are
     // grouped by (nx/16, ny/8) blocks; a block's nz span (both signs) becomes the tile's columns,
-    // split into column groups of <= 256 (128 nz values).  A negative stride marks a conjugate.
+    // split into column groups of <= 224 (112 nz values).  A negative stride marks a conjugate.
     std::vector<int64_t> dense_src(nvec, -1), dense_stride(nvec, 0);
     if (!dense_idx.empty()) {
         struct Rep { int x, y, z; bool conj; };

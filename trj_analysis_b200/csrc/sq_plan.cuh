@@ -5,11 +5,11 @@
 #include "trj_common.cuh"
 
 // Tensor-core tile geometry: 128 rows = 16 nx values x 8 ny values; columns are
-// (nz, re/im) pairs, 2*nz_count columns padded to a multiple of 16 (<= 256).
+// (nz, re/im) pairs, 2*nz_count columns padded to a multiple of 16 (<= 224).
 constexpr int kTcTileNx = 16;
 constexpr int kTcTileNy = 8;
 constexpr int kTcRows = kTcTileNx * kTcTileNy;  // 128
-constexpr int kTcMaxCols = 256;
+constexpr int kTcMaxCols = 224;
 
 struct SqTile {
     int nx0, ny0, nz0;  // lattice origin of the tile

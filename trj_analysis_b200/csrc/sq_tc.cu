@@ -8,25 +8,30 @@
 //   K index 2j = Re, 2j+1 = Im of atom j;  B columns 2t (Re out) = (zr, -zi), 2t+1 (Im out) = (zi, zr).
 // Each factor v is split v = hi + lo with hi = bf16(v), lo = bf16(v - hi); the product keeps
 // hi*hi + hi*lo + lo*hi (three tcgen05.mma kind::f16 per K-step into one FP32 TMEM accumulator).
-// The tensor core's FP32 accumulation is biased (the error of a run grows linearly with its
-// length), so every F stages (F*32 atoms, 256 by default) the accumulator is drained: the
+//
+// Operands: A is built by the producer warps straight into tensor memory (the tcgen05.mma form
+// with A in TMEM), in two alternating half-stage buffers of 16 atoms, so shared-memory bandwidth
+// goes to the B operand only.  B (the split Z factors) is a per-frame table read with 2-D TMA loads
+// (128-byte swizzle, no multicast) through a ring of 32-atom stages; each stage also carries the
+// atoms' x/y phases, from which the producers evaluate the X and Y factors of the tile in shared
+// memory before forming the products.  Tiles are up to 224 columns wide: one tcgen05.mma costs at
+// least ~90 cycles whatever its width, so wide tiles keep the tensor pipe busy.
+//
+// Accumulation: the tensor core's FP32 accumulation is biased (the error of a run grows linearly
+// with its length), so every F stages (F*32 atoms, 256 by default) the accumulator is drained: the
 // epilogue warps add it with round-to-nearest CUDA-core adds into an FP32 running sum kept in
-// TMEM, and the last drain of a work item stores that sum once, in FP64, to global memory.
-// The blocks of one species are then summed in FP64 in a fixed order.
+// TMEM, and the last drain of a work item stores that sum once, in FP64, to global memory.  The
+// blocks of one species are then summed in FP64 in a fixed order.
 //
 // Phases: every coordinate is the 32-bit fixed-point fraction u = (x/L mod 1) 2^32 (from FP64);
 // n*u mod 2^32 in integer arithmetic is exact, and sincospif of the reduced fraction gives each
-// factor at FP32 accuracy.  A per-frame kernel writes the FP32 X and Y factor tables and the
-// split BF16 Z operand; the contraction kernel reads all three with 2-D TMA loads (no multicast).
+// factor at FP32 accuracy.
 //
-// Work item = (group of up to two tiles that share their nz range, chunk of one species' atoms);
-// the B tile is loaded once per stage for both tiles.  Persistent CTAs walk the items chunk-major
-// so that concurrently running CTAs stream the same atoms (L2 reuse of the tables).
-// Roles per CTA (704 threads): warps 0-15 build the A tiles (X*Y products, split, 128-byte swizzle;
-// 4 threads per A row for a single tile, 2 per row for a pair of tiles); warps 16-19 drain the TMEM
-// accumulator into the running sum; warp 20 issues the TMA loads; warp 21 allocates TMEM and one
-// of its lanes issues the MMAs.  Every mbarrier wait is bounded and
-// raises TRJ_DEV_TIMEOUT instead of hanging.
+// Work item = (tile, chunk of one species' atoms).  Persistent CTAs walk their items chunk-major.
+// Roles per CTA (704 threads): warps 0-15 build A (X/Y factors, products, split, tcgen05.st; the
+// four warps of one TMEM lane quarter split a half-stage's 16 atoms); warps 16-19 drain the
+// accumulator; warp 20 issues the TMA loads; warp 21 allocates TMEM and one of its lanes issues
+// the MMAs.  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -38,27 +43,29 @@
 namespace {
 
 constexpr int kProducerWarps = 16;
-constexpr int kProducers = kProducerWarps * 32;
+constexpr int kProducers = kProducerWarps * 32;       // 512
 constexpr int kEpiWarps = 4;
 constexpr int kTmaWarp = kProducerWarps + kEpiWarps;  // 20
-constexpr int kMmaWarp = kTmaWarp + 1;                // 13
+constexpr int kMmaWarp = kTmaWarp + 1;                // 21
 constexpr int kTcThreads = (kMmaWarp + 1) * 32;       // 704
-constexpr int kStageSlots = 32;            // atoms per stage: K = 64 bf16 = one 128-byte swizzle row
-constexpr int kATile = 128 * 128;          // bytes of one 128 x 64 bf16 operand tile
+constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
 constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // 32 atoms x 16 complex FP32
 constexpr int kYBytes = kStageSlots * kTcTileNy * 8;  // 32 atoms x 8 complex FP32
-constexpr int kMaxStages = 4;
+constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
+constexpr int kMaxStages = 8;
+constexpr int kChunkAtoms = 12288;  // atom slots per chunk: the Z-table rows of one chunk are ~10 MB
+constexpr int kMaxTileCols = 224;
+// TMEM columns (512 allocated): accumulator at 0, running sum at 224, A half-stage buffers at 448
+// and 480 (16 columns of packed bf16 pairs for hi, then 16 for lo).
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kSumCol = 224;
+constexpr uint32_t kACol = 448;
+static_assert(kTcRows == 128, "one TMEM lane per A row");
+static_assert(kMaxTileCols <= kTcMaxCols, "tile width");
 
 struct TcTile {
     int nx0, ny0, ncols, brow;  // brow: first Z-table row (2*(nz0 - nz_min))
-    int xcol, ycol;             // first float of the tile's 16 X / 8 Y factors in a table row
     int64_t acc_off;            // doubles: offset of this tile's [ncols][128] block in a chunk's slice
-};
-
-struct TcGroup {
-    int t0, t1;    // tile indices; t1 = -1 for a single tile
-    int bcols;     // B rows loaded per stage (max ncols of the group)
-    int brow;
 };
 
 struct TcChunk {
@@ -68,42 +75,39 @@ struct TcChunk {
 
 struct TcParams {
     const TcTile* tiles;
-    const TcGroup* groups;
     const TcChunk* chunks;
-    const int32_t* cta_items;   // item ids (chunk * ngroups + group) of every CTA, concatenated
-    const int32_t* cta_off;     // gridDim.x + 1 offsets into cta_items
-    double* part;           // [chunk][acc_stride]
+    const int32_t* cta_items;  // item ids (chunk * ntiles + tile) of every CTA, concatenated
+    const int32_t* cta_off;    // gridDim.x + 1 offsets into cta_items
+    const uint2* uxy;          // per slot: x and y phase fractions
+    double* part;              // [chunk][acc_stride]
     int64_t acc_stride;
-    int ngroups, nchunks;
+    int ntiles, nchunks;
     int nstages;
     int flush_stages;
     int stage_bytes;
-    int tpc;                // tiles per CTA slot layout (1 or 2)
+    int bmax;  // B rows of a stage buffer
     unsigned* status;
 };
 
 struct TcState {
-    int nz_min = 0, table_rows = 0, nx_min = 0, nxr = 0, ny_min = 0, nyr = 0;
+    int nz_min = 0, table_rows = 0;
     int64_t total_slots = 0;
     std::vector<int64_t> pad_off;  // nsp+1 padded slot offsets
     std::vector<TcChunk> chunks;
-    std::vector<TcGroup> groups;
     std::vector<int> chunk_of_species_begin;  // nsp+1
     TcTile* tiles_dev = nullptr;
-    TcGroup* groups_dev = nullptr;
-    int32_t* sched_dev = nullptr;   // [grid + 1 offsets][items]
+    int32_t* sched_dev = nullptr;  // [grid + 1 offsets][items]
     TcChunk* chunks_dev = nullptr;
-    int64_t* pad_off_dev = nullptr;
+    int64_t* pad_off_dev = nullptr;  // nsp+1 offsets, then nsp slot -> atom multipliers
     int32_t* chunk_begin_dev = nullptr;
     __nv_bfloat16* tab_hi = nullptr;
     __nv_bfloat16* tab_lo = nullptr;
-    float2* tab_x = nullptr;
-    float2* tab_y = nullptr;
+    uint2* uxy = nullptr;
     double* part = nullptr;
     int64_t acc_stride = 0;
-    CUtensorMap map_hi, map_lo, map_x, map_y;
-    int nstages = 2, stage_bytes = 0, smem_bytes = 0, max_cols = 0, tpc = 2;
-    int flush_stages = 8;   // 256 atoms per FP32 tensor-core run between drains
+    CUtensorMap map_hi, map_lo;
+    int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
+    int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
 };
 
@@ -124,9 +128,7 @@ __device__ __forceinline__ bool bar_any(int id, int n, bool pred) {
     return r != 0;
 }
 
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -148,20 +150,21 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t smem_addr) {
     uint64_t d = 0;
     d |= (uint64_t)((smem_addr & 0x3FFFFu) >> 4);
-    d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset: next 8-row group
-    d |= (uint64_t)1 << 46;              // descriptor version
-    d |= (uint64_t)2 << 61;              // 128-byte swizzle
+    d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset: next 8-row group
+    d |= (uint64_t)1 << 46;            // descriptor version
+    d |= (uint64_t)2 << 61;            // 128-byte swizzle
     return d;
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accum) {
+// D (TMEM) += A (TMEM, 128 lanes x 16 bf16) * B (shared-memory descriptor)^T.
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accum) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }
 
@@ -192,6 +195,12 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
         : "memory");
 }
 
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&r)[4]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
+                 "r"(r[2]), "r"(r[3])
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
@@ -218,7 +227,7 @@ __device__ __forceinline__ bool timed_wait(uint64_t* bar, unsigned parity, unsig
     return false;
 }
 
-// ---- per-frame tables --------------------------------------------------------
+// ---- per-frame table ---------------------------------------------------------
 // slot -> atom of the species-padded layout; padding slots carry zero factors.  Within a species
 // the slots visit the atoms in the order local * mul[a] mod n_a (mul coprime with n_a, near the
 // golden ratio of n_a; mul = pad_off + nsp + 1): packed frames are cell-sorted, so consecutive atoms
@@ -236,22 +245,24 @@ __device__ __forceinline__ bool slot_atom(int64_t slot, const int64_t* pad_off, 
     return true;
 }
 
-// Z factors split into the B operand rows (row 2t: (zr, -zi), row 2t+1: (zi, zr) along K).
+// Z factors split into the B operand rows (row 2t: (zr, -zi), row 2t+1: (zi, zr) along K), and the
+// x/y phase fractions of every slot (zero for padding slots, whose Z rows are zero).
 __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
                                  const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nz_min,
                                  int nz_count, int64_t kdim, __nv_bfloat16* __restrict__ tab_hi,
-                                 __nv_bfloat16* __restrict__ tab_lo) {
+                                 __nv_bfloat16* __restrict__ tab_lo, uint2* __restrict__ uxy) {
     int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= total_slots) return;
-    int64_t atom;
+    int64_t atom = 0;
     const bool real = slot_atom(slot, pad_off, sp_off, nsp, atom);
-    const unsigned uz = real ? phase[atom].z : 0u;
+    const uint4 u = real ? phase[atom] : make_uint4(0u, 0u, 0u, 0u);
+    if (blockIdx.y == 0) uxy[slot] = make_uint2(u.x, u.y);
     uint32_t* hi = reinterpret_cast<uint32_t*>(tab_hi);
     uint32_t* lo = reinterpret_cast<uint32_t*>(tab_lo);
     for (int t = blockIdx.y; t < nz_count; t += gridDim.y) {
         uint32_t h0 = 0u, l0 = 0u, h1 = 0u, l1 = 0u;
         if (real) {
-            const float2 z = phase_factor((unsigned)(nz_min + t) * uz);
+            const float2 z = phase_factor((unsigned)(nz_min + t) * u.z);
             split2(z.x, -z.y, h0, l0);
             split2(z.y, z.x, h1, l1);
         }
@@ -264,62 +275,14 @@ __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t*
     }
 }
 
-// FP32 X and Y factor tables: [slot][n - n_min].
-__global__ void tc_xytable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
-                                  const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nx_min,
-                                  int nxr, int ny_min, int nyr, float2* __restrict__ tab_x,
-                                  float2* __restrict__ tab_y) {
-    const int64_t slot = blockIdx.x;
-    int64_t atom;
-    const bool real = slot_atom(slot, pad_off, sp_off, nsp, atom);
-    uint4 u = real ? phase[atom] : make_uint4(0u, 0u, 0u, 0u);
-    for (int t = threadIdx.x; t < nxr + nyr; t += blockDim.x) {
-        if (t < nxr) {
-            tab_x[slot * nxr + t] = real ? phase_factor((unsigned)(nx_min + t) * u.x) : make_float2(0.f, 0.f);
-        } else {
-            const int k = t - nxr;
-            tab_y[slot * nyr + k] = real ? phase_factor((unsigned)(ny_min + k) * u.y) : make_float2(0.f, 0.f);
-        }
-    }
-}
-
 // ---- the contraction kernel ------------------------------------------------
 
-// CPT 16-byte K-chunks (4 atoms each, starting at chunk c0) of A row m = (nx, ny) = (m % 16, m / 16):
-// A = X[nx] * Y[ny] per atom, split hi/lo, written into the 128-byte-swizzled hi tile at ahi and
-// the lo tile kATile bytes after it.
-template <int CPT>
-__device__ __forceinline__ void build_a_rows(uint8_t* ahi, const uint8_t* xy, int m, int c0) {
-    const float2* X = reinterpret_cast<const float2*>(xy);
-    const float2* Y = reinterpret_cast<const float2*>(xy + kXBytes);
-    const int nxl = m & 15, nyl = m >> 4;
-    const uint32_t rowoff = (uint32_t)((m >> 3) * 1024 + (m & 7) * 128);
-#pragma unroll
-    for (int cc = 0; cc < CPT; ++cc) {
-        const int c = c0 + cc;
-        uint32_t hw[4], lw[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int j = c * 4 + q;
-            const float2 x = X[j * kTcTileNx + nxl];
-            const float2 y = Y[j * kTcTileNy + nyl];
-            const float ar = x.x * y.x - x.y * y.y;
-            const float ai = x.x * y.y + x.y * y.x;
-            split2(ar, ai, hw[q], lw[q]);
-        }
-        const uint32_t off = rowoff + (uint32_t)((c ^ (m & 7)) << 4);
-        *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        *reinterpret_cast<uint4*>(ahi + kATile + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-    }
-}
-
 __global__ void __launch_bounds__(kTcThreads, 1)
-    sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-                 const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_y, TcParams p) {
+    sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full_tma[kMaxStages], full_a[kMaxStages], empty[kMaxStages];
-    __shared__ __align__(8) uint64_t acc_full, acc_empty;
+    __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
+    __shared__ __align__(8) uint64_t full_a[2], empty_a[2], acc_full, acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -328,26 +291,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int NS = p.nstages;
     const int F = p.flush_stages;
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
-    // stage layout: A hi/lo per tile slot, B hi/lo, X/Y per tile slot
-    const int a_bytes = p.tpc * 2 * kATile;
-    const int bmax = (p.stage_bytes - a_bytes - p.tpc * (kXBytes + kYBytes)) / 256;  // max B rows
+    // stage layout: B hi [bmax rows x 128 B], B lo, x/y phases of the stage's atoms
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
+    float2* xs = reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes);  // [32 atoms][16 nx]
+    float2* ys = xs + kStageSlots * kTcTileNx;                                    // [32 atoms][8 ny]
 
     if (tid == 0) {
         abort_flag = 0;
         for (int s = 0; s < NS; ++s) {
-            trj_mbar_init(&full_tma[s], 1);
-            trj_mbar_init(&full_a[s], kProducerWarps);
-            trj_mbar_init(&empty[s], 1);
+            trj_mbar_init(&full_b[s], 1);
+            trj_mbar_init(&empty_b[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            trj_mbar_init(&full_a[b], kProducerWarps);
+            trj_mbar_init(&empty_a[b], 1);
         }
         trj_mbar_init(&acc_full, 1);
         trj_mbar_init(&acc_empty, kEpiWarps);
+        trj_mbar_init(&mma_done, 1);
         trj_fence_mbar_init();
     }
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          trj_smem_addr(&tmem_slot)),
-                     "r"(512)
+                     "r"(kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -355,109 +322,100 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    // TMEM columns of tile slot i: FP32 accumulator (written by the MMAs) and FP32 running sum.
-    auto acc_col = [&](int i) -> uint32_t { return p.tpc == 2 ? (uint32_t)(i * 256) : 0u; };
-    auto sum_col = [&](int i) -> uint32_t { return p.tpc == 2 ? (uint32_t)(i * 256 + 128) : 256u; };
 
     if (warp == kTmaWarp) {
         if (lane == 0) {
             int sg = 0;
             for (int li = item0; li < item1 && !abort_flag; ++li) {
                 const int it = p.cta_items[li];
-                const TcGroup G = p.groups[it % p.ngroups];
-                const TcChunk C = p.chunks[it / p.ngroups];
+                const TcTile T = p.tiles[it % p.ntiles];
+                const TcChunk C = p.chunks[it / p.ntiles];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
-                const int ntile = G.t1 >= 0 ? 2 : 1;
-                const TcTile T0 = p.tiles[G.t0];
-                const TcTile T1 = p.tiles[G.t1 >= 0 ? G.t1 : G.t0];
-                const unsigned bytes = (unsigned)(2 * G.bcols * 128 + ntile * (kXBytes + kYBytes));
+                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kUxyBytes);
                 for (int s = 0; s < nst; ++s, ++sg) {
                     const int slot = sg % NS;
-                    if (!timed_wait(&empty[slot], ((sg / NS) & 1) ^ 1, p.status)) {
+                    if (!timed_wait(&empty_b[slot], ((sg / NS) & 1) ^ 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                    uint8_t* st = stage_ptr(slot);
-                    uint8_t* bh = st + a_bytes;
-                    uint8_t* bl = bh + bmax * 128;
-                    uint8_t* xy = bl + bmax * 128;
-                    trj_mbar_arrive_expect_tx(&full_tma[slot], bytes);
+                    uint8_t* bh = stage_ptr(slot);
+                    uint8_t* bl = bh + p.bmax * 128;
+                    uint8_t* ux = bl + p.bmax * 128;
+                    trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
                     const int k0 = 2 * slot0;
-                    for (int r = 0; r < G.bcols / 16; ++r) {
-                        tma_load_2d(bh + r * 2048, &map_hi, k0, G.brow + 16 * r, &full_tma[slot]);
-                        tma_load_2d(bl + r * 2048, &map_lo, k0, G.brow + 16 * r, &full_tma[slot]);
+                    for (int r = 0; r < T.ncols / 16; ++r) {
+                        tma_load_2d(bh + r * 2048, &map_hi, k0, T.brow + 16 * r, &full_b[slot]);
+                        tma_load_2d(bl + r * 2048, &map_lo, k0, T.brow + 16 * r, &full_b[slot]);
                     }
-                    tma_load_2d(xy, &map_x, T0.xcol, slot0, &full_tma[slot]);
-                    tma_load_2d(xy + kXBytes, &map_y, T0.ycol, slot0, &full_tma[slot]);
-                    if (ntile == 2) {
-                        tma_load_2d(xy + kXBytes + kYBytes, &map_x, T1.xcol, slot0, &full_tma[slot]);
-                        tma_load_2d(xy + 2 * kXBytes + kYBytes, &map_y, T1.ycol, slot0, &full_tma[slot]);
-                    }
+                    trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
                 }
             }
+            // the copies issued last land before the CTA may exit (they have, unless a wait gave up)
+            for (int q = sg > NS ? sg - NS : 0; q < sg; ++q) trj_mbar_wait(&full_b[q % NS], (q / NS) & 1);
         }
     } else if (warp == kMmaWarp) {
         if (lane == 0) {
-            // Descriptors of stage slot 0; slot k sits k * stage_bytes further (the start-address field
-            // holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds without
-            // carry).  A K-step of 16 bf16 (32 bytes) adds 2; the lo operand of A sits kATile bytes after
-            // the hi one.
-            const uint32_t base0 = trj_smem_addr(stage_ptr(0));
-            const uint64_t a0desc = sw128_desc(base0), a1desc = sw128_desc(base0 + 2 * kATile);
-            const uint64_t b0desc = sw128_desc(base0 + a_bytes);
-            const uint64_t a_lo = (uint64_t)(kATile >> 4), b_lo = (uint64_t)((bmax * 128) >> 4);
+            // B descriptor of stage slot 0; slot k sits k * stage_bytes further (the start-address
+            // field holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds
+            // without carry).  A K-step of 16 bf16 (32 bytes) adds 2; the lo operand of B sits bmax
+            // rows after the hi one.  A K-step of A in TMEM is 8 columns.
+            const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
+            const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
             int sg = 0, fg = 0;
             for (int li = item0; li < item1 && !abort_flag; ++li) {
                 const int it = p.cta_items[li];
-                const TcGroup G = p.groups[it % p.ngroups];
-                const TcChunk C = p.chunks[it / p.ngroups];
+                const TcTile T = p.tiles[it % p.ntiles];
+                const TcChunk C = p.chunks[it / p.ntiles];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
-                const int ntile = G.t1 >= 0 ? 2 : 1;
-                uint32_t idesc[2];
-                for (int i = 0; i < 2; ++i) {
-                    const int nc = p.tiles[i == 0 ? G.t0 : (G.t1 >= 0 ? G.t1 : G.t0)].ncols;
-                    idesc[i] = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nc >> 3) << 17) |
-                               ((uint32_t)(128 >> 4) << 24);
-                }
+                const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
+                                       ((uint32_t)(128 >> 4) << 24);
                 for (int s = 0; s < nst; ++s, ++sg) {
                     const int slot = sg % NS;
-                    const unsigned par = (sg / NS) & 1;
                     const bool first = (s % F) == 0;
                     // the epilogue must have read the previous run out of the accumulator
                     if (first && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                    if (!timed_wait(&full_tma[slot], par, p.status) || !timed_wait(&full_a[slot], par, p.status)) {
+                    if (!timed_wait(&full_b[slot], (sg / NS) & 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                    tc_fence_after();
-                    const uint64_t so = (uint64_t)(((uint32_t)slot * (uint32_t)p.stage_bytes) >> 4);
-                    const uint64_t bh = b0desc + so, bl = bh + b_lo;
-                    const uint32_t d0 = tmem + acc_col(0), d1 = tmem + acc_col(1);
-                    const uint64_t a0h = a0desc + so, a0l = a0h + a_lo;
-                    const uint64_t a1h = a1desc + so, a1l = a1h + a_lo;
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        const uint64_t o = 2 * kk;
-                        mma_bf16(d0, a0h + o, bh + o, idesc[0], (first && kk == 0) ? 0u : 1u);
-                        mma_bf16(d0, a0h + o, bl + o, idesc[0], 1u);
-                        mma_bf16(d0, a0l + o, bh + o, idesc[0], 1u);
-                        if (ntile == 2) {
-                            mma_bf16(d1, a1h + o, bh + o, idesc[1], (first && kk == 0) ? 0u : 1u);
-                            mma_bf16(d1, a1h + o, bl + o, idesc[1], 1u);
-                            mma_bf16(d1, a1l + o, bh + o, idesc[1], 1u);
+                    const uint64_t bh = b0desc + (uint64_t)(((uint32_t)slot * (uint32_t)p.stage_bytes) >> 4);
+                    const uint64_t bl = bh + b_lo;
+                    bool ok = true;
+                    for (int hh = 0; hh < 2 && ok; ++hh) {
+                        const int hg = 2 * sg + hh, hb = hg & 1;
+                        if (!timed_wait(&full_a[hb], (hg >> 1) & 1, p.status)) {
+                            ok = false;
+                            break;
                         }
+                        tc_fence_after();
+                        const uint32_t ah = tmem + kACol + (uint32_t)(32 * hb), al = ah + 16;
+#pragma unroll
+                        for (int k2 = 0; k2 < 2; ++k2) {
+                            const int kk = 2 * hh + k2;
+                            mma_ts(tmem, ah + 8 * k2, bh + 2 * kk, idesc, (first && kk == 0) ? 0u : 1u);
+                            mma_ts(tmem, ah + 8 * k2, bl + 2 * kk, idesc, 1u);
+                            mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
+                        }
+                        mma_commit(&empty_a[hb]);
                     }
-                    mma_commit(&empty[slot]);
+                    if (!ok) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    mma_commit(&empty_b[slot]);
                     if ((s + 1) % F == 0 || s == nst - 1) {
                         mma_commit(&acc_full);
                         ++fg;
                     }
                 }
             }
+            // every MMA of this CTA has completed before TMEM is released
+            mma_commit(&mma_done);
+            trj_mbar_wait(&mma_done, 0);
         }
     } else if (warp >= kProducerWarps) {
         // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
@@ -469,12 +427,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
-            const TcGroup G = p.groups[it % p.ngroups];
-            const int chunk = it / p.ngroups;
+            const TcTile T = p.tiles[it % p.ntiles];
+            const int chunk = it / p.ntiles;
             const TcChunk C = p.chunks[chunk];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
             const int nflush = (nst + F - 1) / F;
-            const int ntile = G.t1 >= 0 ? 2 : 1;
+            double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
             for (int f = 0; f < nflush; ++f, ++fg) {
                 const bool ok = trj_mbar_wait(&acc_full, fg & 1);
                 if (!__all_sync(0xffffffffu, ok)) {
@@ -485,26 +443,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 tc_fence_after();
                 const bool last = f == nflush - 1;
-                for (int i = 0; i < ntile; ++i) {
-                    const TcTile T = p.tiles[i == 0 ? G.t0 : G.t1];
-                    double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
-                    const uint32_t ta = tmem + lanes + acc_col(i), ts = tmem + lanes + sum_col(i);
-                    for (int c = 0; c < T.ncols; c += 16) {  // ncols is a multiple of 16
-                        uint32_t a0[16], s0[16];
-                        tmem_ld16_nowait(ta + (uint32_t)c, a0);
-                        if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
-                        tmem_wait_ld();
+                const uint32_t ta = tmem + lanes, ts = tmem + lanes + kSumCol;
+                for (int c = 0; c < T.ncols; c += 16) {  // ncols is a multiple of 16
+                    uint32_t a0[16], s0[16];
+                    tmem_ld16_nowait(ta + (uint32_t)c, a0);
+                    if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
+                    tmem_wait_ld();
 #pragma unroll
-                        for (int k = 0; k < 16; ++k) {
-                            const float v = __uint_as_float(a0[k]);
-                            s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
-                        }
-                        if (last) {
+                    for (int k = 0; k < 16; ++k) {
+                        const float v = __uint_as_float(a0[k]);
+                        s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
+                    }
+                    if (last) {
 #pragma unroll
-                            for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
-                        } else {
-                            tmem_st16(ts + (uint32_t)c, s0);
-                        }
+                        for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
+                    } else {
+                        tmem_st16(ts + (uint32_t)c, s0);
                     }
                 }
                 if (!last) tmem_wait_st();
@@ -514,40 +468,65 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         }
     } else {
-        // ---- A producers (warps 0-15): row m of tile slot i, K-chunks [h*cpt, (h+1)*cpt) ----
-        const int R = kProducers / (p.tpc * 128);  // threads per A row: 4 (one tile) or 2 (two)
-        const int i = tid / (128 * R);
-        const int h = (tid >> 7) % R;
-        const int m = tid & 127;
+        // ---- A producers (warps 0-15): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
+        //      half-stage buffer, the K-columns of atoms [4*(w/4), 4*(w/4) + 4) ----
+        const int q = warp & 3, h = warp >> 2;
+        const int m = 32 * q + lane;
+        const int nxl = m & 15, nyl = m >> 4;
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
         int sg = 0;
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
-            const TcGroup G = p.groups[it % p.ngroups];
-            const TcChunk C = p.chunks[it / p.ngroups];
+            const TcTile T = p.tiles[it % p.ntiles];
+            const TcChunk C = p.chunks[it / p.ntiles];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            const bool active = i == 0 || G.t1 >= 0;
             for (int s = 0; s < nst; ++s, ++sg) {
                 const int slot = sg % NS;
-                const bool ok = trj_mbar_wait(&full_tma[slot], (sg / NS) & 1);
+                const bool ok = trj_mbar_wait(&full_b[slot], (sg / NS) & 1);
+                // also: every producer is done with the previous stage's X/Y factors
                 if (bar_any(1, kProducers, !ok || abort_flag)) {
                     if (tid == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
                     stop = true;
                     break;
                 }
-                if (active) {
-                    uint8_t* st = stage_ptr(slot);
-                    uint8_t* ahi = st + i * 2 * kATile;
-                    const uint8_t* xy = st + a_bytes + 2 * bmax * 128 + i * (kXBytes + kYBytes);
-                    if (R == 4)
-                        build_a_rows<2>(ahi, xy, m, 2 * h);
-                    else
-                        build_a_rows<4>(ahi, xy, m, 4 * h);
-                    fence_proxy_async();
+                const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128);
+                {
+                    const int j = tid >> 4, t = tid & 15;  // 512 X factors
+                    xs[tid] = phase_factor((unsigned)(T.nx0 + t) * u[j].x);
                 }
-                __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&full_a[slot]);
+                if (tid < kStageSlots * kTcTileNy) {
+                    const int j = tid >> 3, t = tid & 7;  // 256 Y factors
+                    ys[tid] = phase_factor((unsigned)(T.ny0 + t) * u[j].y);
+                }
+                bar_sync(2, kProducers);
+                for (int hh = 0; hh < 2; ++hh) {
+                    const int hg = 2 * sg + hh, hb = hg & 1;
+                    if (!trj_mbar_wait(&empty_a[hb], ((hg >> 1) & 1) ^ 1)) {
+                        // the MMA lane has stopped; leave at the next stage's group barrier
+                        abort_flag = 1;
+                        continue;
+                    }
+                    tc_fence_after();
+                    uint32_t hw[4], lw[4];
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) {
+                        const int j = 16 * hh + 4 * h + jj;
+                        const float2 x = xs[j * kTcTileNx + nxl];
+                        const float2 y = ys[j * kTcTileNy + nyl];
+                        const float ar = x.x * y.x - x.y * y.y;
+                        const float ai = x.x * y.y + x.y * y.x;
+                        split2(ar, ai, hw[jj], lw[jj]);
+                    }
+                    const uint32_t ta = tmem + lanes + kACol + (uint32_t)(32 * hb + 4 * h);
+                    tmem_st4(ta, hw);
+                    tmem_st4(ta + 16, lw);
+                    tmem_wait_st();
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) trj_mbar_arrive(&full_a[hb]);
+                }
             }
         }
     }
@@ -555,7 +534,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __syncthreads();
     if (warp == kMmaWarp) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
 }
 
@@ -612,8 +591,8 @@ int encode_map(trj_ctx* ctx, CUtensorMap* map, void* base, CUtensorMapDataType d
 void trj_sq_tc_release(trj_sq_plan* plan) {
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (!st) return;
-    void* ptrs[] = {st->sched_dev, st->tiles_dev, st->groups_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
-                    st->tab_hi, st->tab_lo, st->tab_x, st->tab_y, st->part};
+    void* ptrs[] = {st->sched_dev, st->tiles_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
+                    st->tab_hi,    st->tab_lo,    st->uxy,        st->part};
     for (void* q : ptrs) trj_dev_free(plan->ctx, q);
     delete st;
     plan->tc_state = nullptr;
@@ -631,54 +610,29 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         st->pad_off[a + 1] = st->pad_off[a] + (plan->species_counts[a] + kStageSlots - 1) / kStageSlots * kStageSlots;
     st->total_slots = std::max<int64_t>(st->pad_off[nsp], kStageSlots);
     if (2 * st->total_slots > (int64_t)INT32_MAX) return trj_fail(ctx, TRJ_ERR_CAPACITY, "tensor path: frame too large");
-    // table extents
+    // Z-table extent and tile widths
     int nz_min = plan->tiles[0].nz0, nz_max = nz_min;
-    int nx_min = plan->tiles[0].nx0, nx_max = nx_min, ny_min = plan->tiles[0].ny0, ny_max = ny_min;
     for (const SqTile& t : plan->tiles) {
         nz_min = std::min(nz_min, t.nz0);
         nz_max = std::max(nz_max, t.nz0 + t.ncols / 2 - 1);
-        nx_min = std::min(nx_min, t.nx0);
-        nx_max = std::max(nx_max, t.nx0 + kTcTileNx);
-        ny_min = std::min(ny_min, t.ny0);
-        ny_max = std::max(ny_max, t.ny0 + kTcTileNy);
-        st->max_cols = std::max(st->max_cols, t.ncols);
+        st->bmax = std::max(st->bmax, t.ncols);
     }
+    if (st->bmax > kMaxTileCols)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile of %d columns > %d", st->bmax, kMaxTileCols);
     st->nz_min = nz_min;
     st->table_rows = 2 * (nz_max - nz_min + 1);
-    st->nx_min = nx_min;
-    st->nxr = nx_max - nx_min;
-    st->ny_min = ny_min;
-    st->nyr = ny_max - ny_min;
-    std::vector<TcTile> tt(plan->tiles.size());
+    const int ntiles = (int)plan->tiles.size();
+    std::vector<TcTile> tt(ntiles);
     int64_t acc = 0;
-    for (size_t i = 0; i < plan->tiles.size(); ++i) {
+    for (int i = 0; i < ntiles; ++i) {
         const SqTile& s = plan->tiles[i];
-        tt[i] = TcTile{s.nx0, s.ny0, s.ncols, 2 * (s.nz0 - nz_min), 2 * (s.nx0 - nx_min), 2 * (s.ny0 - ny_min), acc};
+        tt[i] = TcTile{s.nx0, s.ny0, s.ncols, 2 * (s.nz0 - nz_min), acc};
         acc += (int64_t)s.ncols * 128;
     }
     st->acc_stride = acc;
-    // groups: pair tiles of equal nz0 (sorted by width) when every tile fits two accumulators
-    st->tpc = st->max_cols <= 128 ? 2 : 1;
-    {
-        std::vector<int> order(tt.size());
-        for (size_t i = 0; i < tt.size(); ++i) order[i] = (int)i;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            if (plan->tiles[x].nz0 != plan->tiles[y].nz0) return plan->tiles[x].nz0 < plan->tiles[y].nz0;
-            return tt[x].ncols > tt[y].ncols;
-        });
-        size_t k = 0;
-        while (k < order.size()) {
-            const int a = order[k];
-            int b = -1;
-            if (st->tpc == 2 && k + 1 < order.size() && plan->tiles[order[k + 1]].nz0 == plan->tiles[a].nz0)
-                b = order[k + 1];
-            st->groups.push_back(TcGroup{a, b, std::max(tt[a].ncols, b >= 0 ? tt[b].ncols : 0), tt[a].brow});
-            k += b >= 0 ? 2 : 1;
-        }
-    }
-    // chunks: each species' slots split so that groups x chunks covers the GPU a few times
-    const int64_t ngroups = (int64_t)st->groups.size();
-    const int64_t target_chunks = std::max<int64_t>(nsp, (6 * ctx->sm_count + ngroups - 1) / ngroups);
+    // chunks: each species' slots split into runs of about kChunkAtoms atoms, and into at least as
+    // many chunks as it takes for tiles x chunks to cover the GPU a few times
+    const int64_t target_chunks = std::max<int64_t>(nsp, (6 * ctx->sm_count + ntiles - 1) / ntiles);
     const int64_t total_real = std::max<int64_t>(1, plan->n_total);
     st->chunk_of_species_begin.assign(nsp + 1, 0);
     for (int a = 0; a < nsp; ++a) {
@@ -687,6 +641,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         const int64_t stages = slots / kStageSlots;
         if (stages == 0) continue;
         int64_t k = std::max<int64_t>(1, (target_chunks * plan->species_counts[a] + total_real - 1) / total_real);
+        k = std::max<int64_t>(k, (slots + kChunkAtoms - 1) / kChunkAtoms);
         k = std::min<int64_t>(k, stages);
         for (int64_t i = 0; i < k; ++i) {
             const int64_t s0 = stages * i / k, s1 = stages * (i + 1) / k;
@@ -697,93 +652,88 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     }
     st->chunk_of_species_begin[nsp] = (int)st->chunks.size();
     if (st->chunks.empty()) return TRJ_OK;
-    // shared memory stage: A hi/lo per tile slot, B hi/lo (max width), X/Y per tile slot
-    st->stage_bytes = st->tpc * 2 * kATile + 2 * st->max_cols * 128 + st->tpc * (kXBytes + kYBytes);
-    const int avail = (int)ctx->smem_optin - 1024 - 512;
+    // shared memory: a ring of B stages (hi, lo, x/y phases), then the X/Y factor buffer
+    st->stage_bytes = (2 * st->bmax * 128 + kUxyBytes + 1023) / 1024 * 1024;
+    const int avail = (int)ctx->smem_optin - 2048 - kXBytes - kYBytes;
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
-    st->smem_bytes = st->nstages * st->stage_bytes + 1024;
-    const int64_t nitems = ngroups * (int64_t)st->chunks.size();
+    st->smem_bytes = st->nstages * st->stage_bytes + kXBytes + kYBytes + 1024;
+    const int64_t nitems = (int64_t)ntiles * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
-    // Longest-processing-time-first schedule: items costed by (columns + producer work) x stages,
-    // each assigned to the least-loaded CTA; every CTA then walks its items in chunk order.
+    // Schedule: the items in chunk-major order are cut into windows of `grid` items; within a window
+    // each item (costed by (columns + A-build work) x stages, longest first) goes to the least-loaded
+    // CTA.  Every CTA walks its items window by window, so at any time the CTAs stream the Z-table
+    // rows of the same few chunks and the L2 serves each chunk to every tile.
     std::vector<int32_t> sched;
     {
-        std::vector<std::pair<double, int32_t>> items;
-        items.reserve(nitems);
-        for (int64_t c = 0; c < (int64_t)st->chunks.size(); ++c) {
-            const double stages = (double)(st->chunks[c].slot1 - st->chunks[c].slot0) / kStageSlots;
-            for (int64_t g = 0; g < ngroups; ++g) {
-                const TcGroup& G = st->groups[g];
-                const double cols = tt[G.t0].ncols + (G.t1 >= 0 ? tt[G.t1].ncols : 0);
-                const double rows = G.t1 >= 0 ? 256.0 : 128.0;
-                items.push_back({stages * (cols + 0.5 * rows), (int32_t)(c * ngroups + g)});
-            }
-        }
-        std::stable_sort(items.begin(), items.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
         std::vector<std::vector<int32_t>> lists(st->grid);
         std::vector<std::pair<double, int>> heap;  // (load, cta), min-heap
         for (int b = 0; b < st->grid; ++b) heap.push_back({0.0, b});
         auto cmp = [](const std::pair<double, int>& a, const std::pair<double, int>& b) { return a > b; };
         std::make_heap(heap.begin(), heap.end(), cmp);
-        for (const auto& it : items) {
-            std::pop_heap(heap.begin(), heap.end(), cmp);
-            heap.back().first += it.first;
-            lists[heap.back().second].push_back(it.second);
-            std::push_heap(heap.begin(), heap.end(), cmp);
+        std::vector<std::pair<double, int32_t>> win;
+        for (int64_t w0 = 0; w0 < nitems; w0 += st->grid) {
+            win.clear();
+            for (int64_t it = w0; it < std::min<int64_t>(nitems, w0 + st->grid); ++it) {
+                const TcChunk& C = st->chunks[it / ntiles];
+                const double stages = (double)(C.slot1 - C.slot0) / kStageSlots;
+                win.push_back({stages * (tt[it % ntiles].ncols + 24.0), (int32_t)it});
+            }
+            std::stable_sort(win.begin(), win.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+            for (const auto& it : win) {
+                std::pop_heap(heap.begin(), heap.end(), cmp);
+                heap.back().first += it.first;
+                lists[heap.back().second].push_back(it.second);
+                std::push_heap(heap.begin(), heap.end(), cmp);
+            }
         }
         sched.assign(st->grid + 1, 0);
-        for (int b = 0; b < st->grid; ++b) {
-            std::sort(lists[b].begin(), lists[b].end());
-            sched[b + 1] = sched[b] + (int32_t)lists[b].size();
-        }
+        for (int b = 0; b < st->grid; ++b) sched[b + 1] = sched[b] + (int32_t)lists[b].size();
         for (int b = 0; b < st->grid; ++b) sched.insert(sched.end(), lists[b].begin(), lists[b].end());
     }
 
     const int64_t kdim = 2 * st->total_slots;
     size_t tab_bytes = (size_t)st->table_rows * (size_t)kdim * sizeof(__nv_bfloat16);
-    size_t x_bytes = sizeof(float2) * (size_t)st->total_slots * st->nxr;
-    size_t y_bytes = sizeof(float2) * (size_t)st->total_slots * st->nyr;
+    size_t uxy_bytes = sizeof(uint2) * (size_t)st->total_slots;
     size_t part_bytes = sizeof(double) * (size_t)st->acc_stride * st->chunks.size();
     std::vector<int32_t> cb(st->chunk_of_species_begin.begin(), st->chunk_of_species_begin.end());
-    if (trj_dev_alloc(ctx, (void**)&st->tab_hi, tab_bytes) != cudaSuccess || trj_dev_alloc(ctx, (void**)&st->tab_lo, tab_bytes) != cudaSuccess ||
-        trj_dev_alloc(ctx, (void**)&st->tab_x, x_bytes) != cudaSuccess || trj_dev_alloc(ctx, (void**)&st->tab_y, y_bytes) != cudaSuccess ||
+    if (trj_dev_alloc(ctx, (void**)&st->tab_hi, tab_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->tab_lo, tab_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->uxy, uxy_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->part, part_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
-        trj_dev_alloc(ctx, (void**)&st->groups_dev, sizeof(TcGroup) * st->groups.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->pad_off_dev, sizeof(int64_t) * (2 * nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
-        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
-                        2 * tab_bytes + x_bytes + y_bytes + part_bytes);
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables", 2 * tab_bytes + uxy_bytes + part_bytes);
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(st->groups_dev, st->groups.data(), sizeof(TcGroup) * st->groups.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunks_dev, st->chunks.data(), sizeof(TcChunk) * st->chunks.size(), cudaMemcpyHostToDevice);
     // pad offsets, then the per-species slot -> atom multipliers
     std::vector<int64_t> pad_mul(st->pad_off.begin(), st->pad_off.end());
     for (int a = 0; a < nsp; ++a) {
         const int64_t na = plan->species_counts[a];
         int64_t m = na > 1 ? std::max<int64_t>(1, (int64_t)(0.6180339887498949 * (double)na + 0.5)) % na : 1;
-        auto gcd = [](int64_t x, int64_t y) { while (y) { int64_t t = x % y; x = y; y = t; } return x; };
+        auto gcd = [](int64_t x, int64_t y) {
+            while (y) {
+                int64_t t = x % y;
+                x = y;
+                y = t;
+            }
+            return x;
+        };
         while (na > 1 && (m == 0 || gcd(m, na) != 1)) m = (m + 1) % na;
         pad_mul.push_back(m);
     }
     cudaMemcpy(st->pad_off_dev, pad_mul.data(), sizeof(int64_t) * (2 * nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->sched_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
-    plan->scratch_bytes += (int64_t)(2 * tab_bytes + x_bytes + y_bytes + part_bytes);
+    plan->scratch_bytes += (int64_t)(2 * tab_bytes + uxy_bytes + part_bytes);
     int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
                         16, CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc == TRJ_OK)
         rc = encode_map(ctx, &st->map_lo, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
                         16, CU_TENSOR_MAP_SWIZZLE_128B);
-    if (rc == TRJ_OK)
-        rc = encode_map(ctx, &st->map_x, st->tab_x, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, 2 * (int64_t)st->nxr,
-                        st->total_slots, 2 * kTcTileNx, kStageSlots, CU_TENSOR_MAP_SWIZZLE_NONE);
-    if (rc == TRJ_OK)
-        rc = encode_map(ctx, &st->map_y, st->tab_y, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, 2 * (int64_t)st->nyr,
-                        st->total_slots, 2 * kTcTileNy, kStageSlots, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
@@ -800,43 +750,40 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     const int nz_count = st->table_rows / 2;
     dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 32));
     tc_ztable_kernel<<<zg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
-                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo);
-    tc_xytable_kernel<<<(unsigned)st->total_slots, 128, 0, s>>>(plan->phase_dev, plan->species_off_dev,
-                                                                st->pad_off_dev, plan->nsp, st->total_slots,
-                                                                st->nx_min, st->nxr, st->ny_min, st->nyr, st->tab_x,
-                                                                st->tab_y);
+                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo, st->uxy);
     TcParams P;
     P.tiles = st->tiles_dev;
-    P.groups = st->groups_dev;
     P.chunks = st->chunks_dev;
     P.cta_off = st->sched_dev;
     P.cta_items = st->sched_dev + st->grid + 1;
+    P.uxy = st->uxy;
     P.part = st->part;
     P.acc_stride = st->acc_stride;
-    P.ngroups = (int)st->groups.size();
+    P.ntiles = (int)plan->tiles.size();
     P.nchunks = (int)st->chunks.size();
     P.nstages = st->nstages;
     P.flush_stages = st->flush_stages;
     P.stage_bytes = st->stage_bytes;
-    P.tpc = st->tpc;
+    P.bmax = st->bmax;
     P.status = ctx->status_dev;
     // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
     plan->timer.begin(ctx, s);
-    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_x, st->map_y, P);
+    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, P);
     plan->timer.end(ctx, s);
     tc_reduce_kernel<<<(unsigned)plan->tiles.size(), 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev,
                                                                   plan->tiles_dev, st->chunk_begin_dev, plan->nsp,
                                                                   plan->tc_out_dev);
-    ctx->launches += 4;
+    ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
 }
 
 extern "C" int trj_sq_plan_set_flush(trj_sq_plan* plan, int atoms) {
     if (!plan) return TRJ_ERR_INVALID;
-    if (atoms < kStageSlots) return trj_fail(plan->ctx, TRJ_ERR_INVALID, "flush interval %d < %d atoms", atoms, kStageSlots);
+    if (atoms < kStageSlots)
+        return trj_fail(plan->ctx, TRJ_ERR_INVALID, "flush interval %d < %d atoms", atoms, kStageSlots);
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (st) st->flush_stages = atoms / kStageSlots;
     return TRJ_OK;

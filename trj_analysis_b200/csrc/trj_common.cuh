@@ -109,8 +109,11 @@ __host__ __device__ __forceinline__ int trj_pair_row(int a, int b, int nsp) {
     return a * (nsp - 1) - a * (a - 1) / 2 + b;
 }
 
-// Bound on iterations of any spin wait in this library (mbarrier try_wait loops).
-#define TRJ_SPIN_LIMIT (1u << 26)
+// Bound on any mbarrier wait in this library, in SM clocks (2^32 clocks: about 2 s at 2 GHz).
+#define TRJ_WAIT_CLOCKS (1ll << 32)
+// Longest single hardware suspension of a waiting thread (ns); it resumes as soon as the phase
+// completes, so the value only bounds how often the deadline is checked.
+#define TRJ_SUSPEND_NS 20000u
 
 __device__ __forceinline__ void trj_raise(unsigned* status, unsigned bit) {
     atomicOr(status, bit);
@@ -141,23 +144,24 @@ __device__ __forceinline__ void trj_mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(trj_smem_addr(bar)) : "memory");
 }
 
-// Returns true once phase `parity` of the barrier has completed; false after
-// TRJ_SPIN_LIMIT polls (caller raises TRJ_DEV_TIMEOUT and leaves).
+// Returns true once phase `parity` of the barrier has completed; false after TRJ_WAIT_CLOCKS
+// (caller raises TRJ_DEV_TIMEOUT and leaves).  try_wait with a suspend-time hint parks the thread
+// in hardware until the phase completes, so a waiting warp issues no polling instructions.
 __device__ __forceinline__ bool trj_mbar_wait(uint64_t* bar, unsigned parity) {
-    uint32_t addr = trj_smem_addr(bar);
-    for (unsigned it = 0; it < TRJ_SPIN_LIMIT; ++it) {
+    const uint32_t addr = trj_smem_addr(bar);
+    const long long t0 = clock64();
+    while (true) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(addr), "r"(parity)
+            : "r"(addr), "r"(parity), "r"(TRJ_SUSPEND_NS)
             : "memory");
         if (done) return true;
-        if (it > 64) __nanosleep(32);
+        if (clock64() - t0 > TRJ_WAIT_CLOCKS) return false;
     }
-    return false;
 }
 
 // 1-D bulk copy global -> shared (TMA engine, no multicast), completion on `bar`.
