@@ -28,10 +28,12 @@
 // factor at FP32 accuracy.
 //
 // Work item = (tile, chunk of one species' atoms).  Persistent CTAs walk their items chunk-major.
-// Roles per CTA (704 threads): warps 0-15 build A (X/Y factors, products, split, tcgen05.st; the
-// four warps of one TMEM lane quarter split a half-stage's 16 atoms); warps 16-19 drain the
-// accumulator; warp 20 issues the TMA loads; warp 21 allocates TMEM and one of its lanes issues
-// the MMAs.  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
+// Roles per CTA (704 threads), handing stages to each other through mbarriers only: warps 8-11
+// evaluate the X/Y factors of a stage into one of two shared-memory buffers; warps 0-7 form the
+// products, split them and store them into the A buffers in TMEM (the two warps of one TMEM lane
+// quarter split a half-stage's 16 atoms); warps 12-19 drain the accumulator (two warps per lane
+// quarter, alternating 16-column chunks); warp 20 issues the TMA loads; warp 21 allocates TMEM and
+// one of its lanes issues the MMAs.  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -42,15 +44,18 @@
 
 namespace {
 
-constexpr int kProducerWarps = 16;
-constexpr int kProducers = kProducerWarps * 32;       // 512
-constexpr int kEpiWarps = 4;
-constexpr int kTmaWarp = kProducerWarps + kEpiWarps;  // 20
-constexpr int kMmaWarp = kTmaWarp + 1;                // 21
-constexpr int kTcThreads = (kMmaWarp + 1) * 32;       // 704
+constexpr int kBuildWarps = 8;                     // warps 0-7: A products into TMEM
+constexpr int kXyWarps = 4;                        // warps 8-11: X/Y factors into shared memory
+constexpr int kEpiWarps = 8;                       // warps 12-19: accumulator drains
+constexpr int kXyWarp0 = kBuildWarps;
+constexpr int kEpiWarp0 = kXyWarp0 + kXyWarps;
+constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
+constexpr int kMmaWarp = kTmaWarp + 1;             // 21
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
-constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // 32 atoms x 16 complex FP32
-constexpr int kYBytes = kStageSlots * kTcTileNy * 8;  // 32 atoms x 8 complex FP32
+constexpr int kXBytes = kStageSlots * kTcTileNx * 16;  // 32 atoms x 16 X factors as (xr, xr, xi, xi)
+constexpr int kYBytes = kStageSlots * kTcTileNy * 16;  // 32 atoms x 8 Y factors as (yr, yi, -yi, yr)
+constexpr int kXyBytes = kXBytes + kYBytes;           // one of the two X/Y buffers
 constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
 constexpr int kMaxStages = 8;
 constexpr int kChunkAtoms = 12288;  // atom slots per chunk: the Z-table rows of one chunk are ~10 MB
@@ -105,30 +110,13 @@ struct TcState {
     uint2* uxy = nullptr;
     double* part = nullptr;
     int64_t acc_stride = 0;
-    CUtensorMap map_hi, map_lo;
+    CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
 };
 
 // ---- PTX wrappers ----------------------------------------------------------
-
-// Barrier `id` over n threads that also returns whether any participant passed pred = true,
-// so a group leaves a loop together (a plain named barrier has no timeout).
-__device__ __forceinline__ bool bar_any(int id, int n, bool pred) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, %3, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)pred), "r"(id), "r"(n)
-        : "memory");
-    return r != 0;
-}
-
-__device__ __forceinline__ void bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 
 __device__ __forceinline__ void tc_fence_before() {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -195,15 +183,45 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&r)[4]) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
-                 "r"(r[2]), "r"(r[3])
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
                  : "memory");
 }
 
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// Packed FP32 pairs (sm_100 f32x2 arithmetic, round to nearest): low word = first value.
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// A = X * Y from the packed smem forms X = ((xr, xr), (xi, xi)), Y = ((yr, yi), (-yi, yr)):
+// (ar, ai) = (xr, xr) * (yr, yi) + (xi, xi) * (-yi, yr); then the hi/lo BF16 split of (ar, ai).
+__device__ __forceinline__ void product_split(ulonglong2 x, ulonglong2 y, uint32_t& hi, uint32_t& lo) {
+    const uint64_t r = f2_fma(x.x, y.x, f2_mul(x.y, y.y));
+    const uint32_t h = bf2_bits(__floats2bfloat162_rn(__uint_as_float((uint32_t)r), __uint_as_float((uint32_t)(r >> 32))));
+    const uint64_t hf = ((uint64_t)(h & 0xffff0000u) << 32) | (uint64_t)(h << 16);
+    const uint64_t d = f2_sub(r, hf);  // exact: r minus its 8-bit rounding
+    hi = h;
+    lo = bf2_bits(__floats2bfloat162_rn(__uint_as_float((uint32_t)d), __uint_as_float((uint32_t)(d >> 32))));
+}
 
 // hi/lo BF16 split of a pair (one value in each half of the 32-bit word, low half first).
 __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
@@ -278,11 +296,12 @@ __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t*
 // ---- the contraction kernel ------------------------------------------------
 
 __global__ void __launch_bounds__(kTcThreads, 1)
-    sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo, TcParams p) {
+    sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                 const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t full_a[2], empty_a[2], acc_full, acc_empty, mma_done;
+    __shared__ __align__(8) uint64_t full_a[2], empty_a[2], xy_full[2], xy_empty[2], acc_full, acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -293,8 +312,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
     // stage layout: B hi [bmax rows x 128 B], B lo, x/y phases of the stage's atoms
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
-    float2* xs = reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes);  // [32 atoms][16 nx]
-    float2* ys = xs + kStageSlots * kTcTileNx;                                    // [32 atoms][8 ny]
+    // X/Y buffer b: [32 atoms][16 nx] X factors, then [32 atoms][8 ny] Y factors
+    auto xy_ptr = [&](int b) { return reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
 
     if (tid == 0) {
         abort_flag = 0;
@@ -303,8 +322,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             trj_mbar_init(&empty_b[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
-            trj_mbar_init(&full_a[b], kProducerWarps);
+            trj_mbar_init(&full_a[b], kBuildWarps);
             trj_mbar_init(&empty_a[b], 1);
+            trj_mbar_init(&xy_full[b], kXyWarps);
+            trj_mbar_init(&xy_empty[b], kBuildWarps);
         }
         trj_mbar_init(&acc_full, 1);
         trj_mbar_init(&acc_empty, kEpiWarps);
@@ -325,16 +346,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
     if (warp == kTmaWarp) {
         if (lane == 0) {
-            int sg = 0;
+            // ring position of the next stage (slot, phase) kept incrementally: no divisions per stage
+            int slot = 0, issued = 0;
+            unsigned phase = 0;
             for (int li = item0; li < item1 && !abort_flag; ++li) {
                 const int it = p.cta_items[li];
                 const TcTile T = p.tiles[it % p.ntiles];
                 const TcChunk C = p.chunks[it / p.ntiles];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
                 const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kUxyBytes);
-                for (int s = 0; s < nst; ++s, ++sg) {
-                    const int slot = sg % NS;
-                    if (!timed_wait(&empty_b[slot], ((sg / NS) & 1) ^ 1, p.status)) {
+                const int n64 = T.ncols / 64;  // B rows as 64-row boxes, then 16-row boxes
+                for (int s = 0; s < nst; ++s) {
+                    if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
@@ -344,15 +367,32 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
                     const int k0 = 2 * slot0;
-                    for (int r = 0; r < T.ncols / 16; ++r) {
-                        tma_load_2d(bh + r * 2048, &map_hi, k0, T.brow + 16 * r, &full_b[slot]);
-                        tma_load_2d(bl + r * 2048, &map_lo, k0, T.brow + 16 * r, &full_b[slot]);
+                    int r = 0;
+                    for (int b = 0; b < n64; ++b, r += 64) {
+                        tma_load_2d(bh + r * 128, &map_hi64, k0, T.brow + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo64, k0, T.brow + r, &full_b[slot]);
+                    }
+                    for (; r < T.ncols; r += 16) {
+                        tma_load_2d(bh + r * 128, &map_hi, k0, T.brow + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo, k0, T.brow + r, &full_b[slot]);
                     }
                     trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
+                    ++issued;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                    }
                 }
             }
-            // the copies issued last land before the CTA may exit (they have, unless a wait gave up)
-            for (int q = sg > NS ? sg - NS : 0; q < sg; ++q) trj_mbar_wait(&full_b[q % NS], (q / NS) & 1);
+            // the copies issued last land before the CTA may exit (they have, unless a wait gave up):
+            // walk the ring back over the last min(issued, NS) stages
+            for (int q = 0; q < NS && q < issued; ++q) {
+                if (--slot < 0) {
+                    slot = NS - 1;
+                    phase ^= 1;
+                }
+                trj_mbar_wait(&full_b[slot], phase);
+            }
         }
     } else if (warp == kMmaWarp) {
         if (lane == 0) {
@@ -362,7 +402,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             // rows after the hi one.  A K-step of A in TMEM is 8 columns.
             const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
             const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
-            int sg = 0, fg = 0;
+            const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
+            int slot = 0, fg = 0;
+            unsigned phase = 0, aphase = 0;  // B ring phase; A buffers flip every stage
+            uint64_t bh = b0desc;            // B descriptor of the current slot
             for (int li = item0; li < item1 && !abort_flag; ++li) {
                 const int it = p.cta_items[li];
                 const TcTile T = p.tiles[it % p.ntiles];
@@ -370,24 +413,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
                 const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
                                        ((uint32_t)(128 >> 4) << 24);
-                for (int s = 0; s < nst; ++s, ++sg) {
-                    const int slot = sg % NS;
-                    const bool first = (s % F) == 0;
+                int rs = 0;  // stage within the current run
+                for (int s = 0; s < nst; ++s) {
+                    const bool first = rs == 0;
                     // the epilogue must have read the previous run out of the accumulator
                     if (first && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                    if (!timed_wait(&full_b[slot], (sg / NS) & 1, p.status)) {
+                    if (!timed_wait(&full_b[slot], phase, p.status)) {
                         abort_flag = 1;
                         break;
                     }
-                    const uint64_t bh = b0desc + (uint64_t)(((uint32_t)slot * (uint32_t)p.stage_bytes) >> 4);
                     const uint64_t bl = bh + b_lo;
                     bool ok = true;
                     for (int hh = 0; hh < 2 && ok; ++hh) {
-                        const int hg = 2 * sg + hh, hb = hg & 1;
-                        if (!timed_wait(&full_a[hb], (hg >> 1) & 1, p.status)) {
+                        const int hb = hh;
+                        if (!timed_wait(&full_a[hb], aphase, p.status)) {
                             ok = false;
                             break;
                         }
@@ -407,9 +449,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         break;
                     }
                     mma_commit(&empty_b[slot]);
-                    if ((s + 1) % F == 0 || s == nst - 1) {
+                    if (++rs == F || s == nst - 1) {
                         mma_commit(&acc_full);
                         ++fg;
+                        rs = 0;
+                    }
+                    aphase ^= 1;
+                    bh += b_step;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                        bh = b0desc;
                     }
                 }
             }
@@ -417,10 +467,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mma_commit(&mma_done);
             trj_mbar_wait(&mma_done, 0);
         }
-    } else if (warp >= kProducerWarps) {
+    } else if (warp >= kEpiWarp0) {
         // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
         //      last run writes (sum + run) to this CTA's FP64 block once ----
         const int q4 = warp & 3;
+        const int c0 = 16 * ((warp - kEpiWarp0) >> 2);  // first 16-column chunk of this warp
         const int row = 32 * q4 + lane;
         const uint32_t lanes = (uint32_t)(32 * q4) << 16;
         int fg = 0;
@@ -444,7 +495,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_after();
                 const bool last = f == nflush - 1;
                 const uint32_t ta = tmem + lanes, ts = tmem + lanes + kSumCol;
-                for (int c = 0; c < T.ncols; c += 16) {  // ncols is a multiple of 16
+                for (int c = c0; c < T.ncols; c += 32) {  // ncols is a multiple of 16
                     uint32_t a0[16], s0[16];
                     tmem_ld16_nowait(ta + (uint32_t)c, a0);
                     if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
@@ -467,14 +518,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (lane == 0) trj_mbar_arrive(&acc_empty);
             }
         }
-    } else {
-        // ---- A producers (warps 0-15): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
-        //      half-stage buffer, the K-columns of atoms [4*(w/4), 4*(w/4) + 4) ----
-        const int q = warp & 3, h = warp >> 2;
-        const int m = 32 * q + lane;
-        const int nxl = m & 15, nyl = m >> 4;
-        const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        int sg = 0;
+    } else if (warp >= kXyWarp0) {
+        // ---- X/Y factors of each stage from the x/y phases that arrived with its B rows ----
+        const int xt = tid - kXyWarp0 * 32;
+        int sg = 0, slot = 0;
+        unsigned phase = 0;
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
@@ -482,51 +530,83 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const TcChunk C = p.chunks[it / p.ntiles];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
             for (int s = 0; s < nst; ++s, ++sg) {
-                const int slot = sg % NS;
-                const bool ok = trj_mbar_wait(&full_b[slot], (sg / NS) & 1);
-                // also: every producer is done with the previous stage's X/Y factors
-                if (bar_any(1, kProducers, !ok || abort_flag)) {
-                    if (tid == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                const int xb = sg & 1;
+                bool ok = trj_mbar_wait(&full_b[slot], phase);
+                ok = ok && trj_mbar_wait(&xy_empty[xb], ((sg >> 1) & 1) ^ 1);
+                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
                     stop = true;
                     break;
                 }
                 const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128);
-                {
-                    const int j = tid >> 4, t = tid & 15;  // 512 X factors
-                    xs[tid] = phase_factor((unsigned)(T.nx0 + t) * u[j].x);
+                float4* xs = xy_ptr(xb);
+                float4* ys = xs + kStageSlots * kTcTileNx;
+                for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32) {
+                    const float2 f = phase_factor((unsigned)(T.nx0 + (e & 15)) * u[e >> 4].x);
+                    xs[e] = make_float4(f.x, f.x, f.y, f.y);
                 }
-                if (tid < kStageSlots * kTcTileNy) {
-                    const int j = tid >> 3, t = tid & 7;  // 256 Y factors
-                    ys[tid] = phase_factor((unsigned)(T.ny0 + t) * u[j].y);
+                for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32) {
+                    const float2 f = phase_factor((unsigned)(T.ny0 + (e & 7)) * u[e >> 3].y);
+                    ys[e] = make_float4(f.x, f.y, -f.y, f.x);
                 }
-                bar_sync(2, kProducers);
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
+                if (++slot == NS) {
+                    slot = 0;
+                    phase ^= 1;
+                }
+            }
+        }
+    } else {
+        // ---- A builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
+        //      half-stage buffer, the K-columns of atoms [8*(w/4), 8*(w/4) + 8) ----
+        const int q = warp & 3, g = warp >> 2;
+        const int m = 32 * q + lane;
+        const int nxl = m & 15, nyl = m >> 4;
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
+        int sg = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cta_items[li];
+            const TcChunk C = p.chunks[it / p.ntiles];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            for (int s = 0; s < nst && !stop; ++s, ++sg) {
+                const int xb = sg & 1;
+                const bool ok = trj_mbar_wait(&xy_full[xb], (sg >> 1) & 1);
+                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                const ulonglong2* xs = reinterpret_cast<const ulonglong2*>(xy_ptr(xb));
+                const ulonglong2* ys = xs + kStageSlots * kTcTileNx;
                 for (int hh = 0; hh < 2; ++hh) {
                     const int hg = 2 * sg + hh, hb = hg & 1;
-                    if (!trj_mbar_wait(&empty_a[hb], ((hg >> 1) & 1) ^ 1)) {
-                        // the MMA lane has stopped; leave at the next stage's group barrier
+                    if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], ((hg >> 1) & 1) ^ 1))) {
+                        if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                         abort_flag = 1;
-                        continue;
+                        stop = true;
+                        break;
                     }
                     tc_fence_after();
-                    uint32_t hw[4], lw[4];
+                    uint32_t hw[8], lw[8];
 #pragma unroll
-                    for (int jj = 0; jj < 4; ++jj) {
-                        const int j = 16 * hh + 4 * h + jj;
-                        const float2 x = xs[j * kTcTileNx + nxl];
-                        const float2 y = ys[j * kTcTileNy + nyl];
-                        const float ar = x.x * y.x - x.y * y.y;
-                        const float ai = x.x * y.y + x.y * y.x;
-                        split2(ar, ai, hw[jj], lw[jj]);
+                    for (int jj = 0; jj < 8; ++jj) {
+                        const int j = 16 * hh + 8 * g + jj;
+                        product_split(xs[j * kTcTileNx + nxl], ys[j * kTcTileNy + nyl], hw[jj], lw[jj]);
                     }
-                    const uint32_t ta = tmem + lanes + kACol + (uint32_t)(32 * hb + 4 * h);
-                    tmem_st4(ta, hw);
-                    tmem_st4(ta + 16, lw);
+                    const uint32_t ta = tmem + lanes + kACol + (uint32_t)(32 * hb + 8 * g);
+                    tmem_st8(ta, hw);
+                    tmem_st8(ta + 16, lw);
                     tmem_wait_st();
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) trj_mbar_arrive(&full_a[hb]);
                 }
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&xy_empty[xb]);
             }
         }
     }
@@ -652,12 +732,12 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     }
     st->chunk_of_species_begin[nsp] = (int)st->chunks.size();
     if (st->chunks.empty()) return TRJ_OK;
-    // shared memory: a ring of B stages (hi, lo, x/y phases), then the X/Y factor buffer
+    // shared memory: a ring of B stages (hi, lo, x/y phases), then the two X/Y factor buffers
     st->stage_bytes = (2 * st->bmax * 128 + kUxyBytes + 1023) / 1024 * 1024;
-    const int avail = (int)ctx->smem_optin - 2048 - kXBytes - kYBytes;
+    const int avail = (int)ctx->smem_optin - 2048 - 2 * kXyBytes;
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
-    st->smem_bytes = st->nstages * st->stage_bytes + kXBytes + kYBytes + 1024;
+    st->smem_bytes = st->nstages * st->stage_bytes + 2 * kXyBytes + 1024;
     const int64_t nitems = (int64_t)ntiles * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
     // Schedule: the items in chunk-major order are cut into windows of `grid` items; within a window
@@ -734,6 +814,12 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     if (rc == TRJ_OK)
         rc = encode_map(ctx, &st->map_lo, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
                         16, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc == TRJ_OK)
+        rc = encode_map(ctx, &st->map_hi64, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
+                        64, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc == TRJ_OK)
+        rc = encode_map(ctx, &st->map_lo64, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
+                        64, CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
@@ -770,7 +856,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
     plan->timer.begin(ctx, s);
-    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, P);
+    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, P);
     plan->timer.end(ctx, s);
     tc_reduce_kernel<<<(unsigned)plan->tiles.size(), 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev,
                                                                   plan->tiles_dev, st->chunk_begin_dev, plan->nsp,

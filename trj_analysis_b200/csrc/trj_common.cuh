@@ -113,7 +113,9 @@ __host__ __device__ __forceinline__ int trj_pair_row(int a, int b, int nsp) {
 #define TRJ_WAIT_CLOCKS (1ll << 32)
 // Longest single hardware suspension of a waiting thread (ns); it resumes as soon as the phase
 // completes, so the value only bounds how often the deadline is checked.
+#ifndef TRJ_SUSPEND_NS
 #define TRJ_SUSPEND_NS 20000u
+#endif
 
 __device__ __forceinline__ void trj_raise(unsigned* status, unsigned bit) {
     atomicOr(status, bit);
