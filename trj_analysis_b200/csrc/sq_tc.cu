@@ -619,20 +619,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 // tc_out[tile][a][col][row] = sum over species a's chunks (fixed order) of the FP64 blocks.
+// Grid (element blocks, tile, species): one thread per output element.
 __global__ void tc_reduce_kernel(const double* __restrict__ part, int64_t acc_stride, const TcTile* __restrict__ tiles,
                                  const SqTile* __restrict__ stiles, const int32_t* __restrict__ chunk_begin, int nsp,
                                  double* __restrict__ out) {
-    const int t = blockIdx.x;
+    const int t = blockIdx.y, a = blockIdx.z;
     const TcTile T = tiles[t];
     const int64_t n = (int64_t)T.ncols * 128;
-    for (int a = 0; a < nsp; ++a) {
-        const int k0 = chunk_begin[a], k1 = chunk_begin[a + 1];
-        for (int64_t e = threadIdx.x; e < n; e += blockDim.x) {
-            double s = 0.0;
-            for (int k = k0; k < k1; ++k) s += part[(int64_t)k * acc_stride + T.acc_off + e];
-            out[stiles[t].out_off + (int64_t)a * n + e] = s;
-        }
-    }
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int k0 = chunk_begin[a], k1 = chunk_begin[a + 1];
+    const double* src = part + T.acc_off + e;
+    double s = 0.0;
+    for (int k = k0; k < k1; ++k) s += __ldcs(src + (int64_t)k * acc_stride);
+    out[stiles[t].out_off + (int64_t)a * n + e] = s;
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -858,9 +858,9 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     plan->timer.begin(ctx, s);
     sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, P);
     plan->timer.end(ctx, s);
-    tc_reduce_kernel<<<(unsigned)plan->tiles.size(), 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev,
-                                                                  plan->tiles_dev, st->chunk_begin_dev, plan->nsp,
-                                                                  plan->tc_out_dev);
+    const dim3 rg((unsigned)((st->bmax * 128 + 255) / 256), (unsigned)plan->tiles.size(), (unsigned)plan->nsp);
+    tc_reduce_kernel<<<rg, 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev, plan->tiles_dev, st->chunk_begin_dev,
+                                        plan->nsp, plan->tc_out_dev);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
