@@ -39,6 +39,20 @@ WORKLOADS = {
 }
 
 
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` on
+    `workload`, from the committed ncu summary profiles/<kernel>_<workload>.md, or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -271,7 +285,7 @@ def run_ours(args, rank, world, local_rank):
         peak = peaks.get("bf16_tflops_sustained", 1400.0)
         achieved = flops / (sq_ms / 1000.0) / 1e12
         roof = {"kernel": "sq_tc (tcgen05 split-BF16)", "bound": "tensor", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": profile_traffic("sq_tc_kernel", args.workload),
                 "peak_source": "measured sustained" if peaks else "fallback",
                 "algorithmic": f"8*N*n_kvec = 8*{n}*{n_dense} flops per launch"}
     elif sq_ms >= rdf_ms:
@@ -287,7 +301,7 @@ def run_ours(args, rank, world, local_rank):
         peak = peaks.get("hbm_gbs", 6650.0)
         achieved = alg / (rdf_ms / 1000.0) / 1e9
         roof = {"kernel": "rdf_pairs (cell list)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": profile_traffic("rdf_pairs_kernel", args.workload),
                 "algorithmic": f"16*N + 8*nit*lsmax = {alg:.0f} bytes per launch"}
     roof["kernels_ms"] = {"rdf_pairs": rdf_ms, "sq_main": sq_ms}
     edge_h = edge.cpu().numpy()
