@@ -178,6 +178,13 @@ TRJ_API int trj_sq_plan_info(const trj_sq_plan* plan, int64_t* n_dense, int64_t*
  * the run length, so longer runs trade accuracy for fewer drains; the default,
  * 256 atoms, keeps the per-shell error of an N = 1e6 frame below 1e-5. */
 TRJ_API int trj_sq_plan_set_flush(trj_sq_plan* plan, int atoms);
+/* Tensor-core tuning: evaluate pairs of tiles that share their nz range as one
+ * M = 256 contraction on a cluster of two CTAs (tcgen05 cta_group::2, each SM
+ * holding half of the shared operand and its running sum in shared memory) when
+ * enable != 0, or each tile on one CTA when 0 (the default, faster on the
+ * N = 1e6 benchmark frame).  Both give the same sums.  The pair form is used
+ * only where the device keeps clusters of two resident. */
+TRJ_API int trj_sq_plan_set_pairs(trj_sq_plan* plan, int enable);
 /* Replaces SQcalc (src/modules/sq.cuf:58-126; kernels sqfnD 523-591, sqfact
  * 372-454): adds, for every bin and species pair (a<=b, row ind_ij(a,b)-1),
  * sum over the bin's vectors of weight * Re(rho_a(k) conj(rho_b(k))) to

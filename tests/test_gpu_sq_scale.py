@@ -29,13 +29,14 @@ def c3():
     return fr, ks, sel, rho_o
 
 
-def _gpu_rho(fr, ks, method, flush=None):
+def _gpu_rho(fr, ks, method, flush=None, pairs=True):
     from trj_analysis_b200 import engine
     ctx = engine.Context(0)
     stage = engine.FrameStage(ctx, fr.n, 3)
     plan = engine.SqPlan(ctx, 3, ks, np.bincount(fr.types - 1, minlength=3))
     if flush:
         plan.set_flush(flush)
+    plan.set_pairs(pairs)
     out = plan.new_out()
     n = stage.upload_and_pack(fr.xyz, fr.types - 1, fr.box)
     plan.accumulate(stage.packed, n, fr.box, out, engine.METHODS[method])
@@ -58,12 +59,12 @@ def _shell_errors(rho_g, rho_o, ks, sel):
     return (np.abs(got - ref)[live] / scale[live]).max()
 
 
-@pytest.mark.parametrize("flush", [None, 128])
-def test_split_bf16_full_scale_within_1e5_per_shell(c3, flush):
+@pytest.mark.parametrize("flush,pairs", [(None, True), (None, False), (128, True)])
+def test_split_bf16_full_scale_within_1e5_per_shell(c3, flush, pairs):
     fr, ks, sel, rho_o = c3
-    rho_g = _gpu_rho(fr, ks, "split", flush)[:, sel]
+    rho_g = _gpu_rho(fr, ks, "split", flush, pairs)[:, sel]
     err = _shell_errors(rho_g, rho_o, ks, sel)
-    print(f"flush={flush}: max per-shell error {err:.3e}")
+    print(f"flush={flush} pairs={pairs}: max per-shell error {err:.3e}")
     assert err <= 1e-5
 
 

@@ -58,6 +58,7 @@ SIGNATURES = {
     "trj_sq_plan_create": (c_int, [vp, c_int, c_int64, vp, vp, vp, vp, c_int, P(c_int64), P(vp)]),
     "trj_sq_plan_info": (c_int, [vp, P(c_int64), P(c_int64), P(c_int64), P(c_int64)]),
     "trj_sq_plan_set_flush": (c_int, [vp, c_int]),
+    "trj_sq_plan_set_pairs": (c_int, [vp, c_int]),
     "trj_sq_accumulate": (c_int, [vp, vp, c_int64, P(c_float), c_int, vp, vp]),
     "trj_sq_rho": (c_int, [vp, vp, vp]),
     "trj_sq_plan_destroy": (c_int, [vp]),

@@ -65,6 +65,11 @@ constexpr int kMaxTileCols = 224;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kSumCol = 224;
 constexpr uint32_t kACol = 448;
+// CTA-pair form: accumulator at 0, four full-stage A buffers (32 columns hi, 32 lo) from 224; its
+// FP32 running sum lives in shared memory.
+constexpr uint32_t kPairACol = 224;
+constexpr int kPairABufs = 4;
+static_assert(kPairACol + 64 * kPairABufs <= kTmemCols, "pair TMEM layout");
 static_assert(kTcRows == 128, "one TMEM lane per A row");
 static_assert(kMaxTileCols <= kTcMaxCols, "tile width");
 
@@ -94,6 +99,33 @@ struct TcParams {
     unsigned* status;
 };
 
+// Two tiles sharing one B (the union of their nz spans): the leader CTA of a cluster holds the first
+// tile's 128 rows of the M = 256 accumulator, the peer the second's; each CTA holds half of B's rows.
+struct TcPairDev {
+    int tile[2];   // tile of the leader / the peer, -1 for none
+    int coff[2];   // accumulator column of each tile's first own column
+    int ncols;     // N of the pair: multiple of 32, <= kMaxTileCols
+    int brow;      // first Z-table row of the pair's B
+    int nx0[2], ny0[2];
+};
+
+struct Tc2Params {
+    const TcTile* tiles;
+    const TcPairDev* pairs;
+    const TcChunk* chunks;
+    const int32_t* cl_items;  // item ids (chunk * npairs + pair) of every cluster, concatenated
+    const int32_t* cl_off;    // nclusters + 1 offsets into cl_items
+    const uint2* uxy;
+    double* part;
+    int64_t acc_stride;
+    int npairs, nchunks;
+    int nstages;
+    int flush_stages;
+    int stage_bytes;
+    int bhalf;  // B rows per CTA of a stage buffer
+    unsigned* status;
+};
+
 struct TcState {
     int nz_min = 0, table_rows = 0;
     int64_t total_slots = 0;
@@ -114,6 +146,11 @@ struct TcState {
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
+    // CTA-pair (cta_group::2) form
+    int pairs_ok = 0, use_pairs = 0;  // pair form on request (slower than one CTA per tile at c3)
+    int npairs = 0, grid2 = 0, nstages2 = 2, stage_bytes2 = 0, smem_bytes2 = 0, bhalf = 0;
+    TcPairDev* pairs_dev = nullptr;
+    int32_t* sched2_dev = nullptr;
 };
 
 // ---- PTX wrappers ----------------------------------------------------------
@@ -618,6 +655,435 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
 }
 
+// ---- CTA-pair (cta_group::2) form -------------------------------------------
+// A cluster of two CTAs on a pair of SMs computes two tiles that share their B rows with one
+// M = 256 tcgen05.mma per K-step: the leader (cluster rank 0) issues the MMAs; each CTA builds
+// its own tile's A into its own TMEM and holds half of B's rows (N/2 each) in its own shared
+// memory, so each SM reads half the B bytes of the one-CTA form from L2.  Loads of both CTAs
+// complete on the leader's full_b barrier (TMA .cta_group::2 form, no multicast), the peer's
+// producers and epilogue arrive on the leader's barriers through their cluster addresses, and
+// the leader's commits arrive on both CTAs' barriers (multicast commit).
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(trj_smem_addr(p)), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void remote_arrive(uint32_t cluster_bar) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+
+// trj_mbar_wait with cluster-scope acquire (arrivals that come from the other CTA of the pair).
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity) {
+    const uint32_t addr = trj_smem_addr(bar);
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity), "r"(TRJ_SUSPEND_NS)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > TRJ_WAIT_CLOCKS) return false;
+    }
+}
+
+__device__ __forceinline__ bool timed_wait_cluster(uint64_t* bar, unsigned parity, unsigned* status) {
+    if (mbar_wait_cluster(bar, parity)) return true;
+    trj_raise(status, TRJ_DEV_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// 2-D TMA load into this CTA's shared memory whose completion is counted on the leader's barrier.
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, int c0, int c1,
+                                                 uint32_t leader_bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];" ::"r"(trj_smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(leader_bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_ts_pair(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+// Arrive on the barrier at this offset in both CTAs of the pair once the leader's MMAs so far are done.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+    const uint16_t mask = 3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            trj_smem_addr(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    sq_tc2_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64,
+                  Tc2Params p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    // full_b, full_a, acc_empty are used in the leader only; the others in both CTAs
+    __shared__ __align__(8) uint64_t full_b[kMaxStages], full_u[kMaxStages], empty_b[kMaxStages];
+    __shared__ __align__(8) uint64_t full_a[kPairABufs], empty_a[kPairABufs], xy_full[2], xy_empty[2], acc_full,
+        acc_empty, mma_done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag_s;
+    volatile int& abort_flag = abort_flag_s;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int cl = blockIdx.x >> 1;
+    const int NS = p.nstages;
+    const int F = p.flush_stages;
+    const int item0 = p.cl_off[cl], item1 = p.cl_off[cl + 1];
+    auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
+    auto xy_ptr = [&](int b) { return reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
+    // FP32 running sum of this CTA's 128 accumulator rows: [16-column chunk][4 x 4 columns][row] float4
+    float4* sums = reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + 2 * kXyBytes);
+
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < NS; ++s) {
+            trj_mbar_init(&full_b[s], 1);
+            trj_mbar_init(&full_u[s], 1);
+            trj_mbar_init(&empty_b[s], 1);
+        }
+        for (int b = 0; b < kPairABufs; ++b) {
+            trj_mbar_init(&full_a[b], 2 * kBuildWarps);
+            trj_mbar_init(&empty_a[b], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            trj_mbar_init(&xy_full[b], kXyWarps);
+            trj_mbar_init(&xy_empty[b], kBuildWarps);
+        }
+        trj_mbar_init(&acc_full, 1);
+        trj_mbar_init(&acc_empty, 2 * kEpiWarps);
+        trj_mbar_init(&mma_done, 1);
+        trj_fence_mbar_init();
+    }
+    if (warp == kMmaWarp) {  // the same warp of both CTAs allocates the pair's TMEM
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         trj_smem_addr(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync_all();  // barrier inits and TMEM of both CTAs visible to both
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == kTmaWarp) {
+        if (lane == 0) {
+            int slot = 0, issued = 0;
+            unsigned phase = 0;
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cl_items[li];
+                const TcPairDev P = p.pairs[it % p.npairs];
+                const TcChunk C = p.chunks[it / p.npairs];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const int half = P.ncols / 2;                 // B rows of this CTA
+                const int row0 = P.brow + (int)rank * half;
+                const int n64 = half / 64;
+                for (int s = 0; s < nst; ++s) {
+                    if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t* bh = stage_ptr(slot);
+                    uint8_t* bl = bh + p.bhalf * 128;
+                    uint8_t* ux = bl + p.bhalf * 128;
+                    const uint32_t lead_full = cluster_addr(&full_b[slot], 0);
+                    if (leader) trj_mbar_arrive_expect_tx(&full_b[slot], (unsigned)(P.ncols * 256));
+                    trj_mbar_arrive_expect_tx(&full_u[slot], (unsigned)kUxyBytes);
+                    const int slot0 = C.slot0 + s * kStageSlots;
+                    const int k0 = 2 * slot0;
+                    int r = 0;
+                    for (int b = 0; b < n64; ++b, r += 64) {
+                        tma_load_2d_pair(bh + r * 128, &map_hi64, k0, row0 + r, lead_full);
+                        tma_load_2d_pair(bl + r * 128, &map_lo64, k0, row0 + r, lead_full);
+                    }
+                    for (; r < half; r += 16) {
+                        tma_load_2d_pair(bh + r * 128, &map_hi, k0, row0 + r, lead_full);
+                        tma_load_2d_pair(bl + r * 128, &map_lo, k0, row0 + r, lead_full);
+                    }
+                    trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_u[slot]);
+                    ++issued;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            // copies issued last land before the CTA may exit (the leader's full_b counts both CTAs')
+            for (int q = 0; q < NS && q < issued; ++q) {
+                if (--slot < 0) {
+                    slot = NS - 1;
+                    phase ^= 1;
+                }
+                trj_mbar_wait(&full_u[slot], phase);
+                if (leader) mbar_wait_cluster(&full_b[slot], phase);
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        if (lane == 0 && leader) {
+            const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
+            const uint64_t b_lo = (uint64_t)((p.bhalf * 128) >> 4);
+            const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
+            int slot = 0, fg = 0, ab = 0;
+            unsigned phase = 0, aphase = 0;
+            uint64_t bh = b0desc;
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cl_items[li];
+                const TcPairDev P = p.pairs[it % p.npairs];
+                const TcChunk C = p.chunks[it / p.npairs];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(P.ncols >> 3) << 17) |
+                                       ((uint32_t)(256 >> 4) << 24);
+                int rs = 0;
+                for (int s = 0; s < nst; ++s) {
+                    const bool first = rs == 0;
+                    if (first && fg >= 1 && !timed_wait_cluster(&acc_empty, (fg - 1) & 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    if (!timed_wait_cluster(&full_b[slot], phase, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    const uint64_t bl = bh + b_lo;
+                    if (!timed_wait_cluster(&full_a[ab], aphase, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t ah = tmem + kPairACol + (uint32_t)(64 * ab), al = ah + 32;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        mma_ts_pair(tmem, ah + 8 * kk, bh + 2 * kk, idesc, (first && kk == 0) ? 0u : 1u);
+                        mma_ts_pair(tmem, ah + 8 * kk, bl + 2 * kk, idesc, 1u);
+                        mma_ts_pair(tmem, al + 8 * kk, bh + 2 * kk, idesc, 1u);
+                    }
+                    mma_commit_pair(&empty_a[ab]);
+                    mma_commit_pair(&empty_b[slot]);
+                    if (++rs == F || s == nst - 1) {
+                        mma_commit_pair(&acc_full);
+                        ++fg;
+                        rs = 0;
+                    }
+                    if (++ab == kPairABufs) {
+                        ab = 0;
+                        aphase ^= 1;
+                    }
+                    bh += b_step;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                        bh = b0desc;
+                    }
+                }
+            }
+            mma_commit_pair(&mma_done);  // every MMA of the pair has completed -> both CTAs
+        }
+        if (lane == 0) trj_mbar_wait(&mma_done, 0);
+    } else if (warp >= kEpiWarp0) {
+        const int q4 = warp & 3;
+        const int c0 = 16 * ((warp - kEpiWarp0) >> 2);
+        const int row = 32 * q4 + lane;
+        const uint32_t lanes = (uint32_t)(32 * q4) << 16;
+        const uint32_t lead_acc_empty = cluster_addr(&acc_empty, 0);
+        int fg = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cl_items[li];
+            const TcPairDev P = p.pairs[it % p.npairs];
+            const int chunk = it / p.npairs;
+            const TcChunk C = p.chunks[chunk];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const int nflush = (nst + F - 1) / F;
+            const int tile = P.tile[rank];
+            const int coff = P.coff[rank];
+            int own = 0;
+            double* dst = nullptr;
+            if (tile >= 0) {
+                const TcTile T = p.tiles[tile];
+                own = T.ncols;
+                dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
+            }
+            for (int f = 0; f < nflush; ++f, ++fg) {
+                const bool ok = trj_mbar_wait(&acc_full, fg & 1);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const bool last = f == nflush - 1;
+                const uint32_t ta = tmem + lanes;
+                for (int c = c0; c < P.ncols; c += 32) {
+                    uint32_t a0[16];
+                    tmem_ld16_nowait(ta + (uint32_t)c, a0);
+                    tmem_wait_ld();
+                    float4* sp = sums + (size_t)(c >> 4) * 4 * 128 + row;  // this row's 4 float4 of the chunk
+#pragma unroll
+                    for (int k4 = 0; k4 < 4; ++k4) {
+                        float4 v = make_float4(__uint_as_float(a0[4 * k4]), __uint_as_float(a0[4 * k4 + 1]),
+                                               __uint_as_float(a0[4 * k4 + 2]), __uint_as_float(a0[4 * k4 + 3]));
+                        if (f > 0) {
+                            const float4 o = sp[k4 * 128];
+                            v.x = __fadd_rn(v.x, o.x), v.y = __fadd_rn(v.y, o.y);
+                            v.z = __fadd_rn(v.z, o.z), v.w = __fadd_rn(v.w, o.w);
+                        }
+                        if (last) {
+                            if (dst) {
+                                const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                                for (int e = 0; e < 4; ++e) {
+                                    const int oc = c + 4 * k4 + e - coff;  // own column
+                                    if (oc >= 0 && oc < own) dst[(int64_t)oc * 128] = (double)vv[e];
+                                }
+                            }
+                        } else {
+                            sp[k4 * 128] = v;
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    if (leader) trj_mbar_arrive(&acc_empty);
+                    else remote_arrive(lead_acc_empty);
+                }
+            }
+        }
+    } else if (warp >= kXyWarp0) {
+        const int xt = tid - kXyWarp0 * 32;
+        int sg = 0, slot = 0;
+        unsigned phase = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cl_items[li];
+            const TcPairDev P = p.pairs[it % p.npairs];
+            const TcChunk C = p.chunks[it / p.npairs];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const int nx0 = P.nx0[rank], ny0 = P.ny0[rank];
+            for (int s = 0; s < nst; ++s, ++sg) {
+                const int xb = sg & 1;
+                bool ok = trj_mbar_wait(&full_u[slot], phase);
+                ok = ok && trj_mbar_wait(&xy_empty[xb], ((sg >> 1) & 1) ^ 1);
+                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bhalf * 128);
+                float4* xs = xy_ptr(xb);
+                float4* ys = xs + kStageSlots * kTcTileNx;
+                for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32) {
+                    const float2 f = phase_factor((unsigned)(nx0 + (e & 15)) * u[e >> 4].x);
+                    xs[e] = make_float4(f.x, f.x, f.y, f.y);
+                }
+                for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32) {
+                    const float2 f = phase_factor((unsigned)(ny0 + (e & 7)) * u[e >> 3].y);
+                    ys[e] = make_float4(f.x, f.y, -f.y, f.x);
+                }
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
+                if (++slot == NS) {
+                    slot = 0;
+                    phase ^= 1;
+                }
+            }
+        }
+    } else {
+        // ---- A builders: warp w writes TMEM lanes 32*(w%4).. and the K-columns of atoms
+        //      [16*(w/4), 16*(w/4) + 16) of the stage's A buffer, arriving on the leader's full_a ----
+        const int q = warp & 3, g = warp >> 2;
+        const int m = 32 * q + lane;
+        const int nxl = m & 15, nyl = m >> 4;
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
+        int sg = 0, ab = 0;
+        unsigned aphase = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cl_items[li];
+            const TcChunk C = p.chunks[it / p.npairs];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            for (int s = 0; s < nst && !stop; ++s, ++sg) {
+                const int xb = sg & 1;
+                bool ok = trj_mbar_wait(&xy_full[xb], (sg >> 1) & 1);
+                ok = ok && trj_mbar_wait(&empty_a[ab], aphase ^ 1);
+                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const ulonglong2* xs = reinterpret_cast<const ulonglong2*>(xy_ptr(xb));
+                const ulonglong2* ys = xs + kStageSlots * kTcTileNx;
+                const uint32_t ta = tmem + lanes + kPairACol + (uint32_t)(64 * ab + 16 * g);
+#pragma unroll
+                for (int h8 = 0; h8 < 2; ++h8) {
+                    uint32_t hw[8], lw[8];
+#pragma unroll
+                    for (int jj = 0; jj < 8; ++jj) {
+                        const int j = 16 * g + 8 * h8 + jj;
+                        product_split(xs[j * kTcTileNx + nxl], ys[j * kTcTileNy + nyl], hw[jj], lw[jj]);
+                    }
+                    tmem_st8(ta + 8 * h8, hw);
+                    tmem_st8(ta + 32 + 8 * h8, lw);
+                }
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    trj_mbar_arrive(&xy_empty[xb]);
+                    if (leader) trj_mbar_arrive(&full_a[ab]);
+                    else remote_arrive(cluster_addr(&full_a[ab], 0));
+                }
+                if (++ab == kPairABufs) {
+                    ab = 0;
+                    aphase ^= 1;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();  // neither CTA leaves while the other may still reach its barriers or TMEM
+    if (warp == kMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
 // tc_out[tile][a][col][row] = sum over species a's chunks (fixed order) of the FP64 blocks.
 // Grid (element blocks, tile, species): one thread per output element.
 __global__ void tc_reduce_kernel(const double* __restrict__ part, int64_t acc_stride, const TcTile* __restrict__ tiles,
@@ -672,10 +1138,126 @@ void trj_sq_tc_release(trj_sq_plan* plan) {
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (!st) return;
     void* ptrs[] = {st->sched_dev, st->tiles_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
-                    st->tab_hi,    st->tab_lo,    st->uxy,        st->part};
+                    st->tab_hi,    st->tab_lo,    st->uxy,        st->part,           st->pairs_dev,
+                    st->sched2_dev};
     for (void* q : ptrs) trj_dev_free(plan->ctx, q);
     delete st;
     plan->tc_state = nullptr;
+}
+
+// CTA-pair form: pairs of tiles sharing their B rows, the per-cluster schedule and the launch
+// shape.  Leaves pairs_ok = 0 (the one-CTA form runs) when the device cannot keep clusters of two
+// resident with this shared-memory size.
+static int prepare_pairs(trj_sq_plan* plan, TcState* st, const std::vector<TcTile>& tt) {
+    trj_ctx* ctx = plan->ctx;
+    const int ntiles = (int)tt.size();
+    const int nz_min = st->nz_min;
+    // tiles by descending span, then origin, so that neighbours have equal or nested nz ranges
+    std::vector<int> ord(ntiles);
+    for (int i = 0; i < ntiles; ++i) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+        if (tt[a].ncols != tt[b].ncols) return tt[a].ncols > tt[b].ncols;
+        return plan->tiles[a].nz0 < plan->tiles[b].nz0;
+    });
+    std::vector<TcPairDev> pairs;
+    for (size_t k = 0; k < ord.size();) {
+        const int a = ord[k];
+        const int za0 = plan->tiles[a].nz0, za1 = za0 + tt[a].ncols / 2 - 1;
+        int b = k + 1 < ord.size() ? ord[k + 1] : -1;
+        int z0 = za0, z1 = za1;
+        if (b >= 0) {
+            const int zb0 = plan->tiles[b].nz0, zb1 = zb0 + tt[b].ncols / 2 - 1;
+            const int u0 = std::min(za0, zb0), u1 = std::max(za1, zb1);
+            if (2 * (u1 - u0 + 1) <= kMaxTileCols) {
+                z0 = u0;
+                z1 = u1;
+            } else {
+                b = -1;
+            }
+        }
+        TcPairDev P;
+        P.tile[0] = a;
+        P.tile[1] = b;
+        P.ncols = (2 * (z1 - z0 + 1) + 31) / 32 * 32;
+        P.brow = 2 * (z0 - nz_min);
+        P.coff[0] = 2 * (za0 - z0);
+        P.coff[1] = b >= 0 ? 2 * (plan->tiles[b].nz0 - z0) : 0;
+        P.nx0[0] = tt[a].nx0;
+        P.ny0[0] = tt[a].ny0;
+        P.nx0[1] = b >= 0 ? tt[b].nx0 : tt[a].nx0;
+        P.ny0[1] = b >= 0 ? tt[b].ny0 : tt[a].ny0;
+        if (P.ncols > kMaxTileCols) return TRJ_OK;  // cannot happen: spans are <= kMaxTileCols / 2
+        pairs.push_back(P);
+        k += b >= 0 ? 2 : 1;
+    }
+    st->npairs = (int)pairs.size();
+    int bmax2 = 0;
+    for (const TcPairDev& P : pairs) bmax2 = std::max(bmax2, P.ncols);
+    st->bhalf = bmax2 / 2;
+    st->stage_bytes2 = (2 * st->bhalf * 128 + kUxyBytes + 1023) / 1024 * 1024;
+    const int sum_bytes = bmax2 * 128 * 4;  // FP32 running sum of 128 rows x N
+    const int avail = (int)ctx->smem_optin - 2048 - 2 * kXyBytes - sum_bytes;
+    st->nstages2 = std::min(kMaxStages, avail / st->stage_bytes2);
+    if (st->nstages2 < 2) return TRJ_OK;
+    st->smem_bytes2 = st->nstages2 * st->stage_bytes2 + 2 * kXyBytes + sum_bytes + 1024;
+    // resident clusters of two with this shared-memory size
+    if (cudaFuncSetAttribute(sq_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, st->smem_bytes2) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return TRJ_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(ctx->sm_count & ~1));
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = (size_t)st->smem_bytes2;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, (void*)sq_tc2_kernel, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        return TRJ_OK;
+    }
+    const int64_t nchunks = (int64_t)st->chunks.size();
+    const int64_t nitems = (int64_t)st->npairs * nchunks;
+    ncl = (int)std::min<int64_t>(ncl, nitems);
+    st->grid2 = 2 * ncl;
+    // windowed longest-first schedule over clusters (as for the one-CTA form)
+    std::vector<std::vector<int32_t>> lists(ncl);
+    std::vector<std::pair<double, int>> heap;
+    for (int b = 0; b < ncl; ++b) heap.push_back({0.0, b});
+    auto cmp = [](const std::pair<double, int>& a, const std::pair<double, int>& b) { return a > b; };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    std::vector<std::pair<double, int32_t>> win;
+    for (int64_t w0 = 0; w0 < nitems; w0 += ncl) {
+        win.clear();
+        for (int64_t it = w0; it < std::min<int64_t>(nitems, w0 + ncl); ++it) {
+            const TcChunk& C = st->chunks[it / st->npairs];
+            const double stages = (double)(C.slot1 - C.slot0) / kStageSlots;
+            win.push_back({stages * (pairs[it % st->npairs].ncols + 24.0), (int32_t)it});
+        }
+        std::stable_sort(win.begin(), win.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        for (const auto& it : win) {
+            std::pop_heap(heap.begin(), heap.end(), cmp);
+            heap.back().first += it.first;
+            lists[heap.back().second].push_back(it.second);
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+    }
+    std::vector<int32_t> sched(ncl + 1, 0);
+    for (int b = 0; b < ncl; ++b) sched[b + 1] = sched[b] + (int32_t)lists[b].size();
+    for (int b = 0; b < ncl; ++b) sched.insert(sched.end(), lists[b].begin(), lists[b].end());
+    if (trj_dev_alloc(ctx, (void**)&st->pairs_dev, sizeof(TcPairDev) * pairs.size()) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->sched2_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: pair schedule");
+    cudaMemcpy(st->pairs_dev, pairs.data(), sizeof(TcPairDev) * pairs.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(st->sched2_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
+    st->pairs_ok = 1;
+    return TRJ_OK;
 }
 
 int trj_sq_tc_prepare(trj_sq_plan* plan) {
@@ -823,7 +1405,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
-    return TRJ_OK;
+    return prepare_pairs(plan, st, tt);
 }
 
 int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
@@ -855,14 +1437,58 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
-    plan->timer.begin(ctx, s);
-    sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, P);
-    plan->timer.end(ctx, s);
+    if (st->pairs_ok && st->use_pairs) {
+        Tc2Params Q;
+        Q.tiles = st->tiles_dev;
+        Q.pairs = st->pairs_dev;
+        Q.chunks = st->chunks_dev;
+        Q.cl_off = st->sched2_dev;
+        Q.cl_items = st->sched2_dev + st->grid2 / 2 + 1;
+        Q.uxy = st->uxy;
+        Q.part = st->part;
+        Q.acc_stride = st->acc_stride;
+        Q.npairs = st->npairs;
+        Q.nchunks = (int)st->chunks.size();
+        Q.nstages = st->nstages2;
+        Q.flush_stages = st->flush_stages;
+        Q.stage_bytes = st->stage_bytes2;
+        Q.bhalf = st->bhalf;
+        Q.status = ctx->status_dev;
+        TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               st->smem_bytes2));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)st->grid2);
+        cfg.blockDim = dim3(kTcThreads);
+        cfg.dynamicSmemBytes = (size_t)st->smem_bytes2;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        plan->timer.begin(ctx, s);
+        TRJ_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, sq_tc2_kernel, st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, Q));
+        plan->timer.end(ctx, s);
+    } else {
+        plan->timer.begin(ctx, s);
+        sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
+                                                                  st->map_lo64, P);
+        plan->timer.end(ctx, s);
+    }
     const dim3 rg((unsigned)((st->bmax * 128 + 255) / 256), (unsigned)plan->tiles.size(), (unsigned)plan->nsp);
     tc_reduce_kernel<<<rg, 256, 0, s>>>(st->part, st->acc_stride, st->tiles_dev, plan->tiles_dev, st->chunk_begin_dev,
                                         plan->nsp, plan->tc_out_dev);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_plan_set_pairs(trj_sq_plan* plan, int enable) {
+    if (!plan) return TRJ_ERR_INVALID;
+    TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
+    if (st) st->use_pairs = enable ? 1 : 0;
     return TRJ_OK;
 }
 

@@ -156,8 +156,12 @@ class SqPlan:
         return torch.zeros((self.kset.nbins, self.nit), dtype=torch.float64, device=self.ctx.torch_device)
 
     def set_flush(self, atoms: int) -> None:
-        """Atoms accumulated in FP32 by the tensor-core path between FP64 drains."""
+        """Atoms the tensor cores accumulate in one FP32 run before it is added into the running sum."""
         check(self.ctx.lib.trj_sq_plan_set_flush(self.h, int(atoms)), self.ctx.h, "trj_sq_plan_set_flush")
+
+    def set_pairs(self, enable: bool) -> None:
+        """Tensor-core tiles in CTA pairs (one M = 256 contraction per two tiles) or one per CTA."""
+        check(self.ctx.lib.trj_sq_plan_set_pairs(self.h, 1 if enable else 0), self.ctx.h, "trj_sq_plan_set_pairs")
 
     def accumulate(self, packed: torch.Tensor, n: int, box, out: torch.Tensor, method: int, stream=None) -> None:
         assert out.dtype == torch.float64 and out.shape == (self.kset.nbins, self.nit)
