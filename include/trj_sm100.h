@@ -109,6 +109,16 @@ TRJ_API int64_t trj_ctx_launches(const trj_ctx* ctx);
 TRJ_API int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
                    int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
                    void* stream);
+/* trj_frame_pack for frames that carry per-atom charges (the NetCDF variable
+ * "q", read as default real by src/core/netcdf.f90:404-408): the charges are
+ * written in the same order as the atoms (netcdf.f90:656-658).
+ *   charge_dev         n float (device)
+ *   charge_packed_dev  n float out: charge of packed atom i
+ * Other arguments and results as trj_frame_pack. */
+TRJ_API int trj_frame_pack_charges(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
+                                   const float* charge_dev, int64_t n, int nsp, const float box[3],
+                                   float* packed_dev, float* charge_packed_dev, int64_t* counts_dev,
+                                   void* stream);
 
 /* trj_frame_pack without any device allocation (this entry point has no
  * counterpart in the reference).  It is for callers that may not have the
@@ -152,6 +162,18 @@ TRJ_API int trj_rdf_plan_info(const trj_rdf_plan* plan, int* lsmax, int* nit, in
  * packed_dev: output of trj_frame_pack.  box: this frame's box. */
 TRJ_API int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int64_t n, const float box[3],
                        uint64_t* hist_dev, uint64_t* edge_dev, void* stream);
+/* trj_rdf_accumulate with the charge-weighted histogram of the reference's
+ * ex_qc branch (rdf.cuf:225-228, 469-472, 271-274): besides the counts, every
+ * counted pair adds q_a*q_b to its bin, and per frame
+ *   gqq_dev[bin-1] += (sum of q_a*q_b in the bin) / avq2,  avq2 = sum(q^2)/N
+ * (gqq_dev: double [lsmax]; avq2 rounded to FP32 as the reference's variable).
+ * charge_packed_dev: the charges written by trj_frame_pack_charges.  Products
+ * and sums are FP64 (the reference adds FP32 products with FP32 atomics).  An
+ * all-zero charge set gives avq2 = 0 and non-finite gqq, as in the reference.
+ * The first charged call on a plan allocates 4*n_max + 8*lsmax bytes. */
+TRJ_API int trj_rdf_accumulate_charged(trj_rdf_plan* plan, const float* packed_dev, const float* charge_packed_dev,
+                                       int64_t n, const float box[3], uint64_t* hist_dev, uint64_t* edge_dev,
+                                       double* gqq_dev, void* stream);
 /* Duration (ms) of the last cell-pair kernel launch; needs trj_ctx_set_timing(ctx, 1). */
 TRJ_API int trj_rdf_kernel_ms(trj_rdf_plan* plan, float* ms);
 TRJ_API int trj_rdf_plan_destroy(trj_rdf_plan* plan);
@@ -192,6 +214,21 @@ TRJ_API int trj_sq_plan_set_pairs(trj_sq_plan* plan, int enable);
  * method: TRJ_SQ_PLAIN_FP32 or TRJ_SQ_SPLIT_BF16X3. */
 TRJ_API int trj_sq_accumulate(trj_sq_plan* plan, const float* packed_dev, int64_t n, const float box[3],
                       int method, double* out_dev, void* stream);
+/* Plan for frames with charges (the reference's ex_qc S(Q), sq.cuf:67, 569-588,
+ * 143-145): arguments as trj_sq_plan_create (nsp <= 15), and the plan adds a
+ * species nsp, the charge density rho_q(k) = sum_j q_j exp(i k.r_j) over every
+ * atom.  Its accumulate output has nit = (nsp+1)(nsp+2)/2 rows: the species
+ * pairs, the cross rows (a, nsp) and, in the last row (nsp, nsp), the sums of
+ * w |rho_q(k)|^2, the reference's sqfq_d before its division by
+ * avq2 = sum(q^2)/N.  trj_sq_rho gives nsp+1 densities. */
+TRJ_API int trj_sq_plan_create_charged(trj_ctx* ctx, int nsp, int64_t nvec, const int32_t* vec_host,
+                                       const int32_t* bin_host, const double* weight_host,
+                                       const uint8_t* dense_host, int nbins, const int64_t* species_counts,
+                                       trj_sq_plan** out);
+/* trj_sq_accumulate for a charged plan; charge_packed_dev as written by
+ * trj_frame_pack_charges.  A charged plan accepts only this call. */
+TRJ_API int trj_sq_accumulate_charged(trj_sq_plan* plan, const float* packed_dev, const float* charge_packed_dev,
+                                      int64_t n, const float box[3], int method, double* out_dev, void* stream);
 /* rho_a(k) of the last accumulate, FP64, [nsp][nvec][2] in the caller's vector order. */
 TRJ_API int trj_sq_rho(trj_sq_plan* plan, double* rho_dev, void* stream);
 /* Duration (ms) of the last main S(Q) kernel launch (tcgen05 contraction for

@@ -15,6 +15,8 @@
  *   histogram layout     src/modules/rdf.cuf:51-66     (lsmax = nint(rcrdf/deltar)+1)
  *   S(Q) direct sum      src/modules/sq.cuf:523-591    (sqfnD; FP32 phase, FP64 sums)
  *                        src/modules/sq.cuf:372-454    (sqfact; axis vectors)
+ *   charge products      src/modules/rdf.cuf:469-472   (gqq_d(ind) += qci*qcj, ex_qc)
+ *   charge density       src/modules/sq.cuf:569-573    (sumqcx += qci*cfk, ex_qc)
  *
  * The exact S(Q) oracle is FP64 throughout: phases from the fractional
  * coordinate s = x/L in FP64, n.s reduced mod 1 in FP64, sin/cos in FP64.
@@ -76,9 +78,9 @@ typedef struct {
     uint64_t counted;    /* pairs counted into the histogram               */
 } orc_edge_stats;
 
-/* One unordered pair: accumulate its count and edge statistics. */
-static inline void do_pair(const float* pi, int si, const float* pj, int sj,
-                           const orc_rdf_params* p, uint64_t* hist, orc_edge_stats* e) {
+/* One unordered pair: accumulate its count and edge statistics; returns its bin (0: not counted). */
+static inline int do_pair(const float* pi, int si, const float* pj, int sj,
+                          const orc_rdf_params* p, uint64_t* hist, orc_edge_stats* e) {
     float xd = pj[0] - pi[0];
     float yd = pj[1] - pi[1];
     float zd = pj[2] - pi[2];
@@ -88,7 +90,7 @@ static inline void do_pair(const float* pi, int si, const float* pj, int sj,
     float x2 = xd * xd, y2 = yd * yd, z2 = zd * zd;
     float rr2 = (x2 + y2) + z2;
     /* Anything at or beyond 1.001*side2 cannot reach the cutoff by an ulp or by FMA. */
-    if (!(rr2 < p->side2 * 1.001f)) return;
+    if (!(rr2 < p->side2 * 1.001f)) return 0;
     int o = pair_outcome(rr2, p);
     if (o) {
         hist[(size_t)pair_row(si, sj, p->nsp) * p->lsmax + (o - 1)] += 1;
@@ -99,6 +101,12 @@ static inline void do_pair(const float* pi, int si, const float* pj, int sj,
     if (olo != o || ohi != o) e->edge_ulp += 1;
     float rr2f = fmaf(zd, zd, fmaf(yd, yd, x2));
     if (pair_outcome(rr2f, p) != o) e->edge_fma += 1;
+    return o;
+}
+
+/* Charge product of a counted pair, added in FP64 (the product of two FP32 values is exact). */
+static inline void add_charge(int o, const float* q, int64_t i, int64_t j, double* gq) {
+    if (o && q) gq[o - 1] += (double)q[i] * (double)q[j];
 }
 
 /*
@@ -107,9 +115,9 @@ static inline void do_pair(const float* pi, int si, const float* pj, int sj,
  * sp:  N species indices (0-based).
  * hist: nit x lsmax uint64, accumulated (+=).
  */
-ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
-                                 const float box[3], float side2, float deltar,
-                                 int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
+static void rdf_allpairs_impl(const float* pos, const int32_t* sp, const float* q, int64_t n,
+                              const float box[3], float side2, float deltar, int lsmax, int nsp,
+                              uint64_t* hist, uint64_t* edge3, double* gqq) {
     orc_rdf_params p = {{box[0], box[1], box[2]}, side2, deltar, lsmax, nsp, g_floor_bins};
     int nit = nsp * (nsp + 1) / 2;
     int nthr = 1;
@@ -118,6 +126,7 @@ ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
 #endif
     size_t hsz = (size_t)nit * lsmax;
     uint64_t* priv = (uint64_t*)calloc((size_t)nthr * hsz, sizeof(uint64_t));
+    double* qpriv = (double*)calloc((size_t)nthr * lsmax, sizeof(double));
     orc_edge_stats* es = (orc_edge_stats*)calloc((size_t)nthr, sizeof(orc_edge_stats));
 #pragma omp parallel
     {
@@ -126,19 +135,29 @@ ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
         t = omp_get_thread_num();
 #endif
         uint64_t* h = priv + (size_t)t * hsz;
+        double* gq = qpriv + (size_t)t * lsmax;
 #pragma omp for schedule(dynamic, 64)
         for (int64_t i = 0; i < n; ++i)
             for (int64_t j = i + 1; j < n; ++j)
-                do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]);
+                add_charge(do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]), q, i, j, gq);
     }
     for (int t = 0; t < nthr; ++t) {
         for (size_t k = 0; k < hsz; ++k) hist[k] += priv[(size_t)t * hsz + k];
+        if (gqq)
+            for (int k = 0; k < lsmax; ++k) gqq[k] += qpriv[(size_t)t * lsmax + k];
         edge3[0] += es[t].edge_ulp;
         edge3[1] += es[t].edge_fma;
         edge3[2] += es[t].counted;
     }
     free(priv);
+    free(qpriv);
     free(es);
+}
+
+ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
+                                 const float box[3], float side2, float deltar,
+                                 int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
+    rdf_allpairs_impl(pos, sp, NULL, n, box, side2, deltar, lsmax, nsp, hist, edge3, NULL);
 }
 
 /*
@@ -150,26 +169,40 @@ ORC_EXPORT void orc_rdf_allpairs(const float* pos, const int32_t* sp, int64_t n,
  */
 /* Same, restricted to home atoms i in [i0, i1) (pairs (i, j>i)); used to time a bounded
  * sample of a large frame for the CPU baseline.  i0=0, i1=n is the whole frame. */
-ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t n,
-                                    const float box[3], float side2, float deltar,
-                                    int lsmax, int nsp, uint64_t* hist, uint64_t* edge3,
-                                    int64_t i0, int64_t i1);
+static void rdf_cells_impl(const float* pos, const int32_t* sp, const float* q, int64_t n,
+                           const float box[3], float side2, float deltar, int lsmax, int nsp,
+                           uint64_t* hist, uint64_t* edge3, double* gqq, int64_t i0, int64_t i1);
 
 ORC_EXPORT void orc_rdf_cells(const float* pos, const int32_t* sp, int64_t n,
                               const float box[3], float side2, float deltar,
                               int lsmax, int nsp, uint64_t* hist, uint64_t* edge3) {
-    orc_rdf_cells_range(pos, sp, n, box, side2, deltar, lsmax, nsp, hist, edge3, 0, n);
+    rdf_cells_impl(pos, sp, NULL, n, box, side2, deltar, lsmax, nsp, hist, edge3, NULL, 0, n);
 }
 
 ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t n,
                                     const float box[3], float side2, float deltar,
                                     int lsmax, int nsp, uint64_t* hist, uint64_t* edge3,
                                     int64_t i0, int64_t i1) {
+    rdf_cells_impl(pos, sp, NULL, n, box, side2, deltar, lsmax, nsp, hist, edge3, NULL, i0, i1);
+}
+
+/* Counts plus gqq[bin-1] += sum over counted pairs of q_i*q_j (FP64, not divided by avq2);
+ * cells != 0 takes the linked-cell sweep. */
+ORC_EXPORT void orc_rdf_charged(const float* pos, const int32_t* sp, const float* q, int64_t n,
+                                const float box[3], float side2, float deltar, int lsmax, int nsp,
+                                uint64_t* hist, uint64_t* edge3, double* gqq, int cells) {
+    if (cells) rdf_cells_impl(pos, sp, q, n, box, side2, deltar, lsmax, nsp, hist, edge3, gqq, 0, n);
+    else rdf_allpairs_impl(pos, sp, q, n, box, side2, deltar, lsmax, nsp, hist, edge3, gqq);
+}
+
+static void rdf_cells_impl(const float* pos, const int32_t* sp, const float* q, int64_t n,
+                           const float box[3], float side2, float deltar, int lsmax, int nsp,
+                           uint64_t* hist, uint64_t* edge3, double* gqq, int64_t i0, int64_t i1) {
     double rc = sqrt((double)side2) * (1.0 + 1.0 / 1024.0);
     int nc[3];
     for (int d = 0; d < 3; ++d) {
         nc[d] = (int)floor((double)box[d] / rc);
-        if (nc[d] < 3) { orc_rdf_allpairs(pos, sp, n, box, side2, deltar, lsmax, nsp, hist, edge3); return; }
+        if (nc[d] < 3) { rdf_allpairs_impl(pos, sp, q, n, box, side2, deltar, lsmax, nsp, hist, edge3, gqq); return; }
     }
     int64_t ncell = (int64_t)nc[0] * nc[1] * nc[2];
     int64_t* head = (int64_t*)malloc(sizeof(int64_t) * ncell);
@@ -200,6 +233,7 @@ ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t
 #endif
     size_t hsz = (size_t)nit * lsmax;
     uint64_t* priv = (uint64_t*)calloc((size_t)nthr * hsz, sizeof(uint64_t));
+    double* qpriv = (double*)calloc((size_t)nthr * lsmax, sizeof(double));
     orc_edge_stats* es = (orc_edge_stats*)calloc((size_t)nthr, sizeof(orc_edge_stats));
 #pragma omp parallel
     {
@@ -208,6 +242,7 @@ ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t
         t = omp_get_thread_num();
 #endif
         uint64_t* h = priv + (size_t)t * hsz;
+        double* gq = qpriv + (size_t)t * lsmax;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t i = i0; i < i1; ++i) {
             for (int dx = -1; dx <= 1; ++dx)
@@ -218,17 +253,22 @@ ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t
                         int cz = (cellof[3 * i + 2] + dz + nc[2]) % nc[2];
                         int64_t c = ((int64_t)cx * nc[1] + cy) * nc[2] + cz;
                         for (int64_t j = head[c]; j >= 0; j = next[j])
-                            if (j > i) do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]);
+                            if (j > i)
+                                add_charge(do_pair(pos + 3 * i, sp[i], pos + 3 * j, sp[j], &p, h, &es[t]), q, i, j,
+                                           gq);
                     }
         }
     }
     for (int t = 0; t < nthr; ++t) {
         for (size_t k = 0; k < hsz; ++k) hist[k] += priv[(size_t)t * hsz + k];
+        if (gqq)
+            for (int k = 0; k < lsmax; ++k) gqq[k] += qpriv[(size_t)t * lsmax + k];
         edge3[0] += es[t].edge_ulp;
         edge3[1] += es[t].edge_fma;
         edge3[2] += es[t].counted;
     }
     free(priv);
+    free(qpriv);
     free(es);
     free(head);
     free(next);
@@ -248,8 +288,24 @@ ORC_EXPORT void orc_rdf_cells_range(const float* pos, const int32_t* sp, int64_t
  * axis is computed by a direct FP64 sincos of the reduced fraction, and the
  * 3-factor product is taken in FP64.
  */
+static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int64_t* sp_off, int nsp,
+                          const float box[3], int64_t nvec, const int32_t* vec, double* rho);
+
 ORC_EXPORT void orc_rho_fp64(const float* pos, int64_t n, const int64_t* sp_off, int nsp,
                              const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
+    rho_fp64_impl(pos, NULL, n, sp_off, nsp, box, nvec, vec, rho);
+}
+
+/* Weighted density sum_{j in a} w_j exp(i 2 pi n_v . s_j); with every atom in one range and
+ * w = charges this is the charge density rho_q(k) of the reference's ex_qc S(Q). */
+ORC_EXPORT void orc_rho_fp64_w(const float* pos, const float* w, int64_t n, const int64_t* sp_off, int nsp,
+                               const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
+    rho_fp64_impl(pos, w, n, sp_off, nsp, box, nvec, vec, rho);
+}
+
+static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int64_t* sp_off, int nsp,
+                          const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
+    (void)n;
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     for (int64_t v = 0; v < nvec; ++v)
         for (int d = 0; d < 3; ++d) {
@@ -308,8 +364,9 @@ ORC_EXPORT void orc_rho_fp64(const float* pos, int64_t n, const int64_t* sp_off,
                         double yr = tq[2 * iy], yi = tq[2 * iy + 1];
                         double zr = tq[2 * iz], zi = tq[2 * iz + 1];
                         double pr = xr * yr - xi * yi, pi2 = xr * yi + xi * yr;
-                        sr += pr * zr - pi2 * zi;
-                        si += pr * zi + pi2 * zr;
+                        const double wq = w ? (double)w[jb + q] : 1.0;
+                        sr += wq * (pr * zr - pi2 * zi);
+                        si += wq * (pr * zi + pi2 * zr);
                     }
                     my[2 * v] += sr;
                     my[2 * v + 1] += si;

@@ -8,7 +8,10 @@ reference's algorithm for the g_ab(r) / S_ab(Q) path on the CPU:
   r - L*int(r/L) and a stable species-contiguous order;
 * pair counts (rdf_sh, src/modules/rdf.cuf:451-475) in oracle.c, all-pairs or
   linked cells, with the reference's FP32 operation order and NINT;
-* rho_a(k) exactly in FP64 (oracle.c, orc_rho_fp64);
+* rho_a(k) exactly in FP64 (oracle.c, orc_rho_fp64), and the charge density
+  rho_q(k) = sum q_j exp(i k.r_j) (orc_rho_fp64_w; sq.cuf:569-573);
+* the charge-product histogram of counted pairs (orc_rdf_charged; rdf.cuf:469-472)
+  and avq2 = sum(q^2)/N (rdf.cuf:272);
 * the reference's FP32-phase S(Q) arithmetic (sqfnD, src/modules/sq.cuf:537-581)
   for the timed CPU baseline (orc_rho_ref32);
 * a pure-Python loop restatement of sq_init's n(Q) count (sq.cuf:328-342) for
@@ -57,6 +60,10 @@ def lib():
             fn = getattr(L, name)
             fn.restype = None
             fn.argtypes = [vp, i64, vp, i32, vp, i64, vp, vp]
+        L.orc_rdf_charged.restype = None
+        L.orc_rdf_charged.argtypes = [vp, vp, vp, i64, vp, f32, f32, i32, i32, vp, vp, vp, i32]
+        L.orc_rho_fp64_w.restype = None
+        L.orc_rho_fp64_w.argtypes = [vp, vp, i64, vp, i32, vp, i64, vp, vp]
         L.orc_num_threads.restype = i32
         L.orc_set_binning.restype = None
         L.orc_set_binning.argtypes = [i32]
@@ -68,8 +75,9 @@ def _p(a: np.ndarray):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def layout(xyz: np.ndarray, species: np.ndarray, box, nsp: int):
-    """Fold + stable species-contiguous order; returns (pos N x 3 FP32, species N, offsets nsp+1)."""
+def layout(xyz: np.ndarray, species: np.ndarray, box, nsp: int, charges=None):
+    """Fold + stable species-contiguous order; returns (pos N x 3 FP32, species N, offsets nsp+1),
+    and the charges in the same order as a fourth item when given (netcdf.f90:656-658)."""
     xyz = np.asarray(xyz, F32)
     box32 = np.asarray(box, F32)
     q = (xyz / box32).astype(F32)
@@ -78,7 +86,10 @@ def layout(xyz: np.ndarray, species: np.ndarray, box, nsp: int):
     sp = np.asarray(species, np.int32)[order]
     off = np.zeros(nsp + 1, np.int64)
     off[1:] = np.cumsum(np.bincount(sp, minlength=nsp))
-    return np.ascontiguousarray(folded[order]), np.ascontiguousarray(sp), off
+    res = (np.ascontiguousarray(folded[order]), np.ascontiguousarray(sp), off)
+    if charges is not None:
+        res = res + (np.ascontiguousarray(np.asarray(charges, F32)[order]),)
+    return res
 
 
 def rdf_counts(pos: np.ndarray, species: np.ndarray, box, side2: float, deltar: float, lsmax: int, nsp: int,
@@ -99,6 +110,40 @@ def rdf_counts(pos: np.ndarray, species: np.ndarray, box, side2: float, deltar: 
     finally:
         lib().orc_set_binning(0)
     return hist, edge
+
+
+def rdf_charged(pos, species, charges, box, side2, deltar, lsmax, nsp, cells: bool = True):
+    """Counts, edge statistics and the FP64 charge-product sums per bin (q_i q_j of counted pairs,
+    not divided by avq2) of one frame."""
+    pos = np.ascontiguousarray(pos, F32)
+    sp = np.ascontiguousarray(species, np.int32)
+    q = np.ascontiguousarray(charges, F32)
+    hist = np.zeros((nsp * (nsp + 1) // 2, lsmax), np.uint64)
+    edge = np.zeros(3, np.uint64)
+    gqq = np.zeros(lsmax, np.float64)
+    b = np.asarray(box, F32)
+    lib().orc_set_binning(0)
+    lib().orc_rdf_charged(_p(pos), _p(sp), _p(q), pos.shape[0], _p(b), float(F32(side2)), float(F32(deltar)),
+                          int(lsmax), int(nsp), _p(hist), _p(edge), _p(gqq), 1 if cells else 0)
+    return hist, edge, gqq
+
+
+def avq2(charges) -> float:
+    """sum(q^2)/N in FP64, rounded to FP32 as the reference's avq2 (rdf.cuf:272, sq.cuf:144)."""
+    q = np.asarray(charges, F32).astype(np.float64)
+    return float(F32(np.sum(q * q) / q.shape[0]))
+
+
+def rho_charge_fp64(pos: np.ndarray, charges: np.ndarray, box, vectors: np.ndarray) -> np.ndarray:
+    """Exact charge density rho_q(k) = sum_j q_j exp(i k.r_j): (nvec,) complex128."""
+    pos = np.ascontiguousarray(pos, F32)
+    q = np.ascontiguousarray(charges, F32)
+    off = np.array([0, pos.shape[0]], np.int64)
+    v = np.ascontiguousarray(vectors, np.int32)
+    out = np.zeros((1, v.shape[0], 2), np.float64)
+    b = np.asarray(box, F32)
+    lib().orc_rho_fp64_w(_p(pos), _p(q), pos.shape[0], _p(off), 1, _p(b), v.shape[0], _p(v), _p(out))
+    return out[0, :, 0] + 1j * out[0, :, 1]
 
 
 def rdf_counts_range(pos, species, box, side2, deltar, lsmax, nsp, i0, i1):

@@ -50,16 +50,20 @@ SIGNATURES = {
     "trj_sq_kernel_ms": (c_int, [vp, P(c_float)]),
     "trj_frame_pack": (c_int, [vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp]),
     "trj_frame_pack_static": (c_int, [vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp]),
+    "trj_frame_pack_charges": (c_int, [vp, vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp, vp]),
     "trj_rdf_plan_create": (c_int, [vp, c_int, c_float, c_float, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_create_floor": (c_int, [vp, c_int, c_float, c_int, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_info": (c_int, [vp, P(c_int), P(c_int), P(c_int), P(c_float), P(c_float), P(c_int64)]),
     "trj_rdf_accumulate": (c_int, [vp, vp, c_int64, P(c_float), vp, vp, vp]),
+    "trj_rdf_accumulate_charged": (c_int, [vp, vp, vp, c_int64, P(c_float), vp, vp, vp, vp]),
     "trj_rdf_plan_destroy": (c_int, [vp]),
     "trj_sq_plan_create": (c_int, [vp, c_int, c_int64, vp, vp, vp, vp, c_int, P(c_int64), P(vp)]),
+    "trj_sq_plan_create_charged": (c_int, [vp, c_int, c_int64, vp, vp, vp, vp, c_int, P(c_int64), P(vp)]),
     "trj_sq_plan_info": (c_int, [vp, P(c_int64), P(c_int64), P(c_int64), P(c_int64)]),
     "trj_sq_plan_set_flush": (c_int, [vp, c_int]),
     "trj_sq_plan_set_pairs": (c_int, [vp, c_int]),
     "trj_sq_accumulate": (c_int, [vp, vp, c_int64, P(c_float), c_int, vp, vp]),
+    "trj_sq_accumulate_charged": (c_int, [vp, vp, vp, c_int64, P(c_float), c_int, vp, vp]),
     "trj_sq_rho": (c_int, [vp, vp, vp]),
     "trj_sq_plan_destroy": (c_int, [vp]),
 }

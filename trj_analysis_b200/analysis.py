@@ -78,6 +78,9 @@ class Session:
         self.sq_out = None
         self.kset = None
         self.n = 0
+        self.ex_qc = None      # frames carry charges (set by the first frame, netcdf.f90:404-408)
+        self.gqq = None        # FP64 [lsmax] charge-product histogram over avq2, summed over frames
+        self.charges = None    # charges of the last frame (FP32, selected atoms)
 
     # ---- layout (select_ncdfinput) ------------------------------------------------
     def _species_of(self, types: np.ndarray) -> np.ndarray:
@@ -104,13 +107,22 @@ class Session:
         keep = species >= 0
         xyz = frame.xyz if keep.all() else frame.xyz[keep]
         species = species if keep.all() else species[keep]
+        if self.ex_qc is None:
+            self.ex_qc = frame.charges is not None
+        if self.ex_qc != (frame.charges is not None):
+            raise ValueError("frames with and without charges in one trajectory")
+        charges = None
+        if self.ex_qc:
+            q = np.asarray(frame.charges, np.float32)
+            charges = q if keep.all() else q[keep]
+            self.charges = charges
         if self.stage is None:
             n_max = self.n_max or xyz.shape[0]
-            self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp)
+            self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp, charged=self.ex_qc)
         self.box = np.asarray(frame.box, np.float32)
         self.volumen = refsem.volume(self.box)
         self.ntype = np.bincount(species, minlength=self.cfg.nsp).astype(np.int64)
-        self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream)
+        self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream, charges=charges)
 
     # ---- g(r) -----------------------------------------------------------------------
     def RDF_init(self) -> None:
@@ -118,20 +130,23 @@ class Session:
         self.rdf = engine.RdfPlan(self.ctx, c.nsp, c.deltar, c.rcrdf, self.box, self.stage.n_max)
         self.hist = self.rdf.new_hist()
         self.edge = torch.zeros(4, dtype=torch.int64, device=self.ctx.torch_device)
+        if self.ex_qc:
+            self.gqq = self.rdf.new_gqq()
 
     def RDFcomp(self) -> None:
-        self.rdf.accumulate(self.stage.packed, self.n, self.box, self.hist, self.edge, stream=self.stream)
+        self.rdf.accumulate(self.stage.packed, self.n, self.box, self.hist, self.edge, stream=self.stream,
+                            qpacked=self.stage.qpacked if self.ex_qc else None, gqq=self.gqq)
 
     # ---- S(Q) -----------------------------------------------------------------------
     def sq_init(self) -> None:
         c = self.cfg
         self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell)
-        self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype)
+        self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype, charged=bool(self.ex_qc))
         self.sq_out = self.sq.new_out()
 
     def SQcalc(self) -> None:
         self.sq.accumulate(self.stage.packed, self.n, self.box, self.sq_out, engine.METHODS[self.cfg.method],
-                           stream=self.stream)
+                           stream=self.stream, qpacked=self.stage.qpacked if self.ex_qc else None)
 
     # ---- frame loop (trj_analysis.f90:173-242) ---------------------------------------
     def add_frame(self, frame: Frame) -> None:
@@ -166,23 +181,35 @@ class Session:
         return {"edge_ulp": int(e[0]), "edge_fma": int(e[1]), "counted": int(e[2]), "tested": int(e[3])}
 
     def sq_transfer_gpu_cpu(self) -> np.ndarray:
-        """FP64 [nbins][nit] sums of w Re(rho_a conj(rho_b))."""
+        """FP64 [nbins][nit] sums of w Re(rho_a conj(rho_b)) (with charges: over the species and the
+        charge density, nit = (nsp+1)(nsp+2)/2)."""
         return self.sq_out.cpu().numpy()
+
+    def gqq_transfer(self) -> Optional[np.ndarray]:
+        """FP64 [lsmax] sum over frames of the charge-product histogram over avq2 (None without charges)."""
+        return None if self.gqq is None else self.gqq.cpu().numpy()
+
+    def avq2(self) -> float:
+        """sum(q^2)/N of the last frame, rounded to FP32 as the reference's variable (sq.cuf:144)."""
+        q = self.charges.astype(np.float64)
+        return float(F32(np.sum(q * q) / q.shape[0]))
 
     def rdf_results(self) -> Dict[str, np.ndarray]:
         return normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
-                             self.ntype, self.nconf)
+                             self.ntype, self.nconf, gqq=self.gqq_transfer())
 
     def sq_results(self) -> Dict[str, np.ndarray]:
-        return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf)
+        return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf,
+                            avq2=self.avq2() if self.ex_qc else None)
 
     def printrdf(self, outdir: str = ".") -> List[str]:
         res = self.rdf_results()
-        return writers.write_gmixsim(outdir, res["r"], res["g"], self.cfg.nsp)
+        return writers.write_gmixsim(outdir, res["r"], res["g"], self.cfg.nsp, g_qq=res.get("g_qq"))
 
     def printSQ(self, outdir: str = ".") -> List[str]:
         res = self.sq_results()
-        return writers.write_sq(outdir, res["q"], res["s_nn"], res["nq"], res["s_self"], res.get("binary"))
+        return writers.write_sq(outdir, res["q"], res["s_nn"], res["nq"], res["s_self"], res.get("binary"),
+                                s_qq=res.get("s_qq"))
 
     def suggested_rcl(self) -> float:
         """First minimum of the total g(r) after its first peak (rdf.cuf:313-352, 755-822)."""
@@ -203,8 +230,9 @@ def shell_volumes(lsmax: int, deltar: float) -> np.ndarray:
 
 
 def normalise_rdf(hist: np.ndarray, nsp: int, lsmax: int, deltar: float, volumen: float, ntype: np.ndarray,
-                  nconf: int) -> Dict[str, np.ndarray]:
-    """printrdf's g_jl(r_i) = (j/l+1) V H_jl(i) / (dV_i N_l N_j Nconf) for i = 1..lsmax-2 (FP64)."""
+                  nconf: int, gqq: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+    """printrdf's g_jl(r_i) = (j/l+1) V H_jl(i) / (dV_i N_l N_j Nconf) for i = 1..lsmax-2 (FP64), and with
+    charges g_qq(r_i) = 2 V gqq(i) / (N^2 dV_i Nconf) (log.f90:502-504)."""
     dv, ri = shell_volumes(lsmax, deltar)
     nrow = max(lsmax - 2, 0)
     g = np.zeros((nrow, nsp, nsp))
@@ -219,7 +247,10 @@ def normalise_rdf(hist: np.ndarray, nsp: int, lsmax: int, deltar: float, volumen
     # total g(r) with the 2V/(dV N^2) normalisation of RDFcomp (rdf.cuf:313-341), per frame
     n = float(np.sum(ntype))
     gtot = 2.0 * volumen * h[:, :nrow].sum(axis=0) / (dv[:nrow] * n * n * nconf)
-    return {"r": ri[:nrow].astype(np.float32), "g": g, "gtot": gtot}
+    res = {"r": ri[:nrow].astype(np.float32), "g": g, "gtot": gtot}
+    if gqq is not None:
+        res["g_qq"] = 2.0 * volumen * np.asarray(gqq, np.float64)[:nrow] / (n * n * dv[:nrow] * nconf)
+    return res
 
 
 def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, natms: int) -> float:
@@ -247,12 +278,27 @@ def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, n
     return deltar * imin
 
 
+def split_charged_rows(out: np.ndarray, nsp: int):
+    """Rows of a charged S(Q) output ((nsp+1)(nsp+2)/2 rows over the species and the charge density
+    nsp): the species-pair rows in the uncharged layout, the cross rows (a, q) and the (q, q) row."""
+    ndens = nsp + 1
+    sp = np.stack([out[:, refsem.pair_row(a, c, ndens)] for a, c in refsem.pair_rows(nsp)], axis=1)
+    cross = np.stack([out[:, refsem.pair_row(a, nsp, ndens)] for a in range(nsp)], axis=1)
+    return sp, cross, out[:, refsem.pair_row(nsp, nsp, ndens)]
+
+
 def normalise_sq(out: np.ndarray, kset: refsem.KSet, ntype: np.ndarray, bsc: np.ndarray,
-                 nconf: int) -> Dict[str, np.ndarray]:
+                 nconf: int, avq2: Optional[float] = None) -> Dict[str, np.ndarray]:
     """printSQ (log.f90:317-412) in FP64: S_NN = sqf/(baver^2 N Nconf nq), S_aa = sqfp_a/(N_a Nconf nq),
     and for two species with bsc = 1 the Bhatia-Thornton S_cc and the partials s11, s22, s12.
-    Also returns every species-pair S_ab = sum Re(rho_a rho_b*)/(sqrt(N_a N_b) Nconf nq)."""
+    Also returns every species-pair S_ab = sum Re(rho_a rho_b*)/(sqrt(N_a N_b) Nconf nq).
+    With avq2 (charged output layout): S_qq = sqfq/(N Nconf nq), sqfq = sum |rho_q|^2 / avq2
+    (sq.cuf:143-145, log.f90:386,393)."""
     nsp = ntype.shape[0]
+    sqfq = None
+    if avq2 is not None:
+        out, _, qq = split_charged_rows(out, nsp)
+        sqfq = qq / avq2
     n = float(ntype.sum())
     b = np.asarray(bsc, np.float64)
     rows = refsem.pair_rows(nsp)
@@ -272,6 +318,9 @@ def normalise_sq(out: np.ndarray, kset: refsem.KSet, ntype: np.ndarray, bsc: np.
     sl = slice(1, kset.nqmax + 1)
     res = {"q": kset.q_column(), "s_nn": s_nn[sl], "nq": kset.nq[sl], "s_self": s_self[sl], "s_pair": s_pair[sl],
            "sqf": sqf[sl]}
+    if sqfq is not None:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            res["s_qq"] = (sqfq / (n * nconf * den))[sl]
     if nsp == 2 and np.all(np.abs(b - 1.0) <= 1e-4):
         x1, x2 = ntype[0] / n, ntype[1] / n
         s11 = x1 * s_self[sl, 0]

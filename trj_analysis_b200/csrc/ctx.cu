@@ -205,7 +205,8 @@ __device__ __forceinline__ float fold_ref(float r, float L) {
 __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t* __restrict__ sp,
                                     int64_t n, int nsp, float Lx, float Ly, float Lz,
                                     const int64_t* __restrict__ block_base,
-                                    float4* __restrict__ packed) {
+                                    float4* __restrict__ packed, const float* __restrict__ q,
+                                    float* __restrict__ qpacked) {
     __shared__ int64_t base[kMaxSpecies];
     __shared__ int warp_cnt[kPackThreads / 32][kMaxSpecies];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -236,6 +237,7 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
             v.z = fold_ref(xyz[3 * i + 2], Lz);
             v.w = __int_as_float(s);
             packed[off] = v;
+            if (q) qpacked[off] = q[i];  // charges follow their atoms (netcdf.f90:656-658)
         }
         __syncthreads();
         if (threadIdx.x < nsp) {
@@ -252,20 +254,22 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
 
 }  // namespace
 
-extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
-                              int64_t n, int nsp, const float box[3], float* packed_dev,
-                              int64_t* counts_dev, void* stream) {
+// Layout with context scratch; q/qpacked null for frames without charges.
+static int frame_pack_impl(trj_ctx* ctx, const char* name, const float* xyz_dev, const int32_t* species_dev,
+                           const float* charge_dev, int64_t n, int nsp, const float box[3], float* packed_dev,
+                           float* charge_packed_dev, int64_t* counts_dev, void* stream) {
     if (!ctx) return TRJ_ERR_INVALID;
     if (n < 0 || nsp < 1 || nsp > kMaxSpecies || !box)
-        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: n=%lld nsp=%d (1..%d)", (long long)n,
-                        nsp, kMaxSpecies);
+        return trj_fail(ctx, TRJ_ERR_INVALID, "%s: n=%lld nsp=%d (1..%d)", name, (long long)n, nsp, kMaxSpecies);
     if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
-        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: box edges must be positive");
+        return trj_fail(ctx, TRJ_ERR_INVALID, "%s: box edges must be positive", name);
     if (n > 0 && (!xyz_dev || !species_dev || !packed_dev))
-        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: null pointer");
-    if (!counts_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: null counts");
+        return trj_fail(ctx, TRJ_ERR_INVALID, "%s: null pointer", name);
+    if (n > 0 && (charge_dev != nullptr) != (charge_packed_dev != nullptr))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "%s: charges need both the input and the output array", name);
+    if (!counts_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "%s: null counts", name);
     if (((uintptr_t)packed_dev) % 16 != 0)
-        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack: packed_dev must be 16-byte aligned");
+        return trj_fail(ctx, TRJ_ERR_INVALID, "%s: packed_dev must be 16-byte aligned", name);
     trj_device_guard g(ctx->device);
     cudaStream_t s = (cudaStream_t)stream;
     int64_t nblocks = (n + kPackChunk - 1) / kPackChunk;
@@ -284,7 +288,7 @@ extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t*
         ps.ptr = nullptr;
         ps.bytes = 0;
         if (trj_dev_alloc(ctx, &ps.ptr, need) != cudaSuccess)
-            return trj_fail(ctx, TRJ_ERR_NOMEM, "trj_frame_pack: scratch of %zu bytes", need);
+            return trj_fail(ctx, TRJ_ERR_NOMEM, "%s: scratch of %zu bytes", name, need);
         ps.bytes = need;
     }
     int64_t* block_base = (int64_t*)ps.ptr;
@@ -292,11 +296,29 @@ extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t*
     pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp,
                                                                  block_counts, ctx->status_dev);
     pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
-    pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(
-        xyz_dev, species_dev, n, nsp, box[0], box[1], box[2], block_base, (float4*)packed_dev);
+    pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, box[0], box[1],
+                                                                   box[2], block_base, (float4*)packed_dev,
+                                                                   charge_dev, charge_packed_dev);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
+}
+
+extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
+                              int64_t n, int nsp, const float box[3], float* packed_dev,
+                              int64_t* counts_dev, void* stream) {
+    return frame_pack_impl(ctx, "trj_frame_pack", xyz_dev, species_dev, nullptr, n, nsp, box, packed_dev, nullptr,
+                           counts_dev, stream);
+}
+
+extern "C" int trj_frame_pack_charges(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
+                                      const float* charge_dev, int64_t n, int nsp, const float box[3],
+                                      float* packed_dev, float* charge_packed_dev, int64_t* counts_dev,
+                                      void* stream) {
+    if (ctx && n > 0 && (!charge_dev || !charge_packed_dev))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_charges: null charge array");
+    return frame_pack_impl(ctx, "trj_frame_pack_charges", xyz_dev, species_dev, charge_dev, n, nsp, box, packed_dev,
+                           charge_packed_dev, counts_dev, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -379,7 +401,8 @@ extern "C" int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const i
                                                                  ctx->status_dev);
     pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
     pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, box[0], box[1],
-                                                                   box[2], block_base, (float4*)packed_dev);
+                                                                   box[2], block_base, (float4*)packed_dev, nullptr,
+                                                                   nullptr);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;

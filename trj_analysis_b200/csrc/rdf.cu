@@ -171,8 +171,12 @@ __device__ __noinline__ int exact_bin(float rr2, float x2, float dy, float dz, c
     return ind;
 }
 
+// QMODE: also adds the charge product q_a*q_b of every counted pair to the bin (FP64; the product
+// of two FP32 charges is exact in FP64).  rdf.cuf:469-472.
+template <bool QMODE>
 __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz, int row, const RdfParams& p,
-                                         unsigned* myhist, PairCounters& pc) {
+                                         unsigned* myhist, PairCounters& pc, double* myq, float qa,
+                                         const float* qbp) {
     const float q = rr2 * rsqrtf(rr2) * p.inv_deltar;
     const float fq = q - floorf(q);
     const float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
@@ -185,12 +189,16 @@ __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz
         ind = p.floor_bins ? (int)floorf(q) + 1 : __float2int_rn(q);
         if (ind > p.lsmax) ind = 0;
     }
-    if (ind > 0) atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
+    if (ind > 0) {
+        atomicAdd(&myhist[row * p.lsmax + ind - 1], 1u);
+        if (QMODE) atomicAdd(&myq[ind - 1], (double)qa * (double)__ldg(qbp));
+    }
 }
 
-template <bool FAST>
+template <bool FAST, bool QMODE>
 __device__ __forceinline__ void pair(const float4& a, const float4& b, bool valid, int si, const RdfParams& p,
-                                     const int* rowtab, unsigned* myhist, PairCounters& pc) {
+                                     const int* rowtab, unsigned* myhist, PairCounters& pc, double* myq,
+                                     float qa, const float* qbp) {
     float dx = __fsub_rn(b.x, a.x);
     float dy = __fsub_rn(b.y, a.y);
     float dz = __fsub_rn(b.z, a.z);
@@ -203,14 +211,16 @@ __device__ __forceinline__ void pair(const float4& a, const float4& b, bool vali
     const float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     if (valid && rr2 < p.side2_hi) {
         const int sj = __float_as_int(b.w);
-        if ((unsigned)sj < (unsigned)p.nsp) bin_pair(rr2, x2, dy, dz, rowtab[si * p.nsp + sj], p, myhist, pc);
+        if ((unsigned)sj < (unsigned)p.nsp)
+            bin_pair<QMODE>(rr2, x2, dy, dz, rowtab[si * p.nsp + sj], p, myhist, pc, myq, qa, qbp);
     }
 }
 
-template <bool FAST>
+template <bool FAST, bool QMODE>
 __device__ __forceinline__ void run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
                                          const float4& a1, bool h0, bool h1, int il0, int il1, int s0, int s1,
-                                         const RdfParams& p, const int* rowtab, unsigned* myhist, PairCounters& pc) {
+                                         const RdfParams& p, const int* rowtab, unsigned* myhist, PairCounters& pc,
+                                         double* myq, float qa0, float qa1, const float* qj) {
     int jbeg = 0;
     if (ti.self) jbeg = max(0, il0 + 1 - ti.jlocal0);  // il0 < il1: a0 starts earlier
     if (!h0 && !h1) jbeg = ti.jcount;
@@ -219,11 +229,15 @@ __device__ __forceinline__ void run_task(const TaskInfo& ti, const float4* __res
 #pragma unroll 2
     for (int jj = jbeg; jj < ti.jcount; ++jj) {
         const float4 b = bj[jj];
-        pair<FAST>(a0, b, h0, s0, p, rowtab, myhist, pc);
-        pair<FAST>(a1, b, h1 && jj > lim1, s1, p, rowtab, myhist, pc);
+        pair<FAST, QMODE>(a0, b, h0, s0, p, rowtab, myhist, pc, myq, qa0, qj + jj);
+        pair<FAST, QMODE>(a1, b, h1 && jj > lim1, s1, p, rowtab, myhist, pc, myq, qa1, qj + jj);
     }
 }
 
+// QMODE: sorted_q holds the charges in cell order and gqq_frame (lsmax doubles) receives this
+// frame's sum of q_a*q_b per bin; each warp's charge replica (lsmax doubles) follows the count
+// replicas in shared memory.
+template <bool QMODE>
 __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
                                                              const int32_t* __restrict__ cstart,
                                                              const int32_t* __restrict__ ccount,
@@ -231,7 +245,9 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
                                                              unsigned long long* __restrict__ work,
                                                              unsigned long long* __restrict__ hist_g,
                                                              unsigned long long* __restrict__ edge_g,
-                                                             unsigned* __restrict__ status) {
+                                                             unsigned* __restrict__ status,
+                                                             const float* __restrict__ sorted_q,
+                                                             double* __restrict__ gqq_frame) {
     extern __shared__ __align__(128) unsigned char smem[];
     float4* buf = reinterpret_cast<float4*>(smem);                       // [2][kJChunk]
     unsigned* hist = reinterpret_cast<unsigned*>(smem + 2 * kJChunk * sizeof(float4));
@@ -244,6 +260,13 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
     const int hsz = p.nit * p.lsmax;
     unsigned* myhist = hist + (size_t)(warp % p.nrep) * hsz;
     for (int k = tid; k < p.nrep * hsz; k += blockDim.x) hist[k] = 0u;
+    double* qhist = nullptr;
+    double* myq = nullptr;
+    if (QMODE) {
+        qhist = reinterpret_cast<double*>(hist + (((size_t)p.nrep * hsz + 1) & ~(size_t)1));
+        myq = qhist + (size_t)(warp % p.nrep) * p.lsmax;
+        for (int k = tid; k < p.nrep * p.lsmax; k += blockDim.x) qhist[k] = 0.0;
+    }
     for (int k = tid; k < p.nsp * p.nsp; k += blockDim.x) rowtab[k] = trj_pair_row(k / p.nsp, k % p.nsp, p.nsp);
     TaskGen gen;
     gen.started = 0;
@@ -284,6 +307,12 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
         const bool h0 = il0 < ti.na && (unsigned)s0 < (unsigned)p.nsp;
         const bool h1 = il1 < ti.na && (unsigned)s1 < (unsigned)p.nsp;
+        float qa0 = 0.f, qa1 = 0.f;
+        if (QMODE) {
+            qa0 = il0 < ti.na ? sorted_q[ti.sa + il0] : 0.f;
+            qa1 = il1 < ti.na ? sorted_q[ti.sa + il1] : 0.f;
+        }
+        const float* qj = QMODE ? sorted_q + ti.sb : nullptr;
         if (!trj_mbar_wait(&bars[slot], (t >> 1) & 1)) {
             trj_raise(status, TRJ_DEV_TIMEOUT);
             abort_flag = 1;
@@ -296,8 +325,11 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         } else {
             n_tested += (unsigned long long)((h0 ? ti.jcount : 0) + (h1 ? ti.jcount : 0));
         }
-        if (ti.fast) run_task<true>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc);
-        else run_task<false>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc);
+        if (ti.fast)
+            run_task<true, QMODE>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc, myq, qa0, qa1, qj);
+        else
+            run_task<false, QMODE>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc, myq, qa0, qa1,
+                                   qj);
     }
     if (tid == 0 && abort_flag) {
         // Let copies still in flight land before the CTA exits (bounded).
@@ -311,6 +343,13 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         for (int r = 0; r < p.nrep; ++r) s += hist[(size_t)r * hsz + k];
         if (s) atomicAdd(&hist_g[k], s);
         pc.counted += s;
+    }
+    if (QMODE) {
+        for (int k = tid; k < p.lsmax; k += blockDim.x) {
+            double s = 0.0;
+            for (int r = 0; r < p.nrep; ++r) s += qhist[(size_t)r * p.lsmax + k];
+            if (s != 0.0) atomicAdd(&gqq_frame[k], s);
+        }
     }
     if (edge_g) {
         unsigned long long n_ulp = pc.ulp, n_fma = pc.fma, n_counted = pc.counted;
@@ -358,10 +397,34 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
 
 __global__ void cell_scatter_kernel(const float4* __restrict__ packed, int64_t n,
                                     const int32_t* __restrict__ acell, const int32_t* __restrict__ aslot,
-                                    const int32_t* __restrict__ cstart, float4* __restrict__ sorted) {
+                                    const int32_t* __restrict__ cstart, float4* __restrict__ sorted,
+                                    const float* __restrict__ q, float* __restrict__ sorted_q) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    sorted[cstart[acell[i]] + aslot[i]] = packed[i];
+    const int64_t d = cstart[acell[i]] + aslot[i];
+    sorted[d] = packed[i];
+    if (q) sorted_q[d] = q[i];
+}
+
+// One block, after the pair kernel: avq2 = sum(q^2)/N in FP64 rounded to FP32 (rdf.cuf:272, where
+// avq2 is a default-real variable), then gqq += gqq_frame/avq2 (rdf.cuf:273).  The reduction order
+// is fixed, so avq2 does not depend on scheduling.
+__global__ void gqq_finish_kernel(const float* __restrict__ q, int64_t n, const double* __restrict__ gqq_frame,
+                                  int lsmax, double* __restrict__ gqq) {
+    __shared__ double part[1024];
+    double s = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = (double)q[i];
+        s += v * v;
+    }
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+        __syncthreads();
+    }
+    const float avq2 = (float)(part[0] / (double)n);
+    for (int k = threadIdx.x; k < lsmax; k += blockDim.x) gqq[k] += gqq_frame[k] / (double)avq2;
 }
 
 // Single-block exclusive scan of int32 counts (length up to a few million).
@@ -404,6 +467,8 @@ struct trj_rdf_plan {
     int32_t* acell = nullptr;   // n_max
     int32_t* aslot = nullptr;   // n_max
     float4* sorted = nullptr;   // n_max
+    float* sorted_q = nullptr;  // n_max charges in cell order (first charged call)
+    double* gqq_frame = nullptr;  // lsmax: this frame's charge-product sums
     int64_t scratch_bytes = 0;
     trj_kernel_timer timer;
 };
@@ -525,17 +590,23 @@ extern "C" int trj_rdf_plan_destroy(trj_rdf_plan* p) {
     {
         trj_device_guard g(p->ctx->device);
         trj_dev_free(p->ctx, p->sorted);
+        trj_dev_free(p->ctx, p->sorted_q);
         p->timer.release();
     }
     delete p;
     return TRJ_OK;
 }
 
-extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int64_t n, const float box[3],
-                                  uint64_t* hist_dev, uint64_t* edge_dev, void* stream) {
+// Frame accumulation; charge_dev/gqq_dev non-null adds the charge-product histogram.
+static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, const float* charge_dev, int64_t n,
+                               const float box[3], uint64_t* hist_dev, uint64_t* edge_dev, double* gqq_dev,
+                               void* stream) {
     if (!plan) return TRJ_ERR_INVALID;
     trj_ctx* ctx = plan->ctx;
     if (!box || !hist_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: null argument");
+    const bool charged = gqq_dev != nullptr;
+    if (charged && n > 0 && !charge_dev)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: null charge array");
     if (n < 0 || n > plan->n_max)
         return trj_fail(ctx, TRJ_ERR_CAPACITY, "rdf accumulate: n=%lld exceeds plan n_max=%lld", (long long)n,
                         (long long)plan->n_max);
@@ -543,9 +614,28 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
         return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: packed_dev null or not 16-byte aligned");
     if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
         return trj_fail(ctx, TRJ_ERR_INVALID, "rdf accumulate: box edges must be positive");
-    if (n < 2) return TRJ_OK;
     trj_device_guard g(ctx->device);
     cudaStream_t s = (cudaStream_t)stream;
+    if (charged && !plan->sorted_q) {
+        const size_t nq = (size_t)std::max<int64_t>(plan->n_max, 1);
+        const size_t qbytes = ((nq * sizeof(float) + 255) & ~(size_t)255) + sizeof(double) * (size_t)plan->lsmax;
+        char* qb = nullptr;
+        if (trj_dev_alloc(ctx, (void**)&qb, qbytes) != cudaSuccess)
+            return trj_fail(ctx, TRJ_ERR_NOMEM, "rdf accumulate: %zu bytes of charge scratch", qbytes);
+        plan->sorted_q = reinterpret_cast<float*>(qb);
+        plan->gqq_frame = reinterpret_cast<double*>(qb + ((nq * sizeof(float) + 255) & ~(size_t)255));
+        plan->scratch_bytes += (int64_t)qbytes;
+    }
+    if (n < 2) {
+        // No pair; gqq still receives 0/avq2 per bin, as the reference adds gqq_d/avq2 every frame.
+        if (charged && n == 1) {
+            TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
+            gqq_finish_kernel<<<1, 1024, 0, s>>>(charge_dev, n, plan->gqq_frame, plan->lsmax, gqq_dev);
+            ctx->launches += 1;
+            TRJ_CUDA_TRY(ctx, cudaGetLastError());
+        }
+        return TRJ_OK;
+    }
     // Per-frame clip, as select_ncdfinput does on every frame (netcdf.f90:610-617).
     float side = fminf(box[0], fminf(box[1], box[2]));
     plan->rcrdf_eff = fminf(plan->rcrdf_eff, side / 2.0f);
@@ -599,8 +689,8 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
     P.jsplit = (int)std::max<int64_t>(1, std::min<int64_t>(64, (want + base_items - 1) / base_items));
     P.nitems = base_items * P.jsplit;
 
-    // Shared memory: two staging buffers + histogram replicas.
-    size_t hist_bytes = (size_t)P.nit * P.lsmax * 4;
+    // Shared memory: two staging buffers + histogram replicas (+ FP64 charge replicas).
+    size_t hist_bytes = (size_t)P.nit * P.lsmax * 4 + (charged ? (size_t)P.lsmax * 8 + 8 : 0);
     size_t stage = 2 * kJChunk * sizeof(float4);
     size_t optin = ctx->smem_optin;
     // Most CTAs per SM (up to 4, i.e. 32 warps) that still hold >= 2 histogram replicas each;
@@ -620,8 +710,8 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
     if (nrep < 1) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf accumulate: histogram too large");
     P.nrep = nrep;
     size_t smem = stage + (size_t)nrep * hist_bytes;
-    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(rdf_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
+    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(charged ? rdf_pairs_kernel<true> : rdf_pairs_kernel<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     // Cell binning: count, scan, scatter.
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->ccount, 0, sizeof(int32_t) * P.ncell, s));
@@ -632,14 +722,37 @@ extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, i
                                           P.nc[1], P.nc[2], plan->ccount, plan->cflag, plan->acell, plan->aslot);
     scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->ccount, plan->cstart, P.ncell);
     cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->acell, plan->aslot, plan->cstart,
-                                           plan->sorted);
+                                           plan->sorted, charged ? charge_dev : nullptr, plan->sorted_q);
+    if (charged) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
     int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
     plan->timer.begin(ctx, s);
-    rdf_pairs_kernel<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount,
-                                                            plan->cflag, plan->work, (unsigned long long*)hist_dev,
-                                                            (unsigned long long*)edge_dev, ctx->status_dev);
+    if (charged)
+        rdf_pairs_kernel<true><<<(unsigned)grid, kThreads, smem, s>>>(
+            P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work, (unsigned long long*)hist_dev,
+            (unsigned long long*)edge_dev, ctx->status_dev, plan->sorted_q, plan->gqq_frame);
+    else
+        rdf_pairs_kernel<false><<<(unsigned)grid, kThreads, smem, s>>>(
+            P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work, (unsigned long long*)hist_dev,
+            (unsigned long long*)edge_dev, ctx->status_dev, nullptr, nullptr);
     plan->timer.end(ctx, s);
     ctx->launches += 4;
+    if (charged) {
+        gqq_finish_kernel<<<1, 1024, 0, s>>>(charge_dev, n, plan->gqq_frame, plan->lsmax, gqq_dev);
+        ctx->launches += 1;
+    }
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
+}
+
+extern "C" int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                                  uint64_t* hist_dev, uint64_t* edge_dev, void* stream) {
+    return rdf_accumulate_impl(plan, packed_dev, nullptr, n, box, hist_dev, edge_dev, nullptr, stream);
+}
+
+extern "C" int trj_rdf_accumulate_charged(trj_rdf_plan* plan, const float* packed_dev, const float* charge_dev,
+                                          int64_t n, const float box[3], uint64_t* hist_dev, uint64_t* edge_dev,
+                                          double* gqq_dev, void* stream) {
+    if (!plan) return TRJ_ERR_INVALID;
+    if (!gqq_dev) return trj_fail(plan->ctx, TRJ_ERR_INVALID, "rdf accumulate (charged): null gqq");
+    return rdf_accumulate_impl(plan, packed_dev, charge_dev, n, box, hist_dev, edge_dev, gqq_dev, stream);
 }

@@ -27,9 +27,11 @@ constexpr int kPlainVPT = 4;           // k-vectors per thread
 constexpr int kPlainChunk = 1024;      // atoms staged per pass
 constexpr int kPlainSub = 64;          // FP32 partial-sum length before the FP64 add
 
-// Fixed-point phase coordinates of every atom.
+// Fixed-point phase coordinates of every atom.  With charges (q non-null) every atom is written a
+// second time at n + i as a member of the charge species qsp, its charge (FP32 bits) in place of the
+// species index: rho_q(k) = sum_j q_j exp(i k.r_j) (sq.cuf:569-573) is then the sum of that species.
 __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n, double Lx, double Ly,
-                                    double Lz, uint4* __restrict__ out) {
+                                    double Lz, uint4* __restrict__ out, const float* __restrict__ q) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 v = packed[i];
@@ -41,11 +43,13 @@ __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n
         u[d] = (unsigned)(long long)rint(f * 4294967296.0);  // 2^32 wraps to 0
     }
     out[i] = make_uint4(u[0], u[1], u[2], (unsigned)__float_as_int(v.w));
+    if (q) out[n + i] = make_uint4(u[0], u[1], u[2], __float_as_uint(q[i]));
 }
 
 // Direct sum: thread owns kPlainVPT vectors; block y-index selects a slice of every species.
+// Species qsp (if any) is the charge species: each term is weighted by the charge in the entry's w.
 __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
-    const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp,
+    const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp, int qsp,
     const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
     int nsplit, double2* __restrict__ part) {
     __shared__ uint4 atoms[kPlainChunk];
@@ -70,6 +74,7 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
         double accr[kPlainVPT], acci[kPlainVPT];
 #pragma unroll
         for (int q = 0; q < kPlainVPT; ++q) accr[q] = acci[q] = 0.0;
+        const bool weighted = a == qsp;
         for (int64_t c0 = s0; c0 < s1; c0 += kPlainChunk) {
             int cnt = (int)((s1 - c0) < (int64_t)kPlainChunk ? (s1 - c0) : (int64_t)kPlainChunk);
             __syncthreads();
@@ -82,14 +87,15 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
                 for (int q = 0; q < kPlainVPT; ++q) fr[q] = fi[q] = 0.f;
                 for (int j = j0; j < j1; ++j) {
                     uint4 u = atoms[j];
+                    const float w = weighted ? __uint_as_float(u.w) : 1.0f;  // fma with 1: the plain sum
 #pragma unroll
                     for (int q = 0; q < kPlainVPT; ++q) {
                         unsigned ph = nx[q] * u.x + ny[q] * u.y + nz[q] * u.z;
                         float ang = __int2float_rn((int)ph) * kScale;
                         float sn, cs;
                         __sincosf(ang, &sn, &cs);
-                        fr[q] += cs;
-                        fi[q] += sn;
+                        fr[q] = fmaf(w, cs, fr[q]);
+                        fi[q] = fmaf(w, sn, fi[q]);
                     }
                 }
 #pragma unroll
@@ -255,6 +261,7 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
         p->species_off[a + 1] = p->species_off[a] + species_counts[a];
     }
     p->n_total = p->species_off[nsp];
+    p->n_atoms = p->n_total;
     // Plan order: stable sort by bin.
     std::vector<int64_t> order(nvec);
     std::iota(order.begin(), order.end(), 0);
@@ -397,6 +404,27 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     return TRJ_OK;
 }
 
+extern "C" int trj_sq_plan_create_charged(trj_ctx* ctx, int nsp, int64_t nvec, const int32_t* vec_host,
+                                          const int32_t* bin_host, const double* weight_host,
+                                          const uint8_t* dense_host, int nbins, const int64_t* species_counts,
+                                          trj_sq_plan** out) {
+    if (!ctx || !out) return TRJ_ERR_INVALID;
+    *out = nullptr;
+    if (nsp < 1 || nsp > 15) return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan (charged): nsp=%d (1..15)", nsp);
+    if (!species_counts) return trj_fail(ctx, TRJ_ERR_INVALID, "sq plan: null species counts");
+    // species nsp is the charge density over every atom
+    std::vector<int64_t> counts(species_counts, species_counts + nsp);
+    int64_t total = 0;
+    for (int64_t c : counts) total += c;
+    counts.push_back(total);
+    int rc = trj_sq_plan_create(ctx, nsp + 1, nvec, vec_host, bin_host, weight_host, dense_host, nbins,
+                                counts.data(), out);
+    if (rc != TRJ_OK) return rc;
+    (*out)->qsp = nsp;
+    (*out)->n_atoms = total;
+    return TRJ_OK;
+}
+
 extern "C" int trj_sq_plan_info(const trj_sq_plan* p, int64_t* n_dense, int64_t* n_tiles, int64_t* tile_slots,
                                 int64_t* scratch_bytes) {
     if (!p) return TRJ_ERR_INVALID;
@@ -412,7 +440,7 @@ static int run_plain(trj_sq_plan* p, const int32_t* subset, int64_t nsub, int ns
     if (nsub <= 0) return TRJ_OK;
     dim3 grid((unsigned)((nsub + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT)), (unsigned)nsplit);
     if (timed) p->timer.begin(p->ctx, s);
-    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->vec_dev, subset,
+    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->qsp, p->vec_dev, subset,
                                                    (int)nsub, p->nvec, nsplit, p->part_dev);
     if (timed) p->timer.end(p->ctx, s);
     int64_t tot = nsub * p->nsp;
@@ -422,14 +450,13 @@ static int run_plain(trj_sq_plan* p, const int32_t* subset, int64_t nsub, int ns
     return TRJ_OK;
 }
 
-extern "C" int trj_sq_accumulate(trj_sq_plan* p, const float* packed_dev, int64_t n, const float box[3], int method,
-                                 double* out_dev, void* stream) {
-    if (!p) return TRJ_ERR_INVALID;
+static int sq_accumulate_impl(trj_sq_plan* p, const float* packed_dev, const float* charge_dev, int64_t n,
+                              const float box[3], int method, double* out_dev, void* stream) {
     trj_ctx* ctx = p->ctx;
     if (!box || !out_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: null argument");
-    if (n != p->n_total)
+    if (n != p->n_atoms)
         return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: n=%lld but the plan's species counts sum to %lld",
-                        (long long)n, (long long)p->n_total);
+                        (long long)n, (long long)p->n_atoms);
     if (n > 0 && (!packed_dev || ((uintptr_t)packed_dev) % 16))
         return trj_fail(ctx, TRJ_ERR_INVALID, "sq accumulate: packed_dev null or not 16-byte aligned");
     if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
@@ -441,9 +468,12 @@ extern "C" int trj_sq_accumulate(trj_sq_plan* p, const float* packed_dev, int64_
     cudaStream_t s = (cudaStream_t)stream;
     if (n > 0) {
         phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
-                                                                       (double)box[1], (double)box[2], p->phase_dev);
-        check_counts_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp,
-                                                                        n, ctx->status_dev);
+                                                                       (double)box[1], (double)box[2], p->phase_dev,
+                                                                       charge_dev);
+        // the charge entries (n .. 2n-1) are the same atoms: only the first n carry species to check
+        check_counts_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->phase_dev, p->species_off_dev,
+                                                                        p->qsp >= 0 ? p->qsp : p->nsp, n,
+                                                                        ctx->status_dev);
         ctx->launches += 2;
     }
     if (method == TRJ_SQ_PLAIN_FP32 || p->tiles.empty()) {
@@ -462,6 +492,24 @@ extern "C" int trj_sq_accumulate(trj_sq_plan* p, const float* packed_dev, int64_
     p->last_method = method;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
+}
+
+extern "C" int trj_sq_accumulate(trj_sq_plan* p, const float* packed_dev, int64_t n, const float box[3], int method,
+                                 double* out_dev, void* stream) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (p->qsp >= 0)
+        return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq accumulate: plan made for charges; use trj_sq_accumulate_charged");
+    return sq_accumulate_impl(p, packed_dev, nullptr, n, box, method, out_dev, stream);
+}
+
+extern "C" int trj_sq_accumulate_charged(trj_sq_plan* p, const float* packed_dev, const float* charge_packed_dev,
+                                         int64_t n, const float box[3], int method, double* out_dev, void* stream) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (p->qsp < 0)
+        return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq accumulate (charged): plan made without charges");
+    if (n > 0 && !charge_packed_dev)
+        return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq accumulate (charged): null charge array");
+    return sq_accumulate_impl(p, packed_dev, charge_packed_dev, n, box, method, out_dev, stream);
 }
 
 extern "C" int trj_sq_kernel_ms(trj_sq_plan* p, float* ms) {

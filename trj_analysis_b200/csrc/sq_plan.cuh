@@ -21,7 +21,9 @@ struct trj_sq_plan {
     trj_ctx* ctx = nullptr;
     int nsp = 0, nit = 0, nbins = 0;
     int64_t nvec = 0;
-    int64_t n_total = 0;
+    int64_t n_total = 0;                   // phase entries: atoms, plus the charge species' copies
+    int64_t n_atoms = 0;                   // atoms per frame
+    int qsp = -1;                          // index of the charge species (charged plans), else -1
     std::vector<int64_t> species_counts;   // host
     std::vector<int64_t> species_off;      // host, nsp+1
     // vectors in plan order (sorted by bin); perm[plan_index] = caller index

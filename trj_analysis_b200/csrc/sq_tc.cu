@@ -305,19 +305,23 @@ __device__ __forceinline__ bool slot_atom(int64_t slot, const int64_t* pad_off, 
 __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
                                  const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nz_min,
                                  int nz_count, int64_t kdim, __nv_bfloat16* __restrict__ tab_hi,
-                                 __nv_bfloat16* __restrict__ tab_lo, uint2* __restrict__ uxy) {
+                                 __nv_bfloat16* __restrict__ tab_lo, uint2* __restrict__ uxy, int64_t qbase) {
     int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= total_slots) return;
     int64_t atom = 0;
     const bool real = slot_atom(slot, pad_off, sp_off, nsp, atom);
     const uint4 u = real ? phase[atom] : make_uint4(0u, 0u, 0u, 0u);
     if (blockIdx.y == 0) uxy[slot] = make_uint2(u.x, u.y);
+    // entries from qbase on belong to the charge species: the Z factor carries the charge
+    const float wq = (real && atom >= qbase) ? __uint_as_float(u.w) : 1.0f;
     uint32_t* hi = reinterpret_cast<uint32_t*>(tab_hi);
     uint32_t* lo = reinterpret_cast<uint32_t*>(tab_lo);
     for (int t = blockIdx.y; t < nz_count; t += gridDim.y) {
         uint32_t h0 = 0u, l0 = 0u, h1 = 0u, l1 = 0u;
         if (real) {
-            const float2 z = phase_factor((unsigned)(nz_min + t) * u.z);
+            float2 z = phase_factor((unsigned)(nz_min + t) * u.z);
+            z.x *= wq;
+            z.y *= wq;
             split2(z.x, -z.y, h0, l0);
             split2(z.y, z.x, h1, l1);
         }
@@ -1418,7 +1422,8 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     const int nz_count = st->table_rows / 2;
     dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 32));
     tc_ztable_kernel<<<zg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
-                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo, st->uxy);
+                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo, st->uxy,
+                                        plan->qsp >= 0 ? plan->n_atoms : INT64_MAX);
     TcParams P;
     P.tiles = st->tiles_dev;
     P.chunks = st->chunks_dev;

@@ -61,16 +61,25 @@ class Context:
 
 
 def pack_frame(ctx: Context, xyz: torch.Tensor, species: torch.Tensor, nsp: int, box,
-               packed: torch.Tensor, counts: torch.Tensor, stream=None) -> None:
-    """Device layout step (fold + stable species-contiguous order)."""
+               packed: torch.Tensor, counts: torch.Tensor, stream=None, charges: Optional[torch.Tensor] = None,
+               qpacked: Optional[torch.Tensor] = None) -> None:
+    """Device layout step (fold + stable species-contiguous order); charges, when given, are written
+    to ``qpacked`` in the packed order."""
     n = int(xyz.shape[0])
     assert xyz.dtype == torch.float32 and xyz.is_contiguous() and xyz.is_cuda
     assert species.dtype == torch.int32 and species.is_contiguous()
     assert packed.dtype == torch.float32 and packed.shape[0] >= n and packed.shape[1] == 4
     assert counts.dtype == torch.int64 and counts.numel() >= nsp
-    rc = ctx.lib.trj_frame_pack(ctx.h, _ptr(xyz), _ptr(species), n, nsp, box3(box), _ptr(packed),
-                                _ptr(counts), _stream(stream))
-    check(rc, ctx.h, "trj_frame_pack")
+    if charges is None:
+        rc = ctx.lib.trj_frame_pack(ctx.h, _ptr(xyz), _ptr(species), n, nsp, box3(box), _ptr(packed),
+                                    _ptr(counts), _stream(stream))
+        check(rc, ctx.h, "trj_frame_pack")
+        return
+    assert charges.dtype == torch.float32 and charges.is_contiguous() and charges.numel() >= n
+    assert qpacked is not None and qpacked.dtype == torch.float32 and qpacked.numel() >= n
+    rc = ctx.lib.trj_frame_pack_charges(ctx.h, _ptr(xyz), _ptr(species), _ptr(charges), n, nsp, box3(box),
+                                        _ptr(packed), _ptr(qpacked), _ptr(counts), _stream(stream))
+    check(rc, ctx.h, "trj_frame_pack_charges")
 
 
 class RdfPlan:
@@ -108,12 +117,26 @@ class RdfPlan:
     def new_hist(self) -> torch.Tensor:
         return torch.zeros((self.nit, self.lsmax), dtype=torch.int64, device=self.ctx.torch_device)
 
+    def new_gqq(self) -> torch.Tensor:
+        """FP64 [lsmax] accumulator of the charge-product histogram divided by avq2 per frame."""
+        return torch.zeros((self.lsmax,), dtype=torch.float64, device=self.ctx.torch_device)
+
     def accumulate(self, packed: torch.Tensor, n: int, box, hist: torch.Tensor,
-                   edge: Optional[torch.Tensor] = None, stream=None) -> None:
+                   edge: Optional[torch.Tensor] = None, stream=None, qpacked: Optional[torch.Tensor] = None,
+                   gqq: Optional[torch.Tensor] = None) -> None:
+        """Adds the frame's pair counts to ``hist``; with ``qpacked`` (charges in packed order) and
+        ``gqq`` also the charge-product histogram over avq2."""
         assert hist.dtype == torch.int64 and hist.shape == (self.nit, self.lsmax)
-        rc = self.ctx.lib.trj_rdf_accumulate(self.h, _ptr(packed), int(n), box3(box), _ptr(hist), _ptr(edge),
-                                             _stream(stream))
-        check(rc, self.ctx.h, "trj_rdf_accumulate")
+        if qpacked is None and gqq is None:
+            rc = self.ctx.lib.trj_rdf_accumulate(self.h, _ptr(packed), int(n), box3(box), _ptr(hist), _ptr(edge),
+                                                 _stream(stream))
+            check(rc, self.ctx.h, "trj_rdf_accumulate")
+            return
+        assert qpacked is not None and gqq is not None
+        assert qpacked.dtype == torch.float32 and gqq.dtype == torch.float64 and gqq.shape == (self.lsmax,)
+        rc = self.ctx.lib.trj_rdf_accumulate_charged(self.h, _ptr(packed), _ptr(qpacked), int(n), box3(box),
+                                                     _ptr(hist), _ptr(edge), _ptr(gqq), _stream(stream))
+        check(rc, self.ctx.h, "trj_rdf_accumulate_charged")
 
     def close(self) -> None:
         if getattr(self, "h", None):
@@ -128,9 +151,13 @@ class RdfPlan:
 
 
 class SqPlan:
-    def __init__(self, ctx: Context, nsp: int, kset: KSet, species_counts):
+    """S(Q) plan.  ``charged=True`` adds the charge density as species ``nsp``: the output then has
+    (nsp+1)(nsp+2)/2 rows (last row: sums of w |rho_q|^2) and accumulate takes the packed charges."""
+
+    def __init__(self, ctx: Context, nsp: int, kset: KSet, species_counts, charged: bool = False):
         self.ctx = ctx
         self.nsp = nsp
+        self.charged = bool(charged)
         self.kset = kset
         counts = np.ascontiguousarray(np.asarray(species_counts, dtype=np.int64))
         assert counts.shape == (nsp,)
@@ -139,13 +166,15 @@ class SqPlan:
         self._w = np.ascontiguousarray(kset.weights.astype(np.float64))
         self._dense = np.ascontiguousarray(kset.dense.astype(np.uint8))
         h = vp()
-        rc = ctx.lib.trj_sq_plan_create(
+        create = ctx.lib.trj_sq_plan_create_charged if self.charged else ctx.lib.trj_sq_plan_create
+        rc = create(
             ctx.h, nsp, int(kset.nvec), self._vec.ctypes.data_as(vp), self._bin.ctypes.data_as(vp),
             self._w.ctypes.data_as(vp), self._dense.ctypes.data_as(vp), int(kset.nbins),
             counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(h))
         check(rc, ctx.h, "trj_sq_plan_create")
         self.h = h
-        self.nit = nsp * (nsp + 1) // 2
+        self.ndens = nsp + 1 if self.charged else nsp  # densities: species (+ charge)
+        self.nit = self.ndens * (self.ndens + 1) // 2
         self.n_total = int(counts.sum())
         nd, nt, ts, sb = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         check(ctx.lib.trj_sq_plan_info(h, ctypes.byref(nd), ctypes.byref(nt), ctypes.byref(ts), ctypes.byref(sb)),
@@ -163,15 +192,25 @@ class SqPlan:
         """Tensor-core tiles in CTA pairs (one M = 256 contraction per two tiles) or one per CTA."""
         check(self.ctx.lib.trj_sq_plan_set_pairs(self.h, 1 if enable else 0), self.ctx.h, "trj_sq_plan_set_pairs")
 
-    def accumulate(self, packed: torch.Tensor, n: int, box, out: torch.Tensor, method: int, stream=None) -> None:
+    def accumulate(self, packed: torch.Tensor, n: int, box, out: torch.Tensor, method: int, stream=None,
+                   qpacked: Optional[torch.Tensor] = None) -> None:
         assert out.dtype == torch.float64 and out.shape == (self.kset.nbins, self.nit)
+        if self.charged:
+            if qpacked is None:
+                raise ValueError("charged S(Q) plan: pass the packed charges")
+            assert qpacked.dtype == torch.float32 and qpacked.numel() >= n
+            rc = self.ctx.lib.trj_sq_accumulate_charged(self.h, _ptr(packed), _ptr(qpacked), int(n), box3(box),
+                                                        int(method), _ptr(out), _stream(stream))
+            check(rc, self.ctx.h, "trj_sq_accumulate_charged")
+            return
         rc = self.ctx.lib.trj_sq_accumulate(self.h, _ptr(packed), int(n), box3(box), int(method), _ptr(out),
                                             _stream(stream))
         check(rc, self.ctx.h, "trj_sq_accumulate")
 
     def rho(self, stream=None) -> torch.Tensor:
-        """rho_a(k) of the last accumulate, (nsp, nvec) complex128, caller vector order."""
-        t = torch.empty((self.nsp, self.kset.nvec, 2), dtype=torch.float64, device=self.ctx.torch_device)
+        """rho_a(k) of the last accumulate, (ndens, nvec) complex128, caller vector order (charged plans:
+        the charge density last)."""
+        t = torch.empty((self.ndens, self.kset.nvec, 2), dtype=torch.float64, device=self.ctx.torch_device)
         check(self.ctx.lib.trj_sq_rho(self.h, _ptr(t), _stream(stream)), self.ctx.h, "trj_sq_rho")
         return torch.view_as_complex(t)
 
@@ -194,11 +233,18 @@ METHODS = {"plain": _lib.TRJ_SQ_PLAIN_FP32, "split": _lib.TRJ_SQ_SPLIT_BF16X3,
 class FrameStage:
     """Pinned host staging + device buffers for frames of up to ``n_max`` atoms."""
 
-    def __init__(self, ctx: Context, n_max: int, nsp: int):
+    def __init__(self, ctx: Context, n_max: int, nsp: int, charged: bool = False):
         dev = ctx.torch_device
         self.ctx = ctx
         self.n_max = n_max
         self.nsp = nsp
+        self.charged = bool(charged)
+        if self.charged:
+            self.h_q = torch.empty((n_max,), dtype=torch.float32, pin_memory=True)
+            self.d_q = torch.empty((n_max,), dtype=torch.float32, device=dev)
+            self.qpacked = torch.empty((n_max,), dtype=torch.float32, device=dev)
+        else:
+            self.h_q = self.d_q = self.qpacked = None
         self.h_xyz = torch.empty((n_max, 3), dtype=torch.float32, pin_memory=True)
         self.h_sp = torch.empty((n_max,), dtype=torch.int32, pin_memory=True)
         self.d_xyz = torch.empty((n_max, 3), dtype=torch.float32, device=dev)
@@ -207,20 +253,29 @@ class FrameStage:
         self.counts = torch.zeros((max(nsp, 1),), dtype=torch.int64, device=dev)
         self._copied = None  # event after the last host->device copy out of the pinned buffers
 
-    def upload_and_pack(self, xyz: np.ndarray, species: np.ndarray, box, stream=None) -> int:
+    def upload_and_pack(self, xyz: np.ndarray, species: np.ndarray, box, stream=None,
+                        charges: Optional[np.ndarray] = None) -> int:
         n = int(xyz.shape[0])
         if n > self.n_max:
             raise _lib.TrjError(_lib.TRJ_ERR_CAPACITY, f"frame of {n} atoms exceeds stage size {self.n_max}")
+        if self.charged != (charges is not None):
+            raise ValueError("frame charges: the stage was made " + ("with" if self.charged else "without") +
+                             " charges")
         if self._copied is not None:
             self._copied.synchronize()  # pinned buffers may still feed the previous copy
         self.h_xyz[:n].numpy()[:] = xyz
         self.h_sp[:n].numpy()[:] = species
+        if self.charged:
+            self.h_q[:n].numpy()[:] = charges
         s = stream if stream is not None else torch.cuda.current_stream()
         with torch.cuda.stream(s):
             self.d_xyz[:n].copy_(self.h_xyz[:n], non_blocking=True)
             self.d_sp[:n].copy_(self.h_sp[:n], non_blocking=True)
+            if self.charged:
+                self.d_q[:n].copy_(self.h_q[:n], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(s)
             self._copied = ev
-        pack_frame(self.ctx, self.d_xyz[:n], self.d_sp[:n], self.nsp, box, self.packed, self.counts, stream=s)
+        pack_frame(self.ctx, self.d_xyz[:n], self.d_sp[:n], self.nsp, box, self.packed, self.counts, stream=s,
+                   charges=self.d_q[:n] if self.charged else None, qpacked=self.qpacked)
         return n

@@ -2,8 +2,9 @@
 
 A frame is the raw input of one configuration, before the layout step:
 ``xyz`` (N, 3) float32 positions as a trajectory stores them (not folded),
-``types`` (N,) int32 LAMMPS-style type ids (1-based), and ``box`` (3,) float32
-orthorhombic edge lengths.  This is what ``read_nc_cfg`` hands to
+``types`` (N,) int32 LAMMPS-style type ids (1-based), ``box`` (3,) float32
+orthorhombic edge lengths, and optionally ``charges`` (N,) float32 per-atom
+charges (the NetCDF variable ``q``, read as default real by netcdf.f90:404-408).  This is what ``read_nc_cfg`` hands to
 ``select_ncdfinput`` in the reference (src/core/netcdf.f90:173-550).
 
 The synthetic generator places 4 atoms per cubic FCC cell of edge
@@ -11,13 +12,15 @@ The synthetic generator places 4 atoms per cubic FCC cell of edge
 standard deviation ``sigma * a`` per axis, optionally re-places a fraction of
 atoms uniformly in the box, and assigns types by a seeded shuffle with given
 ratios.  Species identity is fixed per trajectory (seed), displacements differ
-per frame (seed, frame).
+per frame (seed, frame).  With ``charges`` given per type, atoms carry that
+charge plus an optional seeded per-atom offset (``charge_jitter``, fixed per
+trajectory), so both species-constant and per-atom charge sets can be made.
 """
 from __future__ import annotations
 
 import dataclasses
 import os
-from typing import Iterator, Sequence
+from typing import Iterator, Optional, Sequence
 
 import numpy as np
 
@@ -27,6 +30,7 @@ class Frame:
     xyz: np.ndarray      # (N, 3) float32
     types: np.ndarray    # (N,) int32, 1-based type ids
     box: np.ndarray      # (3,) float32
+    charges: Optional[np.ndarray] = None  # (N,) float32
 
     @property
     def n(self) -> int:
@@ -43,6 +47,8 @@ class FCCSpec:
     replace_frac: float = 0.0            # fraction of atoms re-placed uniformly at random
     remove: int = 0                      # atoms removed by a seeded draw (to hit a target N)
     seed: int = 1234
+    charges: Optional[tuple] = None      # charge per type 1..nsp (None: no charges)
+    charge_jitter: float = 0.0           # std. dev. of a seeded per-atom charge offset
 
     @property
     def a(self) -> float:
@@ -95,7 +101,16 @@ class FCCSpec:
             idx = rng.choice(pos.shape[0], size=m, replace=False)
             pos[idx] = rng.uniform(0.0, 1.0, size=(m, 3)) * box
         return Frame(xyz=pos.astype(np.float32), types=types.copy(),
-                     box=self.box.copy())
+                     box=self.box.copy(), charges=self._charges(types))
+
+    def _charges(self, types: np.ndarray) -> Optional[np.ndarray]:
+        if self.charges is None:
+            return None
+        q = np.asarray(self.charges, np.float64)[types - 1]
+        if self.charge_jitter > 0:
+            rng = np.random.default_rng([self.seed, 0xc4a7])
+            q = q + rng.normal(0.0, self.charge_jitter, size=q.shape)
+        return q.astype(np.float32)
 
     def frames(self, count: int, start: int = 0) -> Iterator[Frame]:
         for i in range(start, start + count):
@@ -128,8 +143,16 @@ def c4_spec(seed: int = 4) -> FCCSpec:
 WORKLOADS = {"c1": c1_spec, "c2": c2_spec, "c3": c3_spec, "c4": c4_spec}
 
 
+def _frame_charges(var, f: int) -> Optional[np.ndarray]:
+    if var is None:
+        return None
+    v = np.asarray(var[f] if len(var.shape) == 2 else var[:], np.float32)
+    return np.ascontiguousarray(v)
+
+
 class NpzTrajectory:
-    """Frames stored as ``coordinates`` (F, N, 3), ``cell_lengths`` (F, 3), ``type`` (F, N) or (N,)."""
+    """Frames stored as ``coordinates`` (F, N, 3), ``cell_lengths`` (F, 3), ``type`` (F, N) or (N,),
+    and optionally ``q`` (F, N) or (N,) charges."""
 
     def __init__(self, path: str):
         self._z = np.load(path)
@@ -141,15 +164,16 @@ class NpzTrajectory:
         coords = self._z["coordinates"]
         cells = self._z["cell_lengths"]
         types = self._z["type"] if "type" in self._z else None
+        q = self._z["q"] if "q" in self._z else None
         for f in range(coords.shape[0]):
             t = np.ones(coords.shape[1], np.int32) if types is None else (
                 types[f] if types.ndim == 2 else types)
             yield Frame(xyz=np.asarray(coords[f], np.float32), types=np.asarray(t, np.int32),
-                        box=np.asarray(cells[f], np.float32))
+                        box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f))
 
 
 class NetCDFTrajectory:
-    """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type``).
+    """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type`` and ``q``).
 
     Uses netCDF4 when importable, else scipy's reader for classic CDF-1/2 files.
     """
@@ -172,11 +196,12 @@ class NetCDFTrajectory:
         coords = self._v["coordinates"]
         cells = self._v["cell_lengths"]
         has_type = "type" in self._v
+        q = self._v["q"] if "q" in self._v else None
         for f in range(coords.shape[0]):
             xyz = np.asarray(coords[f], dtype=np.float32)
             t = (np.asarray(self._v["type"][f], np.int32) if has_type
                  else np.ones(xyz.shape[0], np.int32))
-            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32))
+            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f))
 
 
 def open_trajectory(path: str):
@@ -187,14 +212,18 @@ def open_trajectory(path: str):
 
 
 def write_npz_trajectory(path: str, frames: Sequence[Frame]) -> None:
+    extra = {}
+    if frames[0].charges is not None:
+        extra["q"] = np.stack([f.charges for f in frames])
     np.savez(path, coordinates=np.stack([f.xyz for f in frames]),
              cell_lengths=np.stack([f.box for f in frames]),
-             type=np.stack([f.types for f in frames]))
+             type=np.stack([f.types for f in frames]), **extra)
 
 
 def write_netcdf_trajectory(path: str, frames: Sequence[Frame]) -> None:
     """Classic NetCDF (CDF-2) file with the AMBER-convention variables the reference reads:
-    coordinates (frame, atom, spatial), cell_lengths (frame, cell_spatial), type (frame, atom)."""
+    coordinates (frame, atom, spatial), cell_lengths (frame, cell_spatial), type (frame, atom), and
+    q (frame, atom) when the frames carry charges."""
     from scipy.io import netcdf_file
     nf = len(frames)
     n = frames[0].n
@@ -208,7 +237,10 @@ def write_netcdf_trajectory(path: str, frames: Sequence[Frame]) -> None:
         c = nc.createVariable("coordinates", "f4", ("frame", "atom", "spatial"))
         L = nc.createVariable("cell_lengths", "f4", ("frame", "cell_spatial"))
         t = nc.createVariable("type", "i4", ("frame", "atom"))
+        q = nc.createVariable("q", "f4", ("frame", "atom")) if frames[0].charges is not None else None
         for k, f in enumerate(frames):
             c[k] = f.xyz
             L[k] = f.box
             t[k] = f.types
+            if q is not None:
+                q[k] = f.charges

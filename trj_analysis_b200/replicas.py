@@ -63,7 +63,7 @@ def merge(hist: Optional[torch.Tensor] = None, sq_sums: Optional[torch.Tensor] =
 def run_sharded(session, frames: Iterable, rank: int, world: int, group=None) -> Dict[str, object]:
     """Analyse this rank's frames with an `analysis.Session`, then merge over the group.
 
-    Afterwards the session's device accumulators (counts, edge statistics, S sums) and its frame
+    Afterwards the session's device accumulators (counts, edge statistics, S sums, g_qq sums) and its frame
     count hold the whole trajectory on every rank, so its printrdf/printSQ give the one-GPU result.
     Needs at least one frame per rank (the plans are sized from a rank's first frame).
     """
@@ -77,5 +77,8 @@ def run_sharded(session, frames: Iterable, rank: int, world: int, group=None) ->
     out = merge(session.hist, session.sq_out, nframes=len(mine), group=group)
     if session.edge is not None:
         dist.all_reduce(session.edge, op=dist.ReduceOp.SUM, group=group)
+    gqq = getattr(session, "gqq", None)
+    if gqq is not None:  # charge-product histogram over avq2: a per-frame sum like the counts
+        dist.all_reduce(gqq, op=dist.ReduceOp.SUM, group=group)
     session.nconf = int(out["nframes"])
     return out

@@ -3,9 +3,12 @@
 printrdf  -> gmixsim.dat (src/core/log.f90:414-596): header
              '#       r        ',9x,16('g_',2i1,'(r)',9x:), rows '(16f16.5)'
              (nsp > 6: one file gmixsim<k>.dat per species k, full rows g_k1..g_knsp).
+             With charges a g_qq(r) column follows r (log.f90:456-458, 559-560: rows
+             '(16f16.6)'; nsp > 6: in gmixsim1.dat only, rows '(16f16.5)', 565-567).
 printSQ   -> sq.dat  (log.f90:317-412): '(2f15.7,i12)' or, for 2 species with all
              bsc = 1, '(6f15.7,i12)' with S_NN, S_cc, S_11, S_22, S_12, n(Q);
-             sqmix.dat '(15f16.7)' with S_aa per species.
+             with charges S_qq(Q) follows S_NN ('(3f15.7,i12)' / '(7f15.7,i12)',
+             log.f90:353-362, 385-394); sqmix.dat '(15f16.7)' with S_aa per species.
 freud-style tools -> gr.dat / Sq.dat as numpy.savetxt writes them ('%.18e', header
              '# r g(r)' / '# k S(k)'); species-resolved columns are appended.
 
@@ -17,7 +20,7 @@ field prints as asterisks; an i1 field of a value >= 10 prints '*'.
 from __future__ import annotations
 
 import decimal
-from typing import Iterable, List, Sequence
+from typing import Iterable, List, Optional, Sequence
 
 import numpy as np
 
@@ -59,17 +62,21 @@ def _group_header(prefix: str, labels: Sequence[str], per_line: int, sep: str) -
     return lines or [prefix.rstrip()]
 
 
-def write_gmixsim(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int) -> List[str]:
-    """g: (nrows, nsp, nsp) symmetric partial g_ab(r).  Returns the files written."""
+def write_gmixsim(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int,
+                  g_qq: Optional[np.ndarray] = None) -> List[str]:
+    """g: (nrows, nsp, nsp) symmetric partial g_ab(r); g_qq: (nrows,) charge-charge g(r) or None.
+    Returns the files written."""
     import os
     files = []
+    qhead = "#       r        " + " " * 9 + ("g_qq(r)" + " " * 9 if g_qq is not None else "")
     if nsp <= 6:
         labels = [f"g_{_i1(j + 1)}{_i1(k + 1)}(r)" for j in range(nsp) for k in range(j, nsp)]
-        head = _group_header("#       r        " + " " * 9, labels, 16, " " * 9)
+        head = _group_header(qhead, labels, 16, " " * 9)
         rows = []
         for i in range(r.shape[0]):
-            vals = [r[i]] + [g[i, j, k] for j in range(nsp) for k in range(j, nsp)]
-            rows.extend(_records(vals, 16, 16, 5))
+            vals = [r[i]] + ([g_qq[i]] if g_qq is not None else []) + \
+                [g[i, j, k] for j in range(nsp) for k in range(j, nsp)]
+            rows.extend(_records(vals, 16, 16, 6 if g_qq is not None else 5))
         p = os.path.join(path_dir, "gmixsim.dat")
         with open(p, "w") as f:
             f.write("\n".join(head + rows) + "\n")
@@ -77,10 +84,12 @@ def write_gmixsim(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int) -> List
     else:
         for k in range(nsp):
             labels = [f"g_{_i1(k + 1)}{_i1(j + 1)}(r)" for j in range(nsp)]
-            head = _group_header("#       r        " + " " * 9, labels, 16, " " * 9)
+            withq = g_qq is not None and k == 0
+            head = _group_header(qhead if withq else "#       r        " + " " * 9, labels, 16, " " * 9)
             rows = []
             for i in range(r.shape[0]):
-                rows.extend(_records([r[i]] + [g[i, k, j] for j in range(nsp)], 16, 16, 5))
+                vals = [r[i]] + ([g_qq[i]] if withq else []) + [g[i, k, j] for j in range(nsp)]
+                rows.extend(_records(vals, 16, 16, 5))
             p = os.path.join(path_dir, f"gmixsim{k + 1}.dat")
             with open(p, "w") as f:
                 f.write("\n".join(head + rows) + "\n")
@@ -91,6 +100,9 @@ def write_gmixsim(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int) -> List
 SQ_HEADER_BINARY = ("#           Q        S_NN(Q)          S_cc(Q)       S_11(Q)        S_22(Q)"
                     "           S_12(Q)         n(Q)")
 SQ_HEADER = "#           Q       S_NN(Q)          n(Q)"
+SQ_HEADER_BINARY_QQ = ("#           Q        S_NN(Q)          S_qq(Q)          S_cc(Q)       S_11(Q)        S_22(Q)"
+                       "           S_12(Q)         n(Q)")
+SQ_HEADER_QQ = "#           Q       S_NN(Q)          S_qq(Q)          n(Q)"
 
 
 def sqmix_header(nsp: int) -> List[str]:
@@ -99,16 +111,21 @@ def sqmix_header(nsp: int) -> List[str]:
 
 
 def write_sq(path_dir: str, q: np.ndarray, s_nn: np.ndarray, nq: np.ndarray, s_self: np.ndarray,
-             binary: dict = None) -> List[str]:
-    """q, s_nn, nq: rows 1..nqmax; s_self: (nrows, nsp); binary: scc, s11, s22, s12 arrays."""
+             binary: dict = None, s_qq: Optional[np.ndarray] = None) -> List[str]:
+    """q, s_nn, nq: rows 1..nqmax; s_self: (nrows, nsp); binary: scc, s11, s22, s12 arrays;
+    s_qq: charge-charge S(Q) rows or None."""
     import os
-    lines = [SQ_HEADER_BINARY if binary is not None else SQ_HEADER]
+    if s_qq is not None:
+        lines = [SQ_HEADER_BINARY_QQ if binary is not None else SQ_HEADER_QQ]
+    else:
+        lines = [SQ_HEADER_BINARY if binary is not None else SQ_HEADER]
     for i in range(q.shape[0]):
+        qq = [s_qq[i]] if s_qq is not None else []
         if binary is not None:
-            vals = [q[i], s_nn[i], binary["scc"][i], binary["s11"][i], binary["s22"][i], binary["s12"][i]]
-            lines.append("".join(fmt_f(v, 15, 7) for v in vals) + fmt_i(nq[i], 12))
+            vals = [q[i], s_nn[i]] + qq + [binary["scc"][i], binary["s11"][i], binary["s22"][i], binary["s12"][i]]
         else:
-            lines.append(fmt_f(q[i], 15, 7) + fmt_f(s_nn[i], 15, 7) + fmt_i(nq[i], 12))
+            vals = [q[i], s_nn[i]] + qq
+        lines.append("".join(fmt_f(v, 15, 7) for v in vals) + fmt_i(nq[i], 12))
     p1 = os.path.join(path_dir, "sq.dat")
     with open(p1, "w") as f:
         f.write("\n".join(lines) + "\n")
