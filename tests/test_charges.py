@@ -199,3 +199,24 @@ def test_uncharged_trajectory_has_no_charges(tmp_path):
     path = str(tmp_path / "t.nc")
     frames.write_netcdf_trajectory(path, frs)
     assert next(iter(frames.open_trajectory(path))).charges is None
+
+
+def test_species_charge_derivations_match_charge_density():
+    """Charge-layout rows derived from the species rows equal those of the charge density itself."""
+    spec = frames.FCCSpec(cells=(4, 4, 4), sigma=0.1, fractions=(0.5, 0.3, 0.2), seed=9,
+                          charges=(1.0, -0.8476, 0.4238))
+    fr = spec.frame(0)
+    nsp = 3
+    pos, sps, off, qs = orc.layout(fr.xyz, fr.types - 1, fr.box, nsp, charges=fr.charges)
+    ks = refsem.make_kset("full+axes", fr.box, 5.0, 2.0)
+    rho = orc.rho_fp64(pos, off, fr.box, ks.vectors)
+    rho_all = np.concatenate([rho, orc.rho_charge_fp64(pos, qs, fr.box, ks.vectors)[None, :]])
+    want = orc.bin_sums(rho_all, ks.bins, ks.weights, ks.nbins)
+    got = analysis.species_charged_rows(orc.bin_sums(rho, ks.bins, ks.weights, ks.nbins),
+                                        np.asarray(spec.charges, np.float32), nsp)
+    np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-6)
+    rc = float(F32(min(fr.box) / F32(2)))
+    lsmax = int(math.floor(rc / 0.05 + 0.5)) + 1
+    hist, _, gqq = orc.rdf_charged(pos, sps, qs, fr.box, float(F32(rc * rc)), 0.05, lsmax, nsp)
+    np.testing.assert_allclose(analysis.species_gqq(hist, np.asarray(spec.charges, np.float32), nsp), gqq,
+                               rtol=1e-12, atol=1e-9)

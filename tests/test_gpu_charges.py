@@ -226,3 +226,30 @@ def test_session_with_charges_writes_g_qq_and_s_qq(ctx, tmp_path):
     rel = np.abs(got[live] - want_sqq[live]) / np.abs(want_sqq[live])
     assert rel.max() <= REL_SHELL, rel.max()
     s.close()
+
+
+def test_species_charge_mode_matches_atom_mode(ctx):
+    """Species-constant charges: the derived g_qq/S_qq equal those of the charge-weighted kernels."""
+    spec = CASES["2sp_species_constant"]
+    frs = list(spec.frames(2))
+    res = {}
+    for mode in ("atom", "species"):
+        cfg = analysis.Config(nsp=2, sp_types_selected=(1, 2), deltar=0.02, qmax=6.0, qmin=2.0, method="plain",
+                              charge_mode=mode)
+        s = analysis.Session(cfg, ctx=ctx).run(frs)
+        res[mode] = (s.rdf_results(), s.sq_results(), s.device_charges)
+        s.close()
+    assert res["atom"][2] and not res["species"][2]
+    np.testing.assert_allclose(res["species"][0]["g_qq"], res["atom"][0]["g_qq"], rtol=1e-10, atol=1e-10)
+    a, b = res["atom"][1]["s_qq"], res["species"][1]["s_qq"]
+    live = np.isfinite(a)
+    assert np.all(np.abs(a[live] - b[live]) <= REL_SHELL * np.abs(a[live]) + 1e-9)
+
+
+def test_species_charge_mode_rejects_per_atom_charges(ctx):
+    spec = CASES["3sp_cells"]
+    cfg = analysis.Config(nsp=3, sp_types_selected=(1, 2, 3), charge_mode="species")
+    s = analysis.Session(cfg, ctx=ctx)
+    with pytest.raises(ValueError, match="different charges"):
+        s.add_frame(spec.frame(0))
+    s.close()

@@ -49,6 +49,10 @@ class Config:
     per_shell: int = 200
     seed: int = 0
     units: str = "lj"
+    # Frames with charges: "atom" runs the charge-weighted kernels (any per-atom charges, as the
+    # reference's ex_qc path); "species" requires every atom of a species to carry the same charge in
+    # every frame and derives g_qq and S_qq from the species rows, with no extra device work.
+    charge_mode: str = "atom"
 
     def bsc_list(self) -> List[float]:
         return list(self.bsc) if self.bsc is not None else [1.0] * self.nsp
@@ -81,6 +85,7 @@ class Session:
         self.ex_qc = None      # frames carry charges (set by the first frame, netcdf.f90:404-408)
         self.gqq = None        # FP64 [lsmax] charge-product histogram over avq2, summed over frames
         self.charges = None    # charges of the last frame (FP32, selected atoms)
+        self.species_q = None  # charge of each species (charge_mode "species")
 
     # ---- layout (select_ncdfinput) ------------------------------------------------
     def _species_of(self, types: np.ndarray) -> np.ndarray:
@@ -116,13 +121,40 @@ class Session:
             q = np.asarray(frame.charges, np.float32)
             charges = q if keep.all() else q[keep]
             self.charges = charges
+            if self.cfg.charge_mode == "species":
+                self._check_species_charges(charges, species)
+                charges = None  # nothing charge-weighted runs on the device
+            elif self.cfg.charge_mode != "atom":
+                raise ValueError(f"charge_mode {self.cfg.charge_mode!r}: 'atom' or 'species'")
         if self.stage is None:
             n_max = self.n_max or xyz.shape[0]
-            self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp, charged=self.ex_qc)
+            self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp, charged=self.device_charges)
         self.box = np.asarray(frame.box, np.float32)
         self.volumen = refsem.volume(self.box)
         self.ntype = np.bincount(species, minlength=self.cfg.nsp).astype(np.int64)
         self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream, charges=charges)
+
+    @property
+    def device_charges(self) -> bool:
+        """The charge-weighted kernels run (frames with charges, charge_mode 'atom')."""
+        return bool(self.ex_qc) and self.cfg.charge_mode == "atom"
+
+    def _check_species_charges(self, q: np.ndarray, species: np.ndarray) -> None:
+        """Every atom of a species carries the species' charge, the same in every frame, and the species
+        counts do not change (so avq2 = sum_a N_a q_a^2 / N is the same in every frame)."""
+        nsp = self.cfg.nsp
+        vals, first = np.unique(species, return_index=True)
+        qa = np.zeros(nsp, np.float32)
+        qa[vals] = q[first]
+        if not np.array_equal(q, qa[species]):
+            raise ValueError("charge_mode 'species': atoms of one species carry different charges "
+                             "(use charge_mode 'atom')")
+        counts = np.bincount(species, minlength=nsp)
+        if self.species_q is None:
+            self.species_q, self._species_q_counts = qa, counts
+        elif not (np.array_equal(qa, self.species_q) and np.array_equal(counts, self._species_q_counts)):
+            raise ValueError("charge_mode 'species': species charges or counts change between frames "
+                             "(use charge_mode 'atom')")
 
     # ---- g(r) -----------------------------------------------------------------------
     def RDF_init(self) -> None:
@@ -130,23 +162,24 @@ class Session:
         self.rdf = engine.RdfPlan(self.ctx, c.nsp, c.deltar, c.rcrdf, self.box, self.stage.n_max)
         self.hist = self.rdf.new_hist()
         self.edge = torch.zeros(4, dtype=torch.int64, device=self.ctx.torch_device)
-        if self.ex_qc:
+        if self.device_charges:
             self.gqq = self.rdf.new_gqq()
 
     def RDFcomp(self) -> None:
+        dq = self.device_charges
         self.rdf.accumulate(self.stage.packed, self.n, self.box, self.hist, self.edge, stream=self.stream,
-                            qpacked=self.stage.qpacked if self.ex_qc else None, gqq=self.gqq)
+                            qpacked=self.stage.qpacked if dq else None, gqq=self.gqq)
 
     # ---- S(Q) -----------------------------------------------------------------------
     def sq_init(self) -> None:
         c = self.cfg
         self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell)
-        self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype, charged=bool(self.ex_qc))
+        self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype, charged=self.device_charges)
         self.sq_out = self.sq.new_out()
 
     def SQcalc(self) -> None:
         self.sq.accumulate(self.stage.packed, self.n, self.box, self.sq_out, engine.METHODS[self.cfg.method],
-                           stream=self.stream, qpacked=self.stage.qpacked if self.ex_qc else None)
+                           stream=self.stream, qpacked=self.stage.qpacked if self.device_charges else None)
 
     # ---- frame loop (trj_analysis.f90:173-242) ---------------------------------------
     def add_frame(self, frame: Frame) -> None:
@@ -187,7 +220,19 @@ class Session:
 
     def gqq_transfer(self) -> Optional[np.ndarray]:
         """FP64 [lsmax] sum over frames of the charge-product histogram over avq2 (None without charges)."""
-        return None if self.gqq is None else self.gqq.cpu().numpy()
+        if self.gqq is not None:
+            return self.gqq.cpu().numpy()
+        if self.ex_qc and self.species_q is not None:
+            return species_gqq(self.rdf_transfer(), self.species_q, self.cfg.nsp) / self.avq2()
+        return None
+
+    def sq_charged_sums(self) -> np.ndarray:
+        """S sums in the charged row layout: from the device (charge_mode 'atom') or derived from the
+        species rows (charge_mode 'species')."""
+        out = self.sq_transfer_gpu_cpu()
+        if self.device_charges:
+            return out
+        return species_charged_rows(out, self.species_q, self.cfg.nsp)
 
     def avq2(self) -> float:
         """sum(q^2)/N of the last frame, rounded to FP32 as the reference's variable (sq.cuf:144)."""
@@ -199,8 +244,10 @@ class Session:
                              self.ntype, self.nconf, gqq=self.gqq_transfer())
 
     def sq_results(self) -> Dict[str, np.ndarray]:
-        return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf,
-                            avq2=self.avq2() if self.ex_qc else None)
+        if not self.ex_qc:
+            return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf)
+        return normalise_sq(self.sq_charged_sums(), self.kset, self.ntype, self.bsc_sp, self.nconf,
+                            avq2=self.avq2())
 
     def printrdf(self, outdir: str = ".") -> List[str]:
         res = self.rdf_results()
@@ -276,6 +323,35 @@ def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, n
         den = y1 - 2.0 * y2 + y3
         return x2 + 0.5 * (y1 - y3) / den * (x3 - x1) / 2.0 if abs(den) > 1e-12 else x2
     return deltar * imin
+
+
+def species_gqq(hist: np.ndarray, qa: np.ndarray, nsp: int) -> np.ndarray:
+    """Charge-product sums per bin when species a carries charge q_a: sum_{a<=b} q_a q_b H_ab (FP64),
+    the sum rdf.cuf:469-472 forms pair by pair."""
+    q = np.asarray(qa, np.float32).astype(np.float64)
+    out = np.zeros(hist.shape[1])
+    for a, b in refsem.pair_rows(nsp):
+        out += q[a] * q[b] * hist[refsem.pair_row(a, b, nsp)].astype(np.float64)
+    return out
+
+
+def species_charged_rows(out: np.ndarray, qa: np.ndarray, nsp: int) -> np.ndarray:
+    """Charged-layout S sums from the species rows when species a carries charge q_a:
+    rho_q = sum_a q_a rho_a, so Re(rho_a rho_q*) = sum_b q_b Re(rho_a rho_b*) and
+    |rho_q|^2 = sum_{a,b} q_a q_b Re(rho_a rho_b*)."""
+    q = np.asarray(qa, np.float32).astype(np.float64)
+    ndens = nsp + 1
+    res = np.zeros((out.shape[0], ndens * (ndens + 1) // 2))
+
+    def sp(a, b):
+        return out[:, refsem.pair_row(a, b, nsp)]
+
+    for a, b in refsem.pair_rows(nsp):
+        res[:, refsem.pair_row(a, b, ndens)] = sp(a, b)
+    for a in range(nsp):
+        res[:, refsem.pair_row(a, nsp, ndens)] = sum(q[b] * sp(a, b) for b in range(nsp))
+    res[:, refsem.pair_row(nsp, nsp, ndens)] = sum(q[a] * q[b] * sp(a, b) for a in range(nsp) for b in range(nsp))
+    return res
 
 
 def split_charged_rows(out: np.ndarray, nsp: int):
