@@ -53,6 +53,7 @@ extern "C" {
 typedef struct trj_ctx trj_ctx;
 typedef struct trj_rdf_plan trj_rdf_plan;
 typedef struct trj_sq_plan trj_sq_plan;
+typedef struct trj_dyn_plan trj_dyn_plan;
 
 /* Edge-pair statistics of one or more accumulate calls (device uint64[4]). */
 enum {
@@ -235,6 +236,37 @@ TRJ_API int trj_sq_rho(trj_sq_plan* plan, double* rho_dev, void* stream);
  * TRJ_SQ_SPLIT_BF16X3, direct sum for TRJ_SQ_PLAIN_FP32); needs timing enabled. */
 TRJ_API int trj_sq_kernel_ms(trj_sq_plan* plan, float* ms);
 TRJ_API int trj_sq_plan_destroy(trj_sq_plan* plan);
+
+/* ---- F(Q,t), Fs(Q,t), mean-squared displacement ------------------------ */
+/* Replaces the device part of dyn_init/rtcorr (src/modules/dynamics.cuf:88-135,
+ * 157-276; kernels FqtnD 421-507 and rtcal 510-547).  nbuffer time origins, each
+ * with ndyn lag rows; nvec integer lattice vectors n (k = 2*pi*n/L per axis) with
+ * their output bins 0..nbins-1 (the qw shells of sq.cuf:239-297); bsc: the
+ * coherent weight per species; n: atoms per frame (same order in every frame, as
+ * trj_frame_pack writes them).  Device memory: about 48*nbuffer*n bytes plus the
+ * accumulators (3 x nbuffer*ndyn*nbins doubles). */
+TRJ_API int trj_dyn_plan_create(trj_ctx* ctx, int nsp, int64_t n, int nbuffer, int ndyn, int64_t nvec,
+                                const int32_t* vec_host, const int32_t* bin_host, int nbins,
+                                const float* bsc_host, trj_dyn_plan** out);
+TRJ_API int trj_dyn_plan_info(const trj_dyn_plan* plan, int64_t* scratch_bytes);
+/* One frame: for every buffer b with lag_host[b] >= 0 (0-based lag row,
+ * < ndyn; -1 = buffer not started or finished) adds to its rows
+ *   F_b(bin, lag)  += sum over the bin's k of Re(rho(k,t0) conj(rho(k,t))),
+ *                     rho(k,t) = sum_j bsc[species_j] exp(i k.r_j(t))
+ *   Fs_b(bin, lag) += sum over the bin's k of sum_j cos(k.(r_j(t) - r_j(t0)))
+ *   C_b(lag)       += sum_j |rt_j(t) - r_j(t0)|^2 / n   (rt unwrapped per buffer)
+ * origin_host[b] = 1 makes this frame buffer b's origin t0 (its lag must be 0).
+ * packed_dev: output of trj_frame_pack for this frame. */
+TRJ_API int trj_dyn_accumulate(trj_dyn_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                               const int32_t* lag_host, const uint8_t* origin_host, void* stream);
+/* Adds the rows of every buffer with done_host[b] = 1 to the totals and clears
+ * them (rtcorr, dynamics.cuf:239-269): fkt_dev, fskt_dev double [ndyn][nbins],
+ * r2t_dev double [ndyn]. */
+TRJ_API int trj_dyn_flush(trj_dyn_plan* plan, const uint8_t* done_host, double* fkt_dev, double* fskt_dev,
+                          double* r2t_dev, void* stream);
+/* Duration (ms) of the last self-term kernel launch; needs timing enabled. */
+TRJ_API int trj_dyn_kernel_ms(trj_dyn_plan* plan, float* ms);
+TRJ_API int trj_dyn_plan_destroy(trj_dyn_plan* plan);
 
 #ifdef __cplusplus
 }

@@ -66,6 +66,12 @@ SIGNATURES = {
     "trj_sq_accumulate_charged": (c_int, [vp, vp, vp, c_int64, P(c_float), c_int, vp, vp]),
     "trj_sq_rho": (c_int, [vp, vp, vp]),
     "trj_sq_plan_destroy": (c_int, [vp]),
+    "trj_dyn_plan_create": (c_int, [vp, c_int, c_int64, c_int, c_int, c_int64, vp, vp, c_int, vp, P(vp)]),
+    "trj_dyn_plan_info": (c_int, [vp, P(c_int64)]),
+    "trj_dyn_accumulate": (c_int, [vp, vp, c_int64, P(c_float), vp, vp, vp]),
+    "trj_dyn_flush": (c_int, [vp, vp, vp, vp, vp, vp]),
+    "trj_dyn_kernel_ms": (c_int, [vp, P(c_float)]),
+    "trj_dyn_plan_destroy": (c_int, [vp]),
 }
 
 _lib = None

@@ -28,6 +28,7 @@ import numpy as np
 import torch
 
 from . import engine, refsem, writers
+from .dynamics import DynConfig, Dynamics
 from .frames import Frame
 from .refsem import F32
 
@@ -53,6 +54,9 @@ class Config:
     # reference's ex_qc path); "species" requires every atom of a species to carry the same charge in
     # every frame and derives g_qq and S_qq from the species rows, with no extra device work.
     charge_mode: str = "atom"
+    # F(Q,t), Fs(Q,t), MSD over multiple time origins (rtcorr; needs the trajectory's frame count)
+    run_sqw: bool = False
+    dyn: Optional["DynConfig"] = None
 
     def bsc_list(self) -> List[float]:
         return list(self.bsc) if self.bsc is not None else [1.0] * self.nsp
@@ -62,8 +66,11 @@ class Session:
     """Per-trajectory state of the g(r)/S(Q) path on one device."""
 
     def __init__(self, cfg: Config, device: int = 0, n_max: Optional[int] = None,
-                 ctx: Optional[engine.Context] = None, stream: Optional[torch.cuda.Stream] = None):
+                 ctx: Optional[engine.Context] = None, stream: Optional[torch.cuda.Stream] = None,
+                 nconf_total: Optional[int] = None):
         self.cfg = cfg
+        self.nconf_total = nconf_total  # Nconf of the trajectory (dyn_init sizes its buffers from it)
+        self.dyn = None
         self.ctx = ctx if ctx is not None else engine.Context(device)
         self.stream = stream
         self.n_max = n_max
@@ -194,7 +201,24 @@ class Session:
             self.RDFcomp()
         if self.cfg.run_sq:
             self.SQcalc()
+        if self.cfg.run_sqw:
+            self.rtcorr(frame)
         self.nconf += 1
+
+    # ---- F(Q,t), Fs(Q,t), MSD (dyn_init / rtcorr) -----------------------------------------
+    def dyn_init(self) -> None:
+        if self.nconf_total is None:
+            raise ValueError("run_sqw needs nconf_total (the trajectory's number of frames)")
+        self.dyn = Dynamics(self.ctx, self.cfg.nsp, self.n, self.nconf_total, self.cfg.dyn or DynConfig(),
+                            self.box, self.bsc_sp)
+
+    def rtcorr(self, frame: Frame) -> None:
+        if self.dyn is None:
+            self.dyn_init()
+        self.dyn.rtcorr(self.nconf + 1, self.stage.packed, self.n, self.box, time=frame.time, stream=self.stream)
+
+    def print_rtcor(self, outdir: str = ".") -> List[str]:
+        return self.dyn.print_rtcor(outdir, units=self.cfg.units)
 
     def run(self, frames: Iterable[Frame], check_every: int = 0) -> "Session":
         for k, f in enumerate(frames):
@@ -264,7 +288,7 @@ class Session:
                              int(self.ntype.sum()))
 
     def close(self) -> None:
-        for obj in (self.sq, self.rdf):
+        for obj in (self.sq, self.rdf, self.dyn):
             if obj is not None:
                 obj.close()
 

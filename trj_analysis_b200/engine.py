@@ -226,6 +226,63 @@ class SqPlan:
             pass
 
 
+class DynPlan:
+    """Multiple-origin time correlations (F(Q,t), Fs(Q,t), MSD) over the vectors of an SqwSet."""
+
+    def __init__(self, ctx: Context, nsp: int, n: int, nbuffer: int, ndyn: int, sqw, bsc):
+        self.ctx = ctx
+        self.nsp, self.n, self.nbuffer, self.ndyn = nsp, int(n), int(nbuffer), int(ndyn)
+        self.nbins = int(sqw.qw.size)
+        self._vec = np.ascontiguousarray(sqw.vectors.astype(np.int32))
+        self._bin = np.ascontiguousarray(sqw.bins.astype(np.int32))
+        self._bsc = np.ascontiguousarray(np.asarray(bsc, np.float32))
+        assert self._bsc.shape == (nsp,)
+        h = vp()
+        rc = ctx.lib.trj_dyn_plan_create(ctx.h, nsp, self.n, self.nbuffer, self.ndyn, int(self._vec.shape[0]),
+                                         self._vec.ctypes.data_as(vp), self._bin.ctypes.data_as(vp), self.nbins,
+                                         self._bsc.ctypes.data_as(vp), ctypes.byref(h))
+        check(rc, ctx.h, "trj_dyn_plan_create")
+        self.h = h
+        sb = ctypes.c_int64()
+        check(ctx.lib.trj_dyn_plan_info(h, ctypes.byref(sb)), ctx.h, "trj_dyn_plan_info")
+        self.scratch_bytes = sb.value
+
+    def new_totals(self):
+        """(fkt [ndyn][nbins], fskt [ndyn][nbins], r2t [ndyn]) FP64 device accumulators."""
+        dev = self.ctx.torch_device
+        return (torch.zeros((self.ndyn, self.nbins), dtype=torch.float64, device=dev),
+                torch.zeros((self.ndyn, self.nbins), dtype=torch.float64, device=dev),
+                torch.zeros((self.ndyn,), dtype=torch.float64, device=dev))
+
+    def accumulate(self, packed: torch.Tensor, n: int, box, lags: np.ndarray, origins: np.ndarray,
+                   stream=None) -> None:
+        lag = np.ascontiguousarray(np.asarray(lags, np.int32))
+        org = np.ascontiguousarray(np.asarray(origins, np.uint8))
+        assert lag.shape == (self.nbuffer,) and org.shape == (self.nbuffer,)
+        rc = self.ctx.lib.trj_dyn_accumulate(self.h, _ptr(packed), int(n), box3(box), lag.ctypes.data_as(vp),
+                                             org.ctypes.data_as(vp), _stream(stream))
+        check(rc, self.ctx.h, "trj_dyn_accumulate")
+
+    def flush(self, done: np.ndarray, fkt: torch.Tensor, fskt: torch.Tensor, r2t: torch.Tensor, stream=None) -> None:
+        d = np.ascontiguousarray(np.asarray(done, np.uint8))
+        assert d.shape == (self.nbuffer,)
+        assert fkt.dtype == fskt.dtype == r2t.dtype == torch.float64
+        rc = self.ctx.lib.trj_dyn_flush(self.h, d.ctypes.data_as(vp), _ptr(fkt), _ptr(fskt), _ptr(r2t),
+                                        _stream(stream))
+        check(rc, self.ctx.h, "trj_dyn_flush")
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.ctx.lib.trj_dyn_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 METHODS = {"plain": _lib.TRJ_SQ_PLAIN_FP32, "split": _lib.TRJ_SQ_SPLIT_BF16X3,
            "plain_fp32": _lib.TRJ_SQ_PLAIN_FP32, "split_bf16x3": _lib.TRJ_SQ_SPLIT_BF16X3}
 

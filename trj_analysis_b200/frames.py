@@ -31,6 +31,7 @@ class Frame:
     types: np.ndarray    # (N,) int32, 1-based type ids
     box: np.ndarray      # (3,) float32
     charges: Optional[np.ndarray] = None  # (N,) float32
+    time: Optional[float] = None          # the trajectory's time (NetCDF variable "time") of this frame
 
     @property
     def n(self) -> int:
@@ -117,6 +118,21 @@ class FCCSpec:
             yield self.frame(i)
 
 
+def random_walk_frames(spec: FCCSpec, count: int, step_sigma: float, seed: int = 11,
+                       time_step: float = 1.0) -> Iterator[Frame]:
+    """A seeded trajectory in which every atom of ``spec.frame(0)`` takes Gaussian steps of standard
+    deviation ``step_sigma`` per axis between frames (positions are not folded: atoms leave the box
+    and the layout folds them back); ``time`` = frame index * time_step."""
+    fr0 = spec.frame(0)
+    pos = fr0.xyz.astype(np.float64)
+    rng = np.random.default_rng([seed, 0xd1f])
+    for f in range(count):
+        if f:
+            pos = pos + rng.normal(0.0, step_sigma, size=pos.shape)
+        yield Frame(xyz=pos.astype(np.float32), types=fr0.types.copy(), box=fr0.box.copy(),
+                    charges=None if fr0.charges is None else fr0.charges.copy(), time=float(f * time_step))
+
+
 # Named workloads (shapes of the benchmark configurations).
 def c1_spec(seed: int = 1) -> FCCSpec:
     """N=4000 single species, cubic L=17.0998, sigma=0.12 a."""
@@ -197,11 +213,13 @@ class NetCDFTrajectory:
         cells = self._v["cell_lengths"]
         has_type = "type" in self._v
         q = self._v["q"] if "q" in self._v else None
+        tv = self._v["time"] if "time" in self._v else None
         for f in range(coords.shape[0]):
             xyz = np.asarray(coords[f], dtype=np.float32)
             t = (np.asarray(self._v["type"][f], np.int32) if has_type
                  else np.ones(xyz.shape[0], np.int32))
-            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f))
+            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f),
+                        time=None if tv is None else float(tv[f]))
 
 
 def open_trajectory(path: str):
@@ -238,9 +256,14 @@ def write_netcdf_trajectory(path: str, frames: Sequence[Frame]) -> None:
         L = nc.createVariable("cell_lengths", "f4", ("frame", "cell_spatial"))
         t = nc.createVariable("type", "i4", ("frame", "atom"))
         q = nc.createVariable("q", "f4", ("frame", "atom")) if frames[0].charges is not None else None
+        tv = nc.createVariable("time", "f4", ("frame",)) if frames[0].time is not None else None
+        if tv is not None:
+            tv.units = b"picosecond"
         for k, f in enumerate(frames):
             c[k] = f.xyz
             L[k] = f.box
             t[k] = f.types
             if q is not None:
                 q[k] = f.charges
+            if tv is not None:
+                tv[k] = f.time

@@ -426,3 +426,64 @@ def linear_kset(box, k_min: float, k_max: float, nbins: int) -> KSet:
     np.add.at(nq, b, 2)
     return KSet(mode="linear", dq=float(dk), nqmax=nbins - 1, vectors=v.astype(np.int32), bins=b.astype(np.int32),
                 weights=w, dense=np.zeros(v.shape[0], np.uint8), nq=nq, qmin_eff=float(k_min))
+
+
+# ---------------------------------------------------------------------------
+# S(Q, w) vectors (sq_init, src/modules/sq.cuf:239-297; FqtnD, src/modules/dynamics.cuf:444-471)
+# ---------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class SqwSet:
+    """Lattice vectors of the qw shells, the shell each one is accumulated into, and nw per shell."""
+    qw: np.ndarray        # (nqw,) FP32 shell centres
+    dq: float             # FP32 shell width
+    vectors: np.ndarray   # (nvec, 3) int32, octant i, j, k >= 0
+    bins: np.ndarray      # (nvec,) int32 shell index 0..nqw-1 (FqtnD's search)
+    nw: np.ndarray        # (nqw,) int64 vectors per shell (sq_init's count)
+
+    @property
+    def nvec(self) -> int:
+        return int(self.vectors.shape[0])
+
+
+def _first_shell(q: np.ndarray, qw: np.ndarray, half: np.float32) -> np.ndarray:
+    """Per element, the first l with qw(l) - dq/2 < q < qw(l) + dq/2 (bounds in FP32, q compared in
+    its own precision), or -1."""
+    out = np.full(q.shape, -1, np.int64)
+    for l in range(qw.size - 1, -1, -1):  # last to first: the first match wins
+        lo, hi = F32(qw[l] - half), F32(qw[l] + half)
+        hit = (q > q.dtype.type(lo)) & (q < q.dtype.type(hi))
+        out[hit] = l
+    return out
+
+
+def sqw_kset(box, qw: Sequence[float], dq: float) -> SqwSet:
+    """The S(Q, w) vector set: lattice vectors with 0 <= i <= nint(qmax/fk_x) (and likewise for j,
+    k), not all zero, whose |k| lies inside a shell qw(l) +- dq/2.  nw counts them per shell with
+    sq_init's FP32 |k| = sqrt((i fk_x)^2 + (j fk_y)^2 + (k fk_z)^2); the shell a vector is added to
+    is FqtnD's: the same FP32 sum of squares, square root in FP64.  The storing loop of sq_init is
+    the one followed (its counting loop takes k = 0 only and allocates too few rows for 3D)."""
+    box = np.asarray(box, F32)
+    qw32 = np.asarray(qw, F32)
+    if qw32.size == 0:
+        raise ValueError("qw: no shells")
+    dq32 = F32(dq)
+    half = F32(dq32 / F32(2))
+    fk = np.array([F32(TWOPI32 / L) for L in box], dtype=F32)
+    qmm = F32(qw32.max())
+    lim = [nint(F32(qmm / fk[d])) for d in range(3)]
+    i, j, k = np.meshgrid(np.arange(lim[0] + 1), np.arange(lim[1] + 1), np.arange(lim[2] + 1), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    keep = (i + j + k) != 0
+    i, j, k = i[keep], j[keep], k[keep]
+    a = (i.astype(F32) * fk[0]).astype(F32)
+    b = (j.astype(F32) * fk[1]).astype(F32)
+    c = (k.astype(F32) * fk[2]).astype(F32)
+    s2 = (((a * a).astype(F32) + (b * b).astype(F32)).astype(F32) + (c * c).astype(F32)).astype(F32)
+    l_init = _first_shell(np.sqrt(s2).astype(F32), qw32, half)
+    nw = np.bincount(l_init[l_init >= 0], minlength=qw32.size).astype(np.int64)
+    l_fqt = _first_shell(np.sqrt(s2.astype(np.float64)), qw32, half)
+    # FqtnD finding no shell for a stored vector would write past its arrays; such vectors are dropped
+    sel = (l_init >= 0) & (l_fqt >= 0)
+    v = np.stack([i[sel], j[sel], k[sel]], axis=1).astype(np.int32)
+    return SqwSet(qw=qw32, dq=float(dq32), vectors=v, bins=l_fqt[sel].astype(np.int32), nw=nw)

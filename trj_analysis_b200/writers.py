@@ -141,3 +141,70 @@ def write_sq(path_dir: str, q: np.ndarray, s_nn: np.ndarray, nq: np.ndarray, s_s
 
 def savetxt_columns(path: str, columns: Iterable[np.ndarray], header: str) -> None:
     np.savetxt(path, np.column_stack(list(columns)), header=header)
+
+
+def format_record(values: Sequence[float], descs: Sequence[tuple]) -> List[str]:
+    """Values written with the F edit descriptors ``descs`` [(width, decimals), ...]; when the list
+    outlasts the format, a new record starts at the format's beginning (reversion to the whole
+    format, which has no inner parentheses)."""
+    lines, cur, k = [], "", 0
+    for v in values:
+        if k == len(descs):
+            lines.append(cur)
+            cur, k = "", 0
+        w, d = descs[k]
+        cur += fmt_f(v, w, d)
+        k += 1
+    lines.append(cur)
+    return lines
+
+
+ROW_T8 = [(10, 3)] + [(15, 5)] * 8            # '(f10.3,8f15.5)'
+ROW_2T8 = [(10, 3), (10, 3)] + [(15, 5)] * 8  # '(2f10.3,8f15.5)'
+
+
+def write_dynamics(path_dir: str, res: dict, units: str = "lj") -> List[str]:
+    """print_rtcor (src/modules/dynamics.cuf:278-393) without velocities or stresses:
+    dyn.dat   '#',2x,'t(tau)',9x,'C_r(t)'                  rows (f10.3,8f15.5) t, C_r, i <= itlimit
+    fkt.dat   '#',2x,'t(tau)',9x,8('F(',f6.4,',t)',4x:)    rows (f10.3,8f15.5) t, F(q_1..q_nqw, t)
+    fskt.dat  the same with 'Fs('
+    sqw.dat   '#',2x,'w(1/tau)',5x,8('S(',f6.4,',w)    Ss(',f6.4,',w)',4x:)
+              rows (f10.3,8f15.5) w/2pi, S(q_1,w), Ss(q_1,w), ... for every lag row;
+    other units: 't(ps)', and sqw.dat '#',2x,'w(THz)',7x,'w(meV)',5x,... rows (2f10.3,8f15.5)
+    with w/2pi and 4.135 w/2pi."""
+    import os
+    lj = units == "lj"
+    tl = "t(tau)" if lj else "t(ps)"
+    t, qw = res["t"], res["qw"]
+    ndyn = t.shape[0]
+    rows_t = [i for i in range(ndyn) if i + 1 <= res["itlimit"]]
+    files = []
+
+    def emit(name, lines):
+        p = os.path.join(path_dir, name)
+        with open(p, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        files.append(p)
+
+    emit("dyn.dat", ["#  " + tl + " " * 9 + "C_r(t)"] +
+         [ln for i in rows_t for ln in format_record([t[i], res["r2t"][i]], ROW_T8)])
+    for name, key, lab in (("fkt.dat", "fkt", "F("), ("fskt.dat", "fskt", "Fs(")):
+        head = _group_header("#  " + tl + " " * 9, [f"{lab}{fmt_f(q, 6, 4)},t)" for q in qw], 8, " " * 4)
+        emit(name, head + [ln for i in rows_t for ln in format_record([t[i]] + list(res[key][i]), ROW_T8)])
+    pi = np.float32(3.141592653589793)
+    twopi = np.float32(np.float32(2) * pi)
+    labels = [f"S({fmt_f(q, 6, 4)},w)    Ss({fmt_f(q, 6, 4)},w)" for q in qw]
+    if lj:
+        head = _group_header("#  w(1/tau)" + " " * 5, labels, 8, " " * 4)
+    else:
+        head = _group_header("#  w(THz)" + " " * 7 + "w(meV)" + " " * 5, labels, 8, " " * 4)
+    lines = []
+    for i in range(ndyn):
+        f = np.float32(res["w"][i] / twopi)
+        vals = [v for j in range(len(qw)) for v in (res["sqw"][i, j], res["ssqw"][i, j])]
+        if lj:
+            lines.extend(format_record([f] + vals, ROW_T8))
+        else:
+            lines.extend(format_record([f, np.float32(np.float32(4.135) * res["w"][i] / twopi)] + vals, ROW_2T8))
+    emit("sqw.dat", head + lines)
+    return files
