@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--serving", type=int, default=200, help="requests in the serving run (0: skip)")
+    ap.add_argument("--row", default="main", choices=["main", "charges", "dyn"],
+                    help="main: the g(r)+S(Q) frame rate; charges: the same frames with per-atom charges "
+                         "(g_qq, S_qq); dyn: F(Q,t)/Fs(Q,t)/MSD over time origins")
     return ap.parse_args()
 
 
@@ -432,8 +435,142 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ---------------------------------------------------------------------------
+# secondary rows: charge-weighted columns, time correlations
+# ---------------------------------------------------------------------------
+
+def _events(fn, reps, flush):
+    import torch
+    out = []
+    for i in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn(i)
+        b.record()
+        if flush is not None:
+            flush.zero_()
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def run_charges(args):
+    """The benchmark frame with per-atom charges (species charges 1, -0.8, 0.5 plus a 0.05 spread):
+    pack with charges, g(r) with g_qq, S(Q) with S_qq, against the same frames without charges."""
+    import ctypes
+    import torch
+    from trj_analysis_b200 import _lib, engine, frames, refsem
+    wl = dict(WORKLOADS[args.workload])
+    spec = frames.WORKLOADS[wl["spec"]]()
+    spec.charges = (1.0, -0.8, 0.5, 0.3)[:len(wl["bsc"])]
+    spec.charge_jitter = 0.05
+    fr = [spec.frame(i) for i in range(3)]
+    n, box, nsp = fr[0].n, fr[0].box, len(wl["bsc"])
+    ctx = engine.Context(0)
+    dev = ctx.torch_device
+    d = [(torch.from_numpy(f.xyz).to(dev), torch.from_numpy((f.types - 1).astype(np.int32)).to(dev),
+          torch.from_numpy(f.charges).to(dev)) for f in fr]
+    packed = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    qpacked = torch.empty((n,), dtype=torch.float32, device=dev)
+    counts = torch.zeros(nsp, dtype=torch.int64, device=dev)
+    rdf = engine.RdfPlan(ctx, nsp, wl["deltar"], wl["rcrdf"], box, n)
+    hist, gqq = rdf.new_hist(), rdf.new_gqq()
+    ks = refsem.make_kset(wl["kset"], box, wl["qmax"], wl["qmin"], seed=0)
+    cnt = np.bincount(fr[0].types - 1, minlength=nsp)
+    sq, sqc = engine.SqPlan(ctx, nsp, ks, cnt), engine.SqPlan(ctx, nsp, ks, cnt, charged=True)
+    out, outc = sq.new_out(), sqc.new_out()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    M = engine.METHODS[args.method]
+    res = {}
+    for charged in (False, True):
+        def step(i, charged=charged):
+            x, spc, q = d[i % 3]
+            engine.pack_frame(ctx, x, spc, nsp, box, packed, counts, charges=q if charged else None,
+                              qpacked=qpacked)
+            if charged:
+                rdf.accumulate(packed, n, box, hist, qpacked=qpacked, gqq=gqq)
+                sqc.accumulate(packed, n, box, outc, M, qpacked=qpacked)
+            else:
+                rdf.accumulate(packed, n, box, hist)
+                sq.accumulate(packed, n, box, out, M)
+        _events(step, args.warmup, flush)
+        ctx.check()
+        ctx.lib.trj_ctx_set_timing(ctx.h, 1)
+        r_ms, s_ms = [], []
+
+        def timed(i, step=step, charged=charged):
+            step(i)
+            v = ctypes.c_float()
+            _lib.check(ctx.lib.trj_rdf_kernel_ms(rdf.h, ctypes.byref(v)), ctx.h)
+            r_ms.append(v.value)
+            _lib.check(ctx.lib.trj_sq_kernel_ms((sqc if charged else sq).h, ctypes.byref(v)), ctx.h)
+            s_ms.append(v.value)
+        ms = _events(timed, args.steps, flush)
+        ctx.lib.trj_ctx_set_timing(ctx.h, 0)
+        ctx.check()
+        res["charged" if charged else "uncharged"] = {
+            "frame_ms": statistics.median(ms), "pair_kernel_ms": statistics.median(r_ms),
+            "sq_kernel_ms": statistics.median(s_ms)}
+    c = res["charged"]
+    return {"metric": "g(r)+g_qq+S(Q)+S_qq frames/s, per-atom charges", "value": 1000.0 / c["frame_ms"],
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": c["frame_ms"], "higher_is_better": True, "dtype": "f32/f64",
+            "data": "synthetic", "config": {"workload": args.workload + "+charges", "n_atoms": n,
+                                              "method": args.method, "l2": "flushed between steps"},
+            "detail": res}
+
+
+def run_dyn(args):
+    """F(Q,t), Fs(Q,t) and the MSD over time origins: N = 62,500 (the binary c2 shape), a random walk
+    of 0.2 per axis per frame, 30 frames, 10 buffers one frame apart, shells qw = 1, 2, 4, 7."""
+    import ctypes
+    import torch
+    from trj_analysis_b200 import _lib, dynamics, engine, frames
+    spec = frames.FCCSpec(cells=(25, 25, 25), sigma=0.1, fractions=(0.8, 0.2), seed=2)
+    nconf, nbuf = 30, 10
+    frs = list(frames.random_walk_frames(spec, nconf, 0.2))
+    n, box = frs[0].n, frs[0].box
+    ctx = engine.Context(0)
+    stage = engine.FrameStage(ctx, n, 2)
+    dyn = dynamics.Dynamics(ctx, 2, n, nconf, dynamics.DynConfig(nbuffer=nbuf, jump=1, qw=(1.0, 2.0, 4.0, 7.0)),
+                            box, np.array([1.0, 0.6], np.float32))
+    ctx.lib.trj_ctx_set_timing(ctx.h, 1)
+    ms, kms, terms = [], [], []
+    for iconf in range(1, nconf + 1):
+        f = frs[iconf - 1]
+        nn = stage.upload_and_pack(f.xyz, f.types - 1, box)
+        lags, origins = dyn.sched.schedule(iconf, f.time)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        dyn.plan.accumulate(stage.packed, nn, box, lags, origins)
+        b.record()
+        done = dyn.sched.finish_frame(iconf)
+        if done.any():
+            dyn.plan.flush(done, dyn.fkt, dyn.fskt, dyn.r2t)
+        torch.cuda.synchronize()
+        v = ctypes.c_float()
+        _lib.check(ctx.lib.trj_dyn_kernel_ms(dyn.plan.h, ctypes.byref(v)), ctx.h)
+        if iconf > nbuf:  # every buffer active
+            ms.append(a.elapsed_time(b))
+            kms.append(v.value)
+            terms.append(int((lags >= 0).sum()) * n * dyn.sqw.nvec)
+    ctx.check()
+    self_tps = float(np.median(np.array(terms) / (np.array(kms) * 1e-3)))
+    return {"metric": "F(Q,t)+Fs(Q,t)+MSD frames/s (10 time origins)", "value": 1000.0 / statistics.median(ms),
+            "unit": "frames/s", "n_gpus": 1, "steps": len(ms), "warmup": nbuf, "ms_per_step": statistics.median(ms),
+            "higher_is_better": True, "dtype": "f32 terms, f64 sums", "data": "synthetic",
+            "config": {"workload": "random walk N=62500, 30 frames, nbuffer 10, qw 1/2/4/7",
+                       "n_atoms": n, "nvec": dyn.sqw.nvec},
+            "self_kernel": {"ms": statistics.median(kms), "terms_per_s": self_tps,
+                            "terms_per_clk_per_sm": self_tps / (ctx.sm_count * 1.9e9)}}
+
+
 def main():
     args = parse()
+    if args.row != "main":
+        res = run_charges(args) if args.row == "charges" else run_dyn(args)
+        print(json.dumps(res), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

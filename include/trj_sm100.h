@@ -175,6 +175,18 @@ TRJ_API int trj_rdf_accumulate(trj_rdf_plan* plan, const float* packed_dev, int6
 TRJ_API int trj_rdf_accumulate_charged(trj_rdf_plan* plan, const float* packed_dev, const float* charge_packed_dev,
                                        int64_t n, const float box[3], uint64_t* hist_dev, uint64_t* edge_dev,
                                        double* gqq_dev, void* stream);
+/* Number fluctuations of the frame last passed to trj_rdf_accumulate on this
+ * plan (s2D3_sh, src/modules/rdf.cuf:489-553, run by RDFcomp when nrandom > 0):
+ * nrandom points, point b drawn with the reference's generator and seed
+ * (curand XORWOW, curand_init(b + 12345, 0, 0), b = 1..nrandom; x = L_x *
+ * curand_uniform, then y, z), the same points every frame; for each point N_k =
+ * atoms with FP32 minimum-image distance r, r^2 < side2 and nint(r/deltar) <= k,
+ * k = 0..lsmax; adds sum over points of N_k to gi_dev[k] and of N_k^2 to
+ * g2i_dev[k] (uint64 [lsmax+1]; exact, where the reference sums FP32).
+ * points_dev: NULL, or nrandom x 3 floats out (the sample points).
+ * s2n(r_k) = g2i[k]/(Nconf nrandom) - (gi[k]/(Nconf nrandom))^2 (log.f90:532). */
+TRJ_API int trj_rdf_s2n(trj_rdf_plan* plan, int nrandom, uint64_t* gi_dev, uint64_t* g2i_dev, float* points_dev,
+                        void* stream);
 /* Duration (ms) of the last cell-pair kernel launch; needs trj_ctx_set_timing(ctx, 1). */
 TRJ_API int trj_rdf_kernel_ms(trj_rdf_plan* plan, float* ms);
 TRJ_API int trj_rdf_plan_destroy(trj_rdf_plan* plan);

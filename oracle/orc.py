@@ -146,6 +146,33 @@ def rho_charge_fp64(pos: np.ndarray, charges: np.ndarray, box, vectors: np.ndarr
     return out[0, :, 0] + 1j * out[0, :, 1]
 
 
+def s2n_counts(pos: np.ndarray, box, side2: float, deltar: float, lsmax: int, points: np.ndarray):
+    """s2D3_sh (rdf.cuf:489-553) for given sample points: per point, atoms with FP32 minimum-image
+    distance r (difference point - atom, (x^2 + y^2) + z^2), r^2 < side2, binned at nint(r/deltar) and
+    made cumulative (gi_s(ind:lsmax) += 1); returns the int64 sums over points of N_k and N_k^2."""
+    pos = np.ascontiguousarray(pos, F32)
+    L = np.asarray(box, F32)
+    gi = np.zeros(lsmax + 1, np.int64)
+    g2i = np.zeros(lsmax + 1, np.int64)
+
+    def roundf(x):
+        x = np.asarray(x, np.float64)
+        return np.trunc(x + np.copysign(0.5, x)).astype(F32)
+
+    for p in np.asarray(points, F32).reshape(-1, 3):
+        d = (p[None, :] - pos).astype(F32)
+        d = (d - (L * roundf((d / L).astype(F32))).astype(F32)).astype(F32)
+        sq = (d * d).astype(F32)
+        rr2 = ((sq[:, 0] + sq[:, 1]).astype(F32) + sq[:, 2]).astype(F32)
+        ok = rr2 < F32(side2)
+        ind = roundf((np.sqrt(rr2[ok]).astype(F32) / F32(deltar)).astype(F32)).astype(np.int64)
+        h = np.bincount(ind[(ind >= 0) & (ind <= lsmax)], minlength=lsmax + 1)[:lsmax + 1]
+        nk = np.cumsum(h).astype(np.int64)
+        gi += nk
+        g2i += nk * nk
+    return gi, g2i
+
+
 def rdf_counts_range(pos, species, box, side2, deltar, lsmax, nsp, i0, i1):
     """Linked-cell counts of pairs (i, j>i) with home atom i in [i0, i1)."""
     pos = np.ascontiguousarray(pos, F32)

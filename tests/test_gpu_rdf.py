@@ -152,3 +152,56 @@ def test_pack_matches_oracle_layout(ctx):
     assert np.array_equal(got[:, :3], pos)
     assert np.array_equal(got[:, 3].view(np.int32), sp)
     assert np.array_equal(stage.counts.cpu().numpy(), np.diff(off))
+
+
+@pytest.mark.parametrize("cells,nrandom", [((8, 8, 8), 64), ((3, 3, 3), 9), ((10, 10, 4), 33)])
+def test_s2n_matches_oracle(cells, nrandom):
+    """Number fluctuations: exact int64 sums against the oracle at the GPU's own sample points; the points
+    are the same every frame and lie in the box."""
+    import torch
+    from oracle import orc
+    from trj_analysis_b200 import engine, frames, refsem
+    ctx = engine.Context(0)
+    spec = frames.FCCSpec(cells=cells, sigma=0.1, fractions=(0.5, 0.5), seed=7)
+    frs = [spec.frame(i) for i in range(2)]
+    box = frs[0].box
+    stage = engine.FrameStage(ctx, frs[0].n, 2)
+    plan = engine.RdfPlan(ctx, 2, 0.05, 0.0, box, frs[0].n)
+    hist = plan.new_hist()
+    gi, g2i = plan.new_s2n()
+    want_gi = np.zeros(plan.lsmax + 1, np.int64)
+    want_g2i = np.zeros(plan.lsmax + 1, np.int64)
+    pts_seen = []
+    for fr in frs:
+        n = stage.upload_and_pack(fr.xyz, fr.types - 1, box)
+        plan.accumulate(stage.packed, n, box, hist)
+        pts = torch.zeros(3 * nrandom, dtype=torch.float32, device=ctx.torch_device)
+        plan.s2n(nrandom, gi, g2i, points=pts)
+        p = pts.cpu().numpy().reshape(-1, 3)
+        pts_seen.append(p)
+        pos, sp, off = orc.layout(fr.xyz, fr.types - 1, box, 2)
+        a, b = orc.s2n_counts(pos, box, plan.side2, 0.05, plan.lsmax, p)
+        want_gi += a
+        want_g2i += b
+    ctx.check()
+    np.testing.assert_array_equal(pts_seen[0], pts_seen[1])
+    assert np.all(pts_seen[0] > 0) and np.all(pts_seen[0] <= box)
+    assert len(np.unique(pts_seen[0][:, 0])) == nrandom
+    np.testing.assert_array_equal(gi.cpu().numpy(), want_gi)
+    np.testing.assert_array_equal(g2i.cpu().numpy(), want_g2i)
+    assert want_gi[-1] > 0
+    plan.close()
+    ctx.close()
+
+
+def test_session_writes_s2n(tmp_path):
+    from trj_analysis_b200 import analysis
+    spec = frames.FCCSpec(cells=(6, 6, 6), sigma=0.1, seed=8)
+    cfg = analysis.Config(nsp=1, sp_types_selected=(1,), run_sq=False, deltar=0.05, nrandom=24)
+    s = analysis.Session(cfg).run(list(spec.frames(3)))
+    files = s.printrdf(str(tmp_path))
+    assert files[-1].endswith("s2n.dat")
+    res = s.rdf_results()
+    assert res["s2n"].shape == res["r"].shape and np.all(np.isfinite(res["s2n"]))
+    assert np.all(res["s2n"] >= -1e-9)  # a variance
+    s.close()

@@ -194,3 +194,35 @@ def test_linear_kset_counts():
     q = np.sqrt(((g * fk) ** 2).sum(1))
     sel = (q >= fk) & (q < 2.0)
     assert ks.nq.sum() == sel.sum()
+
+
+def test_s2n_normalisation_and_file(tmp_path):
+    from trj_analysis_b200 import analysis
+    lsmax, nconf, nrandom = 8, 3, 4
+    gi = np.arange(lsmax + 1, dtype=np.int64) * 12
+    g2i = gi * gi // 10 + 7
+    s = analysis.normalise_s2n(gi, g2i, nconf, nrandom, lsmax)
+    m = nconf * nrandom
+    np.testing.assert_allclose(s, g2i[1:lsmax - 1] / m - (gi[1:lsmax - 1] / m) ** 2)
+    r = np.arange(1, lsmax - 1, dtype=np.float32) * np.float32(0.1)
+    p = writers.write_s2n(str(tmp_path), r, s)
+    lines = open(p).read().splitlines()
+    assert lines[0] == "#       r                s2n"
+    assert lines[1] == writers.fmt_f(r[0], 16, 5) + writers.fmt_f(s[0], 16, 5)
+    assert len(lines) == 1 + lsmax - 2
+
+
+def test_oracle_s2n_counts_small_case():
+    """Two atoms around one point: cumulative counts from the bins nint(r/deltar)."""
+    from oracle import orc
+    box = np.array([10.0, 10.0, 10.0], np.float32)
+    pos = np.array([[1.0, 1.0, 1.0], [1.0, 1.0, 1.55], [9.9, 1.0, 1.0]], np.float32)
+    gi, g2i = orc.s2n_counts(pos, box, 4.0, 0.1, 25, np.array([[1.0, 1.0, 1.0]], np.float32))
+    # distances 0 (bin 0); 1.0 - 1.55 = -0.54999995 in FP32, /0.1 = 5.4999995 -> bin 5; 1.1000004 through
+    # the boundary -> bin 11
+    want = np.zeros(26, np.int64)
+    want[0:] += 1
+    want[5:] += 1
+    want[11:] += 1
+    np.testing.assert_array_equal(gi, want)
+    np.testing.assert_array_equal(g2i, want * want)

@@ -57,6 +57,7 @@ SIGNATURES = {
     "trj_rdf_accumulate": (c_int, [vp, vp, c_int64, P(c_float), vp, vp, vp]),
     "trj_rdf_accumulate_charged": (c_int, [vp, vp, vp, c_int64, P(c_float), vp, vp, vp, vp]),
     "trj_rdf_plan_destroy": (c_int, [vp]),
+    "trj_rdf_s2n": (c_int, [vp, c_int, vp, vp, vp, vp]),
     "trj_sq_plan_create": (c_int, [vp, c_int, c_int64, vp, vp, vp, vp, c_int, P(c_int64), P(vp)]),
     "trj_sq_plan_create_charged": (c_int, [vp, c_int, c_int64, vp, vp, vp, vp, c_int, P(c_int64), P(vp)]),
     "trj_sq_plan_info": (c_int, [vp, P(c_int64), P(c_int64), P(c_int64), P(c_int64)]),

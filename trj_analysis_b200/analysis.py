@@ -42,6 +42,7 @@ class Config:
     run_sq: bool = True
     deltar: float = 0.02
     rcrdf: float = 0.0             # <= 0: half the smallest box edge
+    nrandom: int = 0               # /INPUT_RDF/ nrandom: random points for the number fluctuations s2n(r)
     qmax: float = 10.0
     qmin: float = 3.0
     bsc: Optional[Sequence[float]] = None   # per sp_types_selected entry; default 1.0
@@ -91,6 +92,7 @@ class Session:
         self.n = 0
         self.ex_qc = None      # frames carry charges (set by the first frame, netcdf.f90:404-408)
         self.gqq = None        # FP64 [lsmax] charge-product histogram over avq2, summed over frames
+        self.gi = self.g2i = None  # uint64 [lsmax+1] number-fluctuation sums (nrandom > 0)
         self.charges = None    # charges of the last frame (FP32, selected atoms)
         self.species_q = None  # charge of each species (charge_mode "species")
 
@@ -171,11 +173,15 @@ class Session:
         self.edge = torch.zeros(4, dtype=torch.int64, device=self.ctx.torch_device)
         if self.device_charges:
             self.gqq = self.rdf.new_gqq()
+        if self.cfg.nrandom > 0:
+            self.gi, self.g2i = self.rdf.new_s2n()
 
     def RDFcomp(self) -> None:
         dq = self.device_charges
         self.rdf.accumulate(self.stage.packed, self.n, self.box, self.hist, self.edge, stream=self.stream,
                             qpacked=self.stage.qpacked if dq else None, gqq=self.gqq)
+        if self.cfg.nrandom > 0 and self.n >= 2:  # s2D3_sh after rdf_sh (rdf.cuf:243-245)
+            self.rdf.s2n(self.cfg.nrandom, self.gi, self.g2i, stream=self.stream)
 
     # ---- S(Q) -----------------------------------------------------------------------
     def sq_init(self) -> None:
@@ -264,8 +270,12 @@ class Session:
         return float(F32(np.sum(q * q) / q.shape[0]))
 
     def rdf_results(self) -> Dict[str, np.ndarray]:
-        return normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
-                             self.ntype, self.nconf, gqq=self.gqq_transfer())
+        res = normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
+                            self.ntype, self.nconf, gqq=self.gqq_transfer())
+        if self.gi is not None:
+            res["s2n"] = normalise_s2n(self.gi.cpu().numpy(), self.g2i.cpu().numpy(), self.nconf, self.cfg.nrandom,
+                                       self.rdf.lsmax)
+        return res
 
     def sq_results(self) -> Dict[str, np.ndarray]:
         if not self.ex_qc:
@@ -275,7 +285,10 @@ class Session:
 
     def printrdf(self, outdir: str = ".") -> List[str]:
         res = self.rdf_results()
-        return writers.write_gmixsim(outdir, res["r"], res["g"], self.cfg.nsp, g_qq=res.get("g_qq"))
+        files = writers.write_gmixsim(outdir, res["r"], res["g"], self.cfg.nsp, g_qq=res.get("g_qq"))
+        if "s2n" in res:
+            files.append(writers.write_s2n(outdir, res["r"], res["s2n"]))
+        return files
 
     def printSQ(self, outdir: str = ".") -> List[str]:
         res = self.sq_results()
@@ -322,6 +335,14 @@ def normalise_rdf(hist: np.ndarray, nsp: int, lsmax: int, deltar: float, volumen
     if gqq is not None:
         res["g_qq"] = 2.0 * volumen * np.asarray(gqq, np.float64)[:nrow] / (n * n * dv[:nrow] * nconf)
     return res
+
+
+def normalise_s2n(gi: np.ndarray, g2i: np.ndarray, nconf: int, nrandom: int, lsmax: int) -> np.ndarray:
+    """s2n(r_i) = g2i(i)/(Nconf nrandom) - (gi(i)/(Nconf nrandom))^2 for i = 1..lsmax-2 (log.f90:532), FP64."""
+    m = float(nconf * nrandom)
+    g = gi.astype(np.float64)[1:lsmax - 1]
+    g2 = g2i.astype(np.float64)[1:lsmax - 1]
+    return g2 / m - (g / m) ** 2
 
 
 def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, natms: int) -> float:

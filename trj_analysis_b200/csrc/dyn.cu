@@ -395,7 +395,11 @@ extern "C" int trj_dyn_plan_create(trj_ctx* ctx, int nsp, int64_t n, int nbuffer
     const int64_t target = (int64_t)ctx->sm_count * 8;
     const int64_t by_atoms = std::max<int64_t>(1, n / kDynChunk);
     p->nsplit_rho = (int)std::min<int64_t>(by_atoms, std::max<int64_t>(1, (target + p->gx - 1) / p->gx));
-    p->nsplit_cap = (int)(nbuffer + std::min<int64_t>(by_atoms, target));
+    // self-term partial rows (splits x buffers): enough for every buffer to split as far as the atoms
+    // allow, within 256 MB of partials
+    const int64_t split_max = std::min<int64_t>(by_atoms, target);
+    const int64_t rows_budget = std::max<int64_t>(nbuffer, ((int64_t)256 << 20) / (8 * std::max<int64_t>(nvec, 1)));
+    p->nsplit_cap = (int)std::min<int64_t>((int64_t)nbuffer * split_max, std::max<int64_t>(rows_budget, nbuffer));
     std::vector<int4> vecs(nvec);
     std::vector<int32_t> start(nbins + 1, 0), bv(nvec);
     for (int64_t v = 0; v < nvec; ++v) {

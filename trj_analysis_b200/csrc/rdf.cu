@@ -16,6 +16,7 @@
 // Neighbour-cell atoms are staged into shared memory with 1-D TMA bulk copies
 // (cp.async.bulk, no multicast), double-buffered on mbarriers; each warp counts into its own
 // uint32 shared histogram replica; replicas are merged with 64-bit global atomics at exit.
+#include <curand_kernel.h>
 #include <math.h>
 
 #include <algorithm>
@@ -450,6 +451,78 @@ __global__ void scan_exclusive_kernel(const int32_t* __restrict__ in, int32_t* _
     if (threadIdx.x == blockDim.x - 1) out[n] = part[threadIdx.x];
 }
 
+// Number fluctuations (s2D3_sh, rdf.cuf:489-553): block b draws one point uniformly in the box with
+// the reference's generator and seed (XORWOW, curand_init(b + 12345, 0, 0), b 1-based), counts the
+// atoms within each radius r_k = k*deltar (cumulative over nint(r/deltar) bins, the reference's
+// gi_s(ind:lsmax) += 1) from the cells around it, and adds N_k and N_k^2 to the int64 sums.
+__global__ void s2n_kernel(const float4* __restrict__ sorted, const int32_t* __restrict__ cstart,
+                           const int32_t* __restrict__ ccount, float Lx, float Ly, float Lz, int ncx, int ncy,
+                           int ncz, float side2, float deltar, int lsmax, unsigned long long* __restrict__ gi,
+                           unsigned long long* __restrict__ g2i, float* __restrict__ points) {
+    extern __shared__ unsigned long long cnt[];  // lsmax + 1
+    __shared__ float pt[3];
+    for (int k = threadIdx.x; k <= lsmax; k += blockDim.x) cnt[k] = 0ull;
+    if (threadIdx.x == 0) {
+        curandStateXORWOW_t h;
+        curand_init((unsigned long long)blockIdx.x + 1ull + 12345ull, 0ull, 0ull, &h);
+        pt[0] = Lx * curand_uniform(&h);
+        pt[1] = Ly * curand_uniform(&h);
+        pt[2] = Lz * curand_uniform(&h);
+        if (points) {
+            points[3 * blockIdx.x] = pt[0];
+            points[3 * blockIdx.x + 1] = pt[1];
+            points[3 * blockIdx.x + 2] = pt[2];
+        }
+    }
+    __syncthreads();
+    const float L[3] = {Lx, Ly, Lz};
+    const int nc[3] = {ncx, ncy, ncz};
+    int pc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {  // the point's cell, as cell_assign_kernel bins an atom
+        const float w = pt[d] - L[d] * floorf(pt[d] / L[d]);
+        int c = (int)(w * ((float)nc[d] / L[d]));
+        pc[d] = c < 0 ? 0 : (c >= nc[d] ? nc[d] - 1 : c);
+    }
+    const int rx = ncx > 1 ? 1 : 0, ry = ncy > 1 ? 1 : 0, rz = ncz > 1 ? 1 : 0;
+    for (int dx = -rx; dx <= rx; ++dx)
+        for (int dy = -ry; dy <= ry; ++dy)
+            for (int dz = -rz; dz <= rz; ++dz) {
+                const int cx = (pc[0] + dx + ncx) % ncx, cy = (pc[1] + dy + ncy) % ncy, cz = (pc[2] + dz + ncz) % ncz;
+                const int c = (cx * ncy + cy) * ncz + cz;
+                const int a0 = cstart[c], na = ccount[c];
+                for (int j = threadIdx.x; j < na; j += blockDim.x) {
+                    const float4 a = sorted[a0 + j];
+                    // rdf.cuf:533-541: difference point - atom, minimum image, (x^2 + y^2) + z^2, FP32
+                    float xd = __fsub_rn(pt[0], a.x), yd = __fsub_rn(pt[1], a.y), zd = __fsub_rn(pt[2], a.z);
+                    xd = __fsub_rn(xd, __fmul_rn(Lx, roundf(__fdiv_rn(xd, Lx))));
+                    yd = __fsub_rn(yd, __fmul_rn(Ly, roundf(__fdiv_rn(yd, Ly))));
+                    zd = __fsub_rn(zd, __fmul_rn(Lz, roundf(__fdiv_rn(zd, Lz))));
+                    const float rr2 = __fadd_rn(__fadd_rn(__fmul_rn(xd, xd), __fmul_rn(yd, yd)), __fmul_rn(zd, zd));
+                    if (rr2 < side2) {
+                        const int ind = (int)roundf(__fdiv_rn(__fsqrt_rn(rr2), deltar));
+                        if (ind >= 0 && ind <= lsmax) atomicAdd(&cnt[ind], 1ull);
+                    }
+                }
+            }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // cumulative counts N_k = sum_{j <= k} cnt[j]
+        unsigned long long run = 0;
+        for (int k = 0; k <= lsmax; ++k) {
+            run += cnt[k];
+            cnt[k] = run;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k <= lsmax; k += blockDim.x) {
+        const unsigned long long v = cnt[k];
+        if (v) {
+            atomicAdd(&gi[k], v);
+            atomicAdd(&g2i[k], v * v);
+        }
+    }
+}
+
 }  // namespace
 
 struct trj_rdf_plan {
@@ -468,6 +541,8 @@ struct trj_rdf_plan {
     int32_t* aslot = nullptr;   // n_max
     float4* sorted = nullptr;   // n_max
     float* sorted_q = nullptr;  // n_max charges in cell order (first charged call)
+    int cells_valid = 0;        // sorted/cstart/ccount hold the last accumulated frame
+    float box_last[3] = {0.f, 0.f, 0.f};
     double* gqq_frame = nullptr;  // lsmax: this frame's charge-product sums
     int64_t scratch_bytes = 0;
     trj_kernel_timer timer;
@@ -626,6 +701,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
         plan->gqq_frame = reinterpret_cast<double*>(qb + ((nq * sizeof(float) + 255) & ~(size_t)255));
         plan->scratch_bytes += (int64_t)qbytes;
     }
+    plan->cells_valid = 0;
     if (n < 2) {
         // No pair; gqq still receives 0/avq2 per bin, as the reference adds gqq_d/avq2 every frame.
         if (charged && n == 1) {
@@ -663,7 +739,10 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     if (P.ncell > plan->ncell_cap)
         return trj_fail(ctx, TRJ_ERR_CAPACITY, "rdf accumulate: %d cells exceed plan capacity %d", P.ncell,
                         plan->ncell_cap);
-    for (int d = 0; d < 3; ++d) plan->nc[d] = P.nc[d];
+    for (int d = 0; d < 3; ++d) {
+        plan->nc[d] = P.nc[d];
+        plan->box_last[d] = box[d];
+    }
     // Half-shell stencil over the split axes: (0,0,0) first, then offsets > 0 lexicographically.
     int no = 0;
     P.off[no][0] = P.off[no][1] = P.off[no][2] = 0;
@@ -735,6 +814,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
             P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work, (unsigned long long*)hist_dev,
             (unsigned long long*)edge_dev, ctx->status_dev, nullptr, nullptr);
     plan->timer.end(ctx, s);
+    plan->cells_valid = 1;
     ctx->launches += 4;
     if (charged) {
         gqq_finish_kernel<<<1, 1024, 0, s>>>(charge_dev, n, plan->gqq_frame, plan->lsmax, gqq_dev);
@@ -755,4 +835,29 @@ extern "C" int trj_rdf_accumulate_charged(trj_rdf_plan* plan, const float* packe
     if (!plan) return TRJ_ERR_INVALID;
     if (!gqq_dev) return trj_fail(plan->ctx, TRJ_ERR_INVALID, "rdf accumulate (charged): null gqq");
     return rdf_accumulate_impl(plan, packed_dev, charge_dev, n, box, hist_dev, edge_dev, gqq_dev, stream);
+}
+
+extern "C" int trj_rdf_s2n(trj_rdf_plan* plan, int nrandom, uint64_t* gi_dev, uint64_t* g2i_dev, float* points_dev,
+                           void* stream) {
+    if (!plan) return TRJ_ERR_INVALID;
+    trj_ctx* ctx = plan->ctx;
+    if (nrandom < 0 || !gi_dev || !g2i_dev) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf s2n: bad arguments");
+    if (plan->floor_bins)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf s2n: needs the reference's nint bins (not a floor-bin plan)");
+    if (!plan->cells_valid)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "rdf s2n: no frame accumulated (call trj_rdf_accumulate first)");
+    if (nrandom == 0) return TRJ_OK;
+    trj_device_guard g(ctx->device);
+    const size_t smem = sizeof(unsigned long long) * (size_t)(plan->lsmax + 1);
+    if (smem > (size_t)ctx->smem_optin - 64)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf s2n: lsmax=%d too large", plan->lsmax);
+    if (smem > 48 * 1024)
+        TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(s2n_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    s2n_kernel<<<(unsigned)nrandom, 256, smem, (cudaStream_t)stream>>>(
+        plan->sorted, plan->cstart, plan->ccount, plan->box_last[0], plan->box_last[1], plan->box_last[2],
+        plan->nc[0], plan->nc[1], plan->nc[2], plan->side2, plan->deltar, plan->lsmax,
+        (unsigned long long*)gi_dev, (unsigned long long*)g2i_dev, points_dev);
+    ctx->launches += 1;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
 }

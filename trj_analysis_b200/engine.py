@@ -138,6 +138,21 @@ class RdfPlan:
                                                      _ptr(hist), _ptr(edge), _ptr(gqq), _stream(stream))
         check(rc, self.ctx.h, "trj_rdf_accumulate_charged")
 
+    def new_s2n(self):
+        """(gi, g2i): uint64 [lsmax+1] sums of N_k and N_k^2 over sample points and frames."""
+        dev = self.ctx.torch_device
+        return (torch.zeros((self.lsmax + 1,), dtype=torch.int64, device=dev),
+                torch.zeros((self.lsmax + 1,), dtype=torch.int64, device=dev))
+
+    def s2n(self, nrandom: int, gi: torch.Tensor, g2i: torch.Tensor, points: Optional[torch.Tensor] = None,
+            stream=None) -> None:
+        """Number fluctuations around nrandom fixed random points for the frame last accumulated."""
+        assert gi.dtype == g2i.dtype == torch.int64 and gi.numel() == g2i.numel() == self.lsmax + 1
+        if points is not None:
+            assert points.dtype == torch.float32 and points.numel() >= 3 * nrandom
+        rc = self.ctx.lib.trj_rdf_s2n(self.h, int(nrandom), _ptr(gi), _ptr(g2i), _ptr(points), _stream(stream))
+        check(rc, self.ctx.h, "trj_rdf_s2n")
+
     def close(self) -> None:
         if getattr(self, "h", None):
             self.ctx.lib.trj_rdf_plan_destroy(self.h)

@@ -208,3 +208,15 @@ def write_dynamics(path_dir: str, res: dict, units: str = "lj") -> List[str]:
             lines.extend(format_record([f, np.float32(np.float32(4.135) * res["w"][i] / twopi)] + vals, ROW_2T8))
     emit("sqw.dat", head + lines)
     return files
+
+
+def write_s2n(path_dir: str, r: np.ndarray, s2n: np.ndarray) -> str:
+    """s2n.dat of printrdf (log.f90:449, 482, 532): header '#       r',16x,'s2n', rows '(18f16.5)' r, s2n."""
+    import os
+    lines = ["#       r" + " " * 16 + "s2n"]
+    for i in range(r.shape[0]):
+        lines.extend(_records([r[i], s2n[i]], 18, 16, 5))
+    p = os.path.join(path_dir, "s2n.dat")
+    with open(p, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return p
