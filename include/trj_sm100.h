@@ -145,6 +145,13 @@ TRJ_API int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const int3
  * n_max: largest frame the plan will accept. */
 TRJ_API int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
                         int64_t n_max, trj_rdf_plan** out);
+/* Plan for two-dimensional frames (ndim = 2; rdf2_sh, rdf.cuf:617-670, and
+ * s2D2_sh, rdf.cuf:555-615): the frames are packed with z = 0 (any positive
+ * box[2]); the clip uses min(box[0], box[1]); distances are (x^2 + y^2) and the
+ * number-fluctuation points lie in the xy plane.  Bins as trj_rdf_plan_create
+ * (bin 0, r < deltar/2, is not counted, as in 3D). */
+TRJ_API int trj_rdf_plan_create_2d(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                                   int64_t n_max, trj_rdf_plan** out);
 /* Plan with nbins bins of width r_max/nbins covering [0, r_max): bin k (1-based)
  * holds r in [(k-1) dr, k dr), i.e. index floor(r/dr)+1, pairs counted for
  * rr2 < r_max^2 (FP32).  This is the binning of the freud RDF used by the

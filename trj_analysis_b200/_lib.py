@@ -53,6 +53,7 @@ SIGNATURES = {
     "trj_frame_pack_charges": (c_int, [vp, vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp, vp]),
     "trj_rdf_plan_create": (c_int, [vp, c_int, c_float, c_float, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_create_floor": (c_int, [vp, c_int, c_float, c_int, P(c_float), c_int64, P(vp)]),
+    "trj_rdf_plan_create_2d": (c_int, [vp, c_int, c_float, c_float, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_info": (c_int, [vp, P(c_int), P(c_int), P(c_int), P(c_float), P(c_float), P(c_int64)]),
     "trj_rdf_accumulate": (c_int, [vp, vp, c_int64, P(c_float), vp, vp, vp]),
     "trj_rdf_accumulate_charged": (c_int, [vp, vp, vp, c_int64, P(c_float), vp, vp, vp, vp]),

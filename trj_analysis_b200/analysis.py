@@ -37,6 +37,7 @@ from .refsem import F32
 class Config:
     """The /INPUT/, /INPUT_SP/, /INPUT_RDF/ and /INPUT_SQ/ keys this path uses (input.f90:64-75)."""
     nsp: int = 1
+    ndim: int = 3                  # 2: the z coordinate of the frames is discarded (netcdf.f90:649-651)
     sp_types_selected: Sequence[int] = (1,)
     run_rdf: bool = True
     run_sq: bool = True
@@ -121,6 +122,14 @@ class Session:
         keep = species >= 0
         xyz = frame.xyz if keep.all() else frame.xyz[keep]
         species = species if keep.all() else species[keep]
+        box = np.asarray(frame.box, np.float32)
+        if self.cfg.ndim == 2:
+            # two-dimensional frames: z discarded (netcdf.f90:649-651); packed with z = 0 in a unit z box
+            xyz = np.array(xyz, np.float32, copy=True)
+            xyz[:, 2] = 0.0
+            box = np.array([box[0], box[1], 1.0], np.float32)
+        elif self.cfg.ndim != 3:
+            raise ValueError(f"ndim={self.cfg.ndim}: 2 or 3")
         if self.ex_qc is None:
             self.ex_qc = frame.charges is not None
         if self.ex_qc != (frame.charges is not None):
@@ -138,8 +147,8 @@ class Session:
         if self.stage is None:
             n_max = self.n_max or xyz.shape[0]
             self.stage = engine.FrameStage(self.ctx, n_max, self.cfg.nsp, charged=self.device_charges)
-        self.box = np.asarray(frame.box, np.float32)
-        self.volumen = refsem.volume(self.box)
+        self.box = box
+        self.volumen = refsem.volume(self.box, self.cfg.ndim)
         self.ntype = np.bincount(species, minlength=self.cfg.nsp).astype(np.int64)
         self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream, charges=charges)
 
@@ -168,7 +177,7 @@ class Session:
     # ---- g(r) -----------------------------------------------------------------------
     def RDF_init(self) -> None:
         c = self.cfg
-        self.rdf = engine.RdfPlan(self.ctx, c.nsp, c.deltar, c.rcrdf, self.box, self.stage.n_max)
+        self.rdf = engine.RdfPlan(self.ctx, c.nsp, c.deltar, c.rcrdf, self.box, self.stage.n_max, ndim=c.ndim)
         self.hist = self.rdf.new_hist()
         self.edge = torch.zeros(4, dtype=torch.int64, device=self.ctx.torch_device)
         if self.device_charges:
@@ -186,7 +195,7 @@ class Session:
     # ---- S(Q) -----------------------------------------------------------------------
     def sq_init(self) -> None:
         c = self.cfg
-        self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell)
+        self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell, ndim=c.ndim)
         self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype, charged=self.device_charges)
         self.sq_out = self.sq.new_out()
 
@@ -216,7 +225,7 @@ class Session:
         if self.nconf_total is None:
             raise ValueError("run_sqw needs nconf_total (the trajectory's number of frames)")
         self.dyn = Dynamics(self.ctx, self.cfg.nsp, self.n, self.nconf_total, self.cfg.dyn or DynConfig(),
-                            self.box, self.bsc_sp)
+                            self.box, self.bsc_sp, ndim=self.cfg.ndim)
 
     def rtcorr(self, frame: Frame) -> None:
         if self.dyn is None:
@@ -271,7 +280,7 @@ class Session:
 
     def rdf_results(self) -> Dict[str, np.ndarray]:
         res = normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
-                            self.ntype, self.nconf, gqq=self.gqq_transfer())
+                            self.ntype, self.nconf, gqq=self.gqq_transfer(), ndim=self.cfg.ndim)
         if self.gi is not None:
             res["s2n"] = normalise_s2n(self.gi.cpu().numpy(), self.g2i.cpu().numpy(), self.nconf, self.cfg.nrandom,
                                        self.rdf.lsmax)
@@ -298,7 +307,7 @@ class Session:
     def suggested_rcl(self) -> float:
         """First minimum of the total g(r) after its first peak (rdf.cuf:313-352, 755-822)."""
         return first_minimum(self.rdf_transfer(), self.rdf.lsmax, self.cfg.deltar, self.volumen,
-                             int(self.ntype.sum()))
+                             int(self.ntype.sum()), ndim=self.cfg.ndim)
 
     def close(self) -> None:
         for obj in (self.sq, self.rdf, self.dyn):
@@ -306,18 +315,21 @@ class Session:
                 obj.close()
 
 
-def shell_volumes(lsmax: int, deltar: float) -> np.ndarray:
-    """4 pi/3 ((r+dr/2)^3 - (r-dr/2)^3) for r = i*dr, i = 1..lsmax (log.f90:475-478)."""
+def shell_volumes(lsmax: int, deltar: float, ndim: int = 3) -> np.ndarray:
+    """4 pi/3 ((r+dr/2)^3 - (r-dr/2)^3), in 2D pi ((r+dr/2)^2 - (r-dr/2)^2), for r = i*dr,
+    i = 1..lsmax (log.f90:475-487)."""
     dr = float(F32(deltar))
     ri = np.array([float(F32(F32(i) * F32(deltar))) for i in range(1, lsmax + 1)])
+    if ndim == 2:
+        return math.pi * ((ri + dr / 2) ** 2 - (ri - dr / 2) ** 2), ri
     return 4.0 * math.pi * ((ri + dr / 2) ** 3 - (ri - dr / 2) ** 3) / 3.0, ri
 
 
 def normalise_rdf(hist: np.ndarray, nsp: int, lsmax: int, deltar: float, volumen: float, ntype: np.ndarray,
-                  nconf: int, gqq: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+                  nconf: int, gqq: Optional[np.ndarray] = None, ndim: int = 3) -> Dict[str, np.ndarray]:
     """printrdf's g_jl(r_i) = (j/l+1) V H_jl(i) / (dV_i N_l N_j Nconf) for i = 1..lsmax-2 (FP64), and with
     charges g_qq(r_i) = 2 V gqq(i) / (N^2 dV_i Nconf) (log.f90:502-504)."""
-    dv, ri = shell_volumes(lsmax, deltar)
+    dv, ri = shell_volumes(lsmax, deltar, ndim)
     nrow = max(lsmax - 2, 0)
     g = np.zeros((nrow, nsp, nsp))
     h = hist.astype(np.float64)
@@ -345,8 +357,8 @@ def normalise_s2n(gi: np.ndarray, g2i: np.ndarray, nconf: int, nrandom: int, lsm
     return g2 / m - (g / m) ** 2
 
 
-def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, natms: int) -> float:
-    dv, _ = shell_volumes(lsmax, deltar)
+def first_minimum(hist: np.ndarray, lsmax: int, deltar: float, volumen: float, natms: int, ndim: int = 3) -> float:
+    dv, _ = shell_volumes(lsmax, deltar, ndim)
     g = np.zeros(lsmax + 1)
     g[1:] = 2.0 * volumen * hist.astype(np.float64).sum(axis=0) / (dv * natms * natms)
     nrdf = lsmax

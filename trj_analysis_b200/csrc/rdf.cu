@@ -458,7 +458,7 @@ __global__ void scan_exclusive_kernel(const int32_t* __restrict__ in, int32_t* _
 __global__ void s2n_kernel(const float4* __restrict__ sorted, const int32_t* __restrict__ cstart,
                            const int32_t* __restrict__ ccount, float Lx, float Ly, float Lz, int ncx, int ncy,
                            int ncz, float side2, float deltar, int lsmax, unsigned long long* __restrict__ gi,
-                           unsigned long long* __restrict__ g2i, float* __restrict__ points) {
+                           unsigned long long* __restrict__ g2i, float* __restrict__ points, int dim) {
     extern __shared__ unsigned long long cnt[];  // lsmax + 1
     __shared__ float pt[3];
     for (int k = threadIdx.x; k <= lsmax; k += blockDim.x) cnt[k] = 0ull;
@@ -467,7 +467,7 @@ __global__ void s2n_kernel(const float4* __restrict__ sorted, const int32_t* __r
         curand_init((unsigned long long)blockIdx.x + 1ull + 12345ull, 0ull, 0ull, &h);
         pt[0] = Lx * curand_uniform(&h);
         pt[1] = Ly * curand_uniform(&h);
-        pt[2] = Lz * curand_uniform(&h);
+        pt[2] = dim == 2 ? 0.f : Lz * curand_uniform(&h);  // s2D2_sh draws x and y only (rdf.cuf:580-581)
         if (points) {
             points[3 * blockIdx.x] = pt[0];
             points[3 * blockIdx.x + 1] = pt[1];
@@ -529,6 +529,7 @@ struct trj_rdf_plan {
     trj_ctx* ctx = nullptr;
     int nsp = 0, nit = 0, lsmax = 0;
     int floor_bins = 0;
+    int dim = 3;                // 2: frames in the xy plane (z = 0); z is neither clipped nor split
     float deltar = 0.f, rcrdf_eff = 0.f, side2 = 0.f;
     int64_t n_max = 0;
     int ncell_cap = 0;
@@ -553,8 +554,13 @@ static int nint_host(float x) {  // Fortran NINT: half away from zero
     return (int)(v >= 0 ? floor(v + 0.5) : -floor(-v + 0.5));
 }
 
-// Cells per axis for cutoff^2 side2 in box L; axes with < 3 cells are not split.
-static void cells_for(const float L[3], float side2, int nc[3]) {
+// Smallest box edge of the plan's geometry (the x and y edges in 2D).
+static float min_edge(const float box[3], int dim) {
+    return dim == 2 ? fminf(box[0], box[1]) : fminf(box[0], fminf(box[1], box[2]));
+}
+
+// Cells per axis for cutoff^2 side2 in box L; axes with < 3 cells are not split (nor z in 2D).
+static void cells_for(const float L[3], float side2, int nc[3], int dim = 3) {
     double rc = sqrt((double)side2) * (1.0 + 1.0 / 1024.0);
     for (int d = 0; d < 3; ++d) {
         int k = rc > 0 ? (int)floor((double)L[d] / rc) : 1;
@@ -562,10 +568,11 @@ static void cells_for(const float L[3], float side2, int nc[3]) {
         if (k > 1024) k = 1024;
         nc[d] = k;
     }
+    if (dim == 2) nc[2] = 1;
 }
 
-extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
-                                   int64_t n_max, trj_rdf_plan** out) {
+static int rdf_plan_create_impl(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                                int64_t n_max, int dim, trj_rdf_plan** out) {
     if (!ctx || !out || !box) return TRJ_ERR_INVALID;
     *out = nullptr;
     if (nsp < 1 || nsp > 16) return trj_fail(ctx, TRJ_ERR_INVALID, "rdf plan: nsp=%d (1..16)", nsp);
@@ -579,8 +586,9 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     p->nsp = nsp;
     p->nit = nsp * (nsp + 1) / 2;
     p->deltar = deltar;
-    // select_ncdfinput (netcdf.f90:610-617): side = minval(L); rcrdf = min(rcrdf, side/2)
-    float side = fminf(box[0], fminf(box[1], box[2]));
+    p->dim = dim;
+    // select_ncdfinput (netcdf.f90:610-617): side = minval(L(1:ndim)); rcrdf = min(rcrdf, side/2)
+    float side = min_edge(box, dim);
     float half = side / 2.0f;
     float rc = fminf(rcrdf, half);
     if (!(rc > 0.f)) rc = half;  // rcrdf <= 0 means half the box (netcdf.f90:613-617)
@@ -597,7 +605,7 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
                         "rdf plan: histogram of %zu bytes exceeds shared memory (%zu); increase deltar "
                         "or reduce rcrdf", hist_bytes, budget);
     }
-    cells_for(box, p->side2, p->nc);
+    cells_for(box, p->side2, p->nc, dim);
     int ncell = p->nc[0] * p->nc[1] * p->nc[2];
     // Room for a box up to 25% smaller per axis (more cells) without re-planning.
     p->ncell_cap = std::max(ncell * 2 + 64, 64);
@@ -620,6 +628,16 @@ extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rc
     p->scratch_bytes = (int64_t)bytes;
     *out = p;
     return TRJ_OK;
+}
+
+extern "C" int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                                   int64_t n_max, trj_rdf_plan** out) {
+    return rdf_plan_create_impl(ctx, nsp, deltar, rcrdf, box, n_max, 3, out);
+}
+
+extern "C" int trj_rdf_plan_create_2d(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
+                                      int64_t n_max, trj_rdf_plan** out) {
+    return rdf_plan_create_impl(ctx, nsp, deltar, rcrdf, box, n_max, 2, out);
 }
 
 extern "C" int trj_rdf_plan_create_floor(trj_ctx* ctx, int nsp, float r_max, int nbins, const float box[3],
@@ -713,7 +731,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
         return TRJ_OK;
     }
     // Per-frame clip, as select_ncdfinput does on every frame (netcdf.f90:610-617).
-    float side = fminf(box[0], fminf(box[1], box[2]));
+    float side = min_edge(box, plan->dim);
     plan->rcrdf_eff = fminf(plan->rcrdf_eff, side / 2.0f);
     plan->side2 = plan->rcrdf_eff * plan->rcrdf_eff;
 
@@ -734,7 +752,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     P.floor_bins = plan->floor_bins;
     P.nsp = plan->nsp;
     P.nit = plan->nit;
-    cells_for(box, plan->side2, P.nc);
+    cells_for(box, plan->side2, P.nc, plan->dim);
     P.ncell = P.nc[0] * P.nc[1] * P.nc[2];
     if (P.ncell > plan->ncell_cap)
         return trj_fail(ctx, TRJ_ERR_CAPACITY, "rdf accumulate: %d cells exceed plan capacity %d", P.ncell,
@@ -761,7 +779,8 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     P.noff = no;
     double avg = (double)n / P.ncell;
     P.hsplit = std::max(1, (int)ceil(avg / kHomeChunk));
-    P.fast_ok = P.nc[0] >= 5 && P.nc[1] >= 5 && P.nc[2] >= 5;
+    // No minimum image needed away from the wrap (2D: z differences are 0, z is never wrapped).
+    P.fast_ok = P.nc[0] >= 5 && P.nc[1] >= 5 && (P.nc[2] >= 5 || plan->dim == 2);
     // Split neighbour ranges when there are too few (cell, offset, home chunk) items to fill the GPU.
     int64_t base_items = (int64_t)P.ncell * P.noff * P.hsplit;
     int64_t want = (int64_t)ctx->sm_count * 4;
@@ -856,7 +875,7 @@ extern "C" int trj_rdf_s2n(trj_rdf_plan* plan, int nrandom, uint64_t* gi_dev, ui
     s2n_kernel<<<(unsigned)nrandom, 256, smem, (cudaStream_t)stream>>>(
         plan->sorted, plan->cstart, plan->ccount, plan->box_last[0], plan->box_last[1], plan->box_last[2],
         plan->nc[0], plan->nc[1], plan->nc[2], plan->side2, plan->deltar, plan->lsmax,
-        (unsigned long long*)gi_dev, (unsigned long long*)g2i_dev, points_dev);
+        (unsigned long long*)gi_dev, (unsigned long long*)g2i_dev, points_dev, plan->dim);
     ctx->launches += 1;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;

@@ -129,7 +129,8 @@ class OriginSchedule:
 class Dynamics:
     """Per-trajectory state of the F(Q,t)/Fs(Q,t)/MSD analysis on one device."""
 
-    def __init__(self, ctx, nsp: int, n: int, nconf: int, cfg: DynConfig, box, bsc, dq: Optional[float] = None):
+    def __init__(self, ctx, nsp: int, n: int, nconf: int, cfg: DynConfig, box, bsc, dq: Optional[float] = None,
+                 ndim: int = 3):
         from . import engine
         if cfg.nbuffer < 2:
             cfg = dataclasses.replace(cfg, nbuffer=2)  # input.f90:162-165
@@ -137,8 +138,8 @@ class Dynamics:
         self.sched = OriginSchedule(nconf, cfg)
         self.ndyn = self.sched.ndyn
         if dq is None:
-            dq = refsem.sq_init_params(box, max(cfg.qw), max(cfg.qw)).dq
-        self.sqw = refsem.sqw_kset(box, cfg.qw, dq)
+            dq = refsem.sq_init_params(box, max(cfg.qw), max(cfg.qw), ndim).dq
+        self.sqw = refsem.sqw_kset(box, cfg.qw, dq, ndim)
         self.n = int(n)
         self.plan = engine.DynPlan(ctx, nsp, n, cfg.nbuffer, self.ndyn, self.sqw, bsc)
         self.fkt, self.fskt, self.r2t = self.plan.new_totals()

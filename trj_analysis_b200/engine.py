@@ -87,10 +87,13 @@ class RdfPlan:
     ``floor_bins=nbins`` gives nbins bins [k dr, (k+1) dr) on [0, rcrdf) instead."""
 
     def __init__(self, ctx: Context, nsp: int, deltar: float, rcrdf: float, box, n_max: int,
-                 floor_bins: Optional[int] = None):
+                 floor_bins: Optional[int] = None, ndim: int = 3):
         self.ctx = ctx
         h = vp()
-        if floor_bins:
+        if ndim == 2:
+            rc = ctx.lib.trj_rdf_plan_create_2d(ctx.h, nsp, float(deltar), float(rcrdf), box3(box), int(n_max),
+                                                ctypes.byref(h))
+        elif floor_bins:
             rc = ctx.lib.trj_rdf_plan_create_floor(ctx.h, nsp, float(rcrdf), int(floor_bins), box3(box), int(n_max),
                                                    ctypes.byref(h))
         else:

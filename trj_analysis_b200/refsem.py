@@ -74,10 +74,10 @@ def fold(xyz: np.ndarray, box: np.ndarray) -> np.ndarray:
     return (xyz - (box * np.trunc(q)).astype(F32)).astype(F32)
 
 
-def volume(box) -> float:
-    """volumen = product of the box edges in FP32 (netcdf.f90:618-622)."""
+def volume(box, ndim: int = 3) -> float:
+    """volumen = product of the first ndim box edges in FP32 (netcdf.f90:618-622)."""
     v = F32(1.0)
-    for L in np.asarray(box, F32):
+    for L in np.asarray(box, F32)[:ndim]:
         v = F32(v * L)
     return float(v)
 
@@ -99,9 +99,9 @@ class RdfParams:
         return self.nsp * (self.nsp + 1) // 2
 
 
-def rdf_params(nsp: int, deltar: float, rcrdf: float, box) -> RdfParams:
+def rdf_params(nsp: int, deltar: float, rcrdf: float, box, ndim: int = 3) -> RdfParams:
     box = np.asarray(box, F32)
-    side = F32(box.min())
+    side = F32(box[:ndim].min())  # minval(sidel(1:ndim)) (netcdf.f90:610)
     half = F32(side / F32(2.0))
     rc = F32(min(F32(rcrdf), half))
     dr = F32(deltar)
@@ -157,14 +157,30 @@ class SqInit:
     qmin_eff: float
 
 
-def sq_init_params(box, qmax: float, qmin: float) -> SqInit:
+def sq_init_params(box, qmax: float, qmin: float, ndim: int = 3) -> SqInit:
     """dq, nqmax, lmax per axis (with the 4-alignment quirk), nqmin and the reduced qmin.
 
     qedge is read uninitialised at sq.cuf:165-166; the shipped example outputs are
     consistent with qedge = qmin (no reduction), which is what is used here.
+    ndim = 2 (sq.cuf:157-158, 185-192): dq and qmin from x and y only, lmax aligned to 16, lmaxz = 0.
     """
     box = np.asarray(box, F32)
     fk = np.array([F32(TWOPI32 / L) for L in box], dtype=F32)
+    if ndim == 2:
+        dq = F32(min(fk[0], fk[1]))
+        nqmax = nint(F32(F32(qmax) / dq))
+        lmax = [nint(F32(F32(qmin) / fk[d])) for d in range(2)]
+        for d in range(2):
+            if lmax[d] % 16 != 0:
+                lmax[d] = lmax[d] - 16 + lmax[d] % 16        # sq.cuf:186-187
+        nqmin = min(lmax)
+        qmin_eff = min(F32(fk[d] * F32(lmax[d])) for d in range(2))  # sq.cuf:191
+        lmax = lmax + [0]
+        if nqmin == 0:
+            nqmin = 1
+            lmax = [1, 1, 1]
+        return SqInit(fk=fk, dq=float(dq), nqmax=int(nqmax), lmax=tuple(int(l) for l in lmax),
+                      nqmin=int(nqmin), qmin_eff=float(qmin_eff))
     dq = F32(fk.min())
     nqmax = nint(F32(F32(qmax) / dq))
     lmax = [nint(F32(F32(qmin) / fk[d])) for d in range(3)]
@@ -181,13 +197,27 @@ def sq_init_params(box, qmax: float, qmin: float) -> SqInit:
                   nqmin=int(nqmin), qmin_eff=float(qmin_eff))
 
 
-def reference_nq(si: SqInit) -> np.ndarray:
-    """n(Q) denominators exactly as sq_init counts them (sq.cuf:303-342), FP32 geometry."""
+def reference_nq(si: SqInit, ndim: int = 3) -> np.ndarray:
+    """n(Q) denominators exactly as sq_init counts them (sq.cuf:303-342), FP32 geometry.
+    In 2D the loops run over 0..lmax inclusive (sq.cuf:313-325) and the default is 2."""
     nq = np.zeros(si.nqmax + 1, dtype=np.int64)
     if si.nqmin <= 1:
-        nq[1:] = 3
+        nq[1:] = 2 if ndim == 2 else 3
         return nq
     fk = si.fk
+    if ndim == 2:
+        i = np.arange(si.lmax[0] + 1, dtype=np.int64)[:, None]
+        j = np.arange(si.lmax[1] + 1, dtype=np.int64)[None, :]
+        a = (i.astype(F32) * fk[0]).astype(F32)
+        b = (j.astype(F32) * fk[1]).astype(F32)
+        rr = np.sqrt(((a * a).astype(F32) + (b * b).astype(F32)).astype(F32)).astype(F32)
+        mask = ((i + j) != 0) & (rr < F32(si.qmin_eff))
+        ind = nint((rr[mask] / F32(si.dq)).astype(F32))
+        indm = int(ind.max()) if ind.size else 0
+        ok = ind <= si.nqmax
+        np.add.at(nq, ind[ok], 1)
+        nq[indm + 1:] = 2
+        return nq
     lx, ly, lz = si.lmax
     i = np.arange(lx, dtype=np.int64)[:, None, None]
     j = np.arange(ly, dtype=np.int64)[None, :, None]
@@ -212,7 +242,7 @@ def _fma32(a, b, c):
     return (np.asarray(a, np.float64) * np.asarray(b, np.float64) + np.asarray(c, np.float64)).astype(F32)
 
 
-def reference_kset(box, qmax: float, qmin: float) -> KSet:
+def reference_kset(box, qmax: float, qmin: float, ndim: int = 3) -> KSet:
     """The vectors the reference's kernels sum, with their bins (reference mode).
 
     sqfnD (sq.cuf:523-591): every (kx,ky,kz) >= 0 of the launch grid with
@@ -221,11 +251,14 @@ def reference_kset(box, qmax: float, qmin: float) -> KSet:
     sqfact (sq.cuf:372-454): (k,0,0), (0,k,0), (0,0,k) for k from nqmin+1 (or 1) to nqmax,
     each binned at k.  Denominators: reference_nq.
     """
-    si = sq_init_params(box, qmax, qmin)
+    si = sq_init_params(box, qmax, qmin, ndim)
     vecs, bins = [], []
     if si.nqmin > 1:
         fk = si.fk
-        ext = [(l // 4 + 1) * 4 for l in si.lmax]  # launch grid (lmax/4+1) blocks of 4
+        if ndim == 2:  # launch grid (lmax/16+1) x 16 per axis, one z thread (sq.cuf:183-189)
+            ext = [(si.lmax[0] // 16 + 1) * 16, (si.lmax[1] // 16 + 1) * 16, 1]
+        else:
+            ext = [(l // 4 + 1) * 4 for l in si.lmax]  # launch grid (lmax/4+1) blocks of 4
         kx = np.arange(ext[0])[:, None, None]
         ky = np.arange(ext[1])[None, :, None]
         kz = np.arange(ext[2])[None, None, :]
@@ -248,7 +281,7 @@ def reference_kset(box, qmax: float, qmin: float) -> KSet:
     ks = np.arange(min_pts, si.nqmax + 1, dtype=np.int64)
     if ks.size:
         z = np.zeros_like(ks)
-        for ax in range(3):
+        for ax in range(ndim):  # sqfact2 in 2D: (k,0) and (0,k) (sq.cuf:456-521)
             cols = [z, z, z]
             cols[ax] = ks
             vecs.append(np.stack(cols, axis=1))
@@ -257,9 +290,10 @@ def reference_kset(box, qmax: float, qmin: float) -> KSet:
     V = np.concatenate(vecs).astype(np.int32) if vecs else np.zeros((0, 3), np.int32)
     B = np.concatenate(bins).astype(np.int32) if bins else np.zeros(0, np.int32)
     dense = np.zeros(V.shape[0], np.uint8)
-    dense[:nd] = 1
+    if ndim == 3:  # 2D vectors (nz = 0 only) fill one column of a tensor tile: direct sum only
+        dense[:nd] = 1
     return KSet(mode="ref", dq=si.dq, nqmax=si.nqmax, vectors=V, bins=B,
-                weights=np.ones(V.shape[0]), dense=dense, nq=reference_nq(si),
+                weights=np.ones(V.shape[0]), dense=dense, nq=reference_nq(si, ndim),
                 qmin_eff=si.qmin_eff, lmax=si.lmax, nqmin=si.nqmin)
 
 
@@ -389,10 +423,15 @@ def _shell_points(box, dq: float, b0: int, b1: int) -> dict:
 
 
 def make_kset(mode: str, box, qmax: float, qmin: Optional[float] = None, seed: int = 0,
-              per_shell: int = 200) -> KSet:
+              per_shell: int = 200, ndim: int = 3) -> KSet:
     """Named k-set modes: ``ref`` (reference octant + axes, reference n(Q)),
     ``full`` (every vector up to qmax), ``full+axes`` and ``full+sampled``
-    (complete shells below qmin, axis or random lattice vectors per shell above)."""
+    (complete shells below qmin, axis or random lattice vectors per shell above).
+    Two-dimensional frames (ndim = 2) take ``ref`` only."""
+    if ndim == 2:
+        if mode != "ref":
+            raise ValueError(f"k-set mode {mode!r}: two-dimensional frames support 'ref' only")
+        return reference_kset(box, qmax, qmax if qmin is None else qmin, ndim=2)
     if mode == "ref":
         return reference_kset(box, qmax, qmax if qmin is None else qmin)
     if mode == "full":
@@ -457,7 +496,7 @@ def _first_shell(q: np.ndarray, qw: np.ndarray, half: np.float32) -> np.ndarray:
     return out
 
 
-def sqw_kset(box, qw: Sequence[float], dq: float) -> SqwSet:
+def sqw_kset(box, qw: Sequence[float], dq: float, ndim: int = 3) -> SqwSet:
     """The S(Q, w) vector set: lattice vectors with 0 <= i <= nint(qmax/fk_x) (and likewise for j,
     k), not all zero, whose |k| lies inside a shell qw(l) +- dq/2.  nw counts them per shell with
     sq_init's FP32 |k| = sqrt((i fk_x)^2 + (j fk_y)^2 + (k fk_z)^2); the shell a vector is added to
@@ -472,6 +511,8 @@ def sqw_kset(box, qw: Sequence[float], dq: float) -> SqwSet:
     fk = np.array([F32(TWOPI32 / L) for L in box], dtype=F32)
     qmm = F32(qw32.max())
     lim = [nint(F32(qmm / fk[d])) for d in range(3)]
+    if ndim == 2:
+        lim[2] = 0  # kmaxz = 0 (sq.cuf:273-277)
     i, j, k = np.meshgrid(np.arange(lim[0] + 1), np.arange(lim[1] + 1), np.arange(lim[2] + 1), indexing="ij")
     i, j, k = i.ravel(), j.ravel(), k.ravel()
     keep = (i + j + k) != 0
