@@ -152,6 +152,9 @@ TRJ_API int trj_rdf_plan_create(trj_ctx* ctx, int nsp, float deltar, float rcrdf
  * (bin 0, r < deltar/2, is not counted, as in 3D). */
 TRJ_API int trj_rdf_plan_create_2d(trj_ctx* ctx, int nsp, float deltar, float rcrdf, const float box[3],
                                    int64_t n_max, trj_rdf_plan** out);
+/* Bin rule of the plan's counts: 0 = nint(r/deltar) (rdf_sh), 1 = int(r/deltar)+1
+ * (rdfxy, rdf.cuf:722, the slab g(r)); bins 1..lsmax either way. */
+TRJ_API int trj_rdf_plan_set_binning(trj_rdf_plan* plan, int floor_bins);
 /* Plan with nbins bins of width r_max/nbins covering [0, r_max): bin k (1-based)
  * holds r in [(k-1) dr, k dr), i.e. index floor(r/dr)+1, pairs counted for
  * rr2 < r_max^2 (FP32).  This is the binning of the freud RDF used by the
@@ -249,6 +252,16 @@ TRJ_API int trj_sq_plan_create_charged(trj_ctx* ctx, int nsp, int64_t nvec, cons
  * trj_frame_pack_charges.  A charged plan accepts only this call. */
 TRJ_API int trj_sq_accumulate_charged(trj_sq_plan* plan, const float* packed_dev, const float* charge_packed_dev,
                                       int64_t n, const float box[3], int method, double* out_dev, void* stream);
+/* Direct sums over caller-defined atom groups, for the plan's vectors:
+ * rho_g(k) = sum over atoms j in group g of exp(i k.r_j), FP64 [ngroups][nvec][2]
+ * in the caller's vector order.  packed_dev holds n atoms (x, y, z; w unused)
+ * with the groups contiguous: group g = atoms group_off_host[g] ..
+ * group_off_host[g+1]-1 (host array of ngroups+1 offsets, 0 .. n).  Groups may
+ * change from call to call; this is how the slab S(Q) (sqf3xy/sqf2xy,
+ * sq.cuf:594-771) forms the density of every species in every z slice.  FP32
+ * terms of exactly reduced phases, FP64 sums (the direct-sum path). */
+TRJ_API int trj_sq_rho_groups(trj_sq_plan* plan, const float* packed_dev, int64_t n, const float box[3],
+                              int ngroups, const int64_t* group_off_host, double* rho_out, void* stream);
 /* rho_a(k) of the last accumulate, FP64, [nsp][nvec][2] in the caller's vector order. */
 TRJ_API int trj_sq_rho(trj_sq_plan* plan, double* rho_dev, void* stream);
 /* Duration (ms) of the last main S(Q) kernel launch (tcgen05 contraction for

@@ -111,3 +111,37 @@ def test_shell_areas_2d():
     dv, ri = analysis.shell_volumes(6, 0.1, ndim=2)
     np.testing.assert_allclose(dv, np.pi * ((ri + 0.05) ** 2 - (ri - 0.05) ** 2), rtol=1e-7)
     assert refsem.volume([3.0, 4.0, 100.0], ndim=2) == 12.0
+
+
+@pytest.mark.parametrize("qmax,qmin", [(8.0, 4.0), (9.0, 3.5), (5.0, 0.4)])
+def test_slab_kset_matches_loops(qmax, qmin):
+    box = np.array([30.0, 26.0, 60.0], np.float32)
+    ks = refsem.slab_kset(box, qmax, qmin)
+    si = refsem.sq_init_params(box, qmax, qmin, ndim=2)
+    want = []
+    for kx in range((si.lmax[0] // 16 + 1) * 16):
+        for ky in range((si.lmax[1] // 16 + 1) * 16):
+            kf1, kf2 = F32(F32(kx) * si.fk[0]), F32(F32(ky) * si.fk[1])
+            q2 = F32(np.float64(kf2) * np.float64(kf2) + np.float64(F32(kf1 * kf1)))
+            if si.nqmin > 1 and 0 < q2 <= F32(F32(si.qmin_eff) * F32(si.qmin_eff)):
+                ind = refsem.nint(F32(F32(math.sqrt(float(q2))) / F32(si.dq)))  # sqf3xy: nint(q/dq)
+                if ind <= si.nqmax:
+                    want.append((kx, ky, 0, ind))
+    for k in range(max(1, si.nqmin + 1), si.nqmax + 1):
+        want.append((k, 0, 0, k))
+    for k in range(max(1, si.nqmin + 1), si.nqmax + 1):
+        want.append((0, k, 0, k))
+    got = [tuple(int(x) for x in v) + (int(b),) for v, b in zip(ks.vectors, ks.bins)]
+    assert got == want
+    np.testing.assert_array_equal(ks.nq, refsem.reference_nq(si, 2))
+
+
+def test_slab_of_matches_minloc():
+    rng = np.random.default_rng(1)
+    z = rng.uniform(-2, 12, size=500).astype(np.float32)
+    zs = [1.0, 4.0, 4.0, 8.5]
+    got = refsem.slab_of(z, zs, 1.5)
+    for k in range(z.shape[0]):
+        d = [abs(F32(F32(c) - z[k])) for c in zs]
+        m = int(np.argmin(d))  # first minimum
+        assert got[k] == (m if d[m] <= F32(F32(1.5) / F32(2.0)) else -1)

@@ -34,6 +34,16 @@ from .refsem import F32
 
 
 @dataclasses.dataclass
+class SlabConfig:
+    """/INPUT_CONF/ zslice, zgrid (input.f90:72): slice centres along z and their width.  With a slab
+    configuration and g(r) or S(Q) requested, the analysis is the reference's twoDstruc_3D one
+    (input.f90:171-191): per-slice g_xy(r) and S_xy(Q) in the xy plane.  z is taken as the trajectory
+    stores it (the confined direction is not folded)."""
+    zslice: Sequence[float] = (0.0,)
+    zgrid: float = 1.0
+
+
+@dataclasses.dataclass
 class Config:
     """The /INPUT/, /INPUT_SP/, /INPUT_RDF/ and /INPUT_SQ/ keys this path uses (input.f90:64-75)."""
     nsp: int = 1
@@ -56,6 +66,7 @@ class Config:
     # reference's ex_qc path); "species" requires every atom of a species to carry the same charge in
     # every frame and derives g_qq and S_qq from the species rows, with no extra device work.
     charge_mode: str = "atom"
+    slab: Optional[SlabConfig] = None
     # F(Q,t), Fs(Q,t), MSD over multiple time origins (rtcorr; needs the trajectory's frame count)
     run_sqw: bool = False
     dyn: Optional["DynConfig"] = None
@@ -94,6 +105,7 @@ class Session:
         self.ex_qc = None      # frames carry charges (set by the first frame, netcdf.f90:404-408)
         self.gqq = None        # FP64 [lsmax] charge-product histogram over avq2, summed over frames
         self.gi = self.g2i = None  # uint64 [lsmax+1] number-fluctuation sums (nrandom > 0)
+        self.slab = None           # per-slice accumulators (SlabState) in the twoDstruc_3D analysis
         self.charges = None    # charges of the last frame (FP32, selected atoms)
         self.species_q = None  # charge of each species (charge_mode "species")
 
@@ -205,6 +217,9 @@ class Session:
 
     # ---- frame loop (trj_analysis.f90:173-242) ---------------------------------------
     def add_frame(self, frame: Frame) -> None:
+        if self.cfg.slab is not None:
+            self._add_slab_frame(frame)
+            return
         self.select_ncdfinput(frame)
         if self.first:
             if self.cfg.run_rdf:
@@ -219,6 +234,42 @@ class Session:
         if self.cfg.run_sqw:
             self.rtcorr(frame)
         self.nconf += 1
+
+    # ---- slabs (twoDstruc_3D: rdfxy, sqf3xy/sqf2xy) -----------------------------------------
+    def _add_slab_frame(self, frame: Frame) -> None:
+        c = self.cfg
+        if c.ndim != 3:
+            raise ValueError("slab analysis needs three-dimensional frames (input.f90:172-175)")
+        if c.charge_mode != "atom" or frame.charges is not None:
+            raise ValueError("slab analysis with charges (gqqxy, sqfqxy) is not part of this build")
+        species = self._species_of(frame.types)
+        keep = species >= 0
+        xyz = np.asarray(frame.xyz if keep.all() else frame.xyz[keep], np.float32)
+        species = species if keep.all() else species[keep]
+        self.box = np.asarray(frame.box, np.float32)
+        self.volumen = refsem.volume(self.box)
+        self.ntype = np.bincount(species, minlength=c.nsp).astype(np.int64)
+        order = np.argsort(species, kind="stable")  # select_ncdfinput's species-contiguous order
+        sp = species[order].astype(np.int32)
+        z = xyz[order, 2]
+        xy = refsem.fold(xyz[order], self.box)
+        xy[:, 2] = 0.0
+        if self.slab is None:
+            self.slab = SlabState(self, xyz.shape[0])
+        self.slab.frame(xy, sp, z, self.box)
+        self.nconf += 1
+
+    def slab_results(self) -> Dict[str, np.ndarray]:
+        return self.slab.results(self.nconf)
+
+    def print_slabs(self, outdir: str = ".") -> List[str]:
+        res = self.slab_results()
+        files = []
+        if "g_xy" in res:
+            files += writers.write_gxy(outdir, res["r"], res["g_xy"], self.cfg.nsp, self.cfg.slab.zslice)
+        if "s_xy" in res:
+            files += writers.write_sqxy(outdir, res["q"], res["s_xy"], res["s_pxy"], self.cfg.slab.zslice)
+        return files
 
     # ---- F(Q,t), Fs(Q,t), MSD (dyn_init / rtcorr) -----------------------------------------
     def dyn_init(self) -> None:
@@ -310,7 +361,127 @@ class Session:
                              int(self.ntype.sum()), ndim=self.cfg.ndim)
 
     def close(self) -> None:
+        if self.slab is not None:
+            self.slab.close()
         for obj in (self.sq, self.rdf, self.dyn):
+            if obj is not None:
+                obj.close()
+
+
+class SlabState:
+    """Per-slice g_xy(r) and S_xy(Q) of the reference's twoDstruc_3D analysis.
+
+    g_xy (RDFcomp with rdfxy, rdf.cuf:218-232, 284-299, 672-738): pairs of atoms in the same slice,
+    xy minimum-image distance, bins int(r/deltar)+1; per frame the slice histogram of species pair
+    (k, j) is divided by countp(k, s) countp(j, s), the atoms of each species in the slice counted
+    over atoms 1..N-1 (rdfxy's home loop stops one short, so the last atom is never counted).  Each
+    slice runs as a two-dimensional pair plan over the slice's atoms with the 3D cutoff.
+    S_xy (SQcalc with sqf3xy/sqf2xy, sq.cuf:73-85, 594-771): per frame and vector, the density of every
+    species in every slice (trj_sq_rho_groups); S_pxy(bin, a, s) += |rho_as|^2 / countsp(s, a) and
+    S_xy(bin, s) += |sum_a bsc_a rho_as|^2 / count(s), counting every atom of the slice.
+    Normalisations of printrdf / printSQ (log.f90:337-376, 424-436, 516-523, 546-554)."""
+
+    def __init__(self, sess: "Session", n_max: int):
+        c = sess.cfg
+        self.sess = sess
+        self.nsp = c.nsp
+        self.zslice = np.asarray(c.slab.zslice, np.float32)
+        self.zgrid = np.float32(c.slab.zgrid)
+        self.nslice = int(self.zslice.size)
+        box = sess.box
+        self.stage = engine.FrameStage(sess.ctx, n_max, c.nsp)
+        self.rdf = None
+        if c.run_rdf:
+            p3 = refsem.rdf_params(c.nsp, c.deltar, c.rcrdf, box)  # the 3D clip of select_ncdfinput
+            box2 = np.array([box[0], box[1], 1.0], np.float32)
+            self.rdf = engine.RdfPlan(sess.ctx, c.nsp, c.deltar, p3.rcrdf, box2, n_max, ndim=2)
+            self.rdf.set_binning(True)
+            self.lsmax = self.rdf.lsmax
+            self.hist_xy = np.zeros((c.nsp, c.nsp, self.nslice, self.lsmax))
+            self.h_dev = self.rdf.new_hist()
+        self.sq = None
+        if c.run_sq:
+            self.kset = refsem.slab_kset(box, c.qmax, c.qmin)
+            self.sq = engine.SqPlan(sess.ctx, c.nsp, self.kset, np.array([n_max] + [0] * (c.nsp - 1)))
+            self.sqf_xy = np.zeros((self.kset.nbins, self.nslice))
+            self.sqf_pxy = np.zeros((self.kset.nbins, c.nsp, self.nslice))
+            self.bsc = np.asarray(sess.bsc_sp, np.float64)
+
+    def frame(self, xy: np.ndarray, sp: np.ndarray, z: np.ndarray, box) -> None:
+        sl = refsem.slab_of(z, self.zslice, self.zgrid)
+        nsp, ns = self.nsp, self.nslice
+        if self.rdf is not None:
+            counted = sl >= 0
+            counted[-1] = False  # rdfxy counts atoms 1..N-1
+            countp = np.zeros((nsp, ns), np.int64)
+            np.add.at(countp, (sp[counted], sl[counted]), 1)
+            box2 = np.array([box[0], box[1], 1.0], np.float32)
+            for s in range(ns):
+                sel = sl == s
+                m = int(sel.sum())
+                if m < 2:
+                    continue
+                self.h_dev.zero_()
+                n = self.stage.upload_and_pack(xy[sel], sp[sel], box2)
+                self.rdf.accumulate(self.stage.packed, n, box2, self.h_dev)
+                h = self.h_dev.cpu().numpy().astype(np.float64)
+                for a in range(nsp):
+                    for b in range(a, nsp):
+                        if countp[a, s] > 0 and countp[b, s] > 0:
+                            self.hist_xy[a, b, s] += h[refsem.pair_row(a, b, nsp)] / (countp[a, s] * countp[b, s])
+        if self.sq is not None:
+            inc = sl >= 0
+            grp = sp[inc].astype(np.int64) * ns + sl[inc]
+            order = np.argsort(grp, kind="stable")
+            cnt = np.bincount(grp, minlength=nsp * ns)
+            off = np.zeros(nsp * ns + 1, np.int64)
+            off[1:] = np.cumsum(cnt)
+            pos = np.zeros((int(inc.sum()), 4), np.float32)
+            pos[:, :2] = xy[inc][order, :2]
+            dev = torch.from_numpy(pos).to(self.sess.ctx.torch_device)
+            rho = self.sq.rho_groups(dev, pos.shape[0], box, off).cpu().numpy().reshape(nsp, ns, -1)
+            countsp = cnt.reshape(nsp, ns)
+            count = countsp.sum(axis=0)
+            bins = self.kset.bins
+            for s in range(ns):
+                for a in range(nsp):
+                    if countsp[a, s] > 0:
+                        np.add.at(self.sqf_pxy[:, a, s], bins, np.abs(rho[a, s]) ** 2 / countsp[a, s])
+                if count[s] > 0:
+                    tot = (self.bsc[:, None] * rho[:, s, :]).sum(axis=0)
+                    np.add.at(self.sqf_xy[:, s], bins, np.abs(tot) ** 2 / count[s])
+
+    def results(self, nconf: int) -> Dict[str, np.ndarray]:
+        out: Dict[str, np.ndarray] = {}
+        sess = self.sess
+        if self.rdf is not None:
+            dr = float(F32(sess.cfg.deltar))
+            nrow = max(self.lsmax - 2, 0)
+            ri = np.array([float(F32(F32(i) * F32(sess.cfg.deltar))) for i in range(1, nrow + 1)])
+            zg = float(self.zgrid)
+            dv = math.pi * ((ri + dr / 2) ** 2 - (ri - dr / 2) ** 2) * zg   # log.f90:478-480
+            fac = sess.volumen * (zg / float(sess.box[2]))
+            g = np.zeros((nrow, self.nsp, self.nsp, self.nslice))
+            for a in range(self.nsp):
+                for b in range(a, self.nsp):
+                    v = (2.0 if a == b else 1.0) * fac * self.hist_xy[a, b, :, :nrow].T / (dv[:, None] * nconf)
+                    g[:, a, b] = v
+                    g[:, b, a] = v
+            out["r"] = ri.astype(np.float32)
+            out["g_xy"] = g
+        if self.sq is not None:
+            nq = self.kset.nq.astype(np.float64)
+            sl = slice(1, self.kset.nqmax + 1)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                den = np.where(nq > 0, nq, np.nan)[:, None] * nconf
+                out["q"] = self.kset.q_column()
+                out["s_xy"] = (self.sqf_xy / den)[sl]
+                out["s_pxy"] = (self.sqf_pxy / den[:, :, None])[sl]
+            out["nq"] = self.kset.nq[sl]
+        return out
+
+    def close(self) -> None:
+        for obj in (self.rdf, self.sq):
             if obj is not None:
                 obj.close()
 

@@ -880,3 +880,9 @@ extern "C" int trj_rdf_s2n(trj_rdf_plan* plan, int nrandom, uint64_t* gi_dev, ui
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
 }
+
+extern "C" int trj_rdf_plan_set_binning(trj_rdf_plan* plan, int floor_bins) {
+    if (!plan) return TRJ_ERR_INVALID;
+    plan->floor_bins = floor_bins ? 1 : 0;
+    return TRJ_OK;
+}

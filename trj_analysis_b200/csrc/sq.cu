@@ -209,6 +209,7 @@ static void sq_plan_free(trj_sq_plan* p) {
                     p->tc_out_dev, p->rho_dev};
     for (void* q : ptrs) trj_dev_free(p->ctx, q);
     trj_sq_tc_release(p);
+    trj_dev_free(p->ctx, p->groups_buf);
     p->timer.release();
 }
 
@@ -510,6 +511,67 @@ extern "C" int trj_sq_accumulate_charged(trj_sq_plan* p, const float* packed_dev
     if (n > 0 && !charge_packed_dev)
         return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq accumulate (charged): null charge array");
     return sq_accumulate_impl(p, packed_dev, charge_packed_dev, n, box, method, out_dev, stream);
+}
+
+// Direct sums over caller-defined atom groups (any order of groups, counts that change per frame):
+// rho_g(k) = sum_{j in g} exp(i k.r_j) for the plan's vectors, groups contiguous in packed_dev.
+extern "C" int trj_sq_rho_groups(trj_sq_plan* p, const float* packed_dev, int64_t n, const float box[3], int ngroups,
+                                 const int64_t* group_off_host, double* rho_out, void* stream) {
+    if (!p) return TRJ_ERR_INVALID;
+    trj_ctx* ctx = p->ctx;
+    if (!box || !group_off_host || !rho_out || ngroups < 1 || ngroups > 4096)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq rho groups: bad arguments (ngroups=%d)", ngroups);
+    if (group_off_host[0] != 0 || group_off_host[ngroups] != n)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq rho groups: offsets must run from 0 to n=%lld", (long long)n);
+    for (int g = 0; g < ngroups; ++g)
+        if (group_off_host[g + 1] < group_off_host[g])
+            return trj_fail(ctx, TRJ_ERR_INVALID, "sq rho groups: offsets decrease at group %d", g);
+    if (n > 0 && (!packed_dev || ((uintptr_t)packed_dev) % 16))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq rho groups: packed_dev null or not 16-byte aligned");
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "sq rho groups: box edges must be positive");
+    if (p->nvec == 0) return TRJ_OK;
+    trj_device_guard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nsplit = plain_nsplit(ctx, p->nvec, std::max<int64_t>(n, 1));
+    const size_t phase_need = sizeof(uint4) * (size_t)std::max<int64_t>(n, 1);
+    const size_t part_need = sizeof(double2) * (size_t)nsplit * ngroups * p->nvec;
+    const size_t rho_need = sizeof(double2) * (size_t)ngroups * p->nvec;
+    const size_t off_need = sizeof(int64_t) * (size_t)(ngroups + 1);
+    const size_t need = phase_need + part_need + rho_need + off_need + 4 * 256;
+    if (need > p->groups_bytes) {
+        if (p->groups_buf) {
+            TRJ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+            trj_dev_free(ctx, p->groups_buf);
+            p->groups_buf = nullptr;
+            p->groups_bytes = 0;
+        }
+        if (trj_dev_alloc(ctx, &p->groups_buf, need) != cudaSuccess)
+            return trj_fail(ctx, TRJ_ERR_NOMEM, "sq rho groups: %zu bytes of scratch", need);
+        p->groups_bytes = need;
+    }
+    auto align = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    char* base = (char*)p->groups_buf;
+    uint4* phase = (uint4*)base;
+    double2* part = (double2*)(base + align(phase_need));
+    double2* rho = (double2*)(base + align(phase_need) + align(part_need));
+    int64_t* off = (int64_t*)(base + align(phase_need) + align(part_need) + align(rho_need));
+    // pageable source: staged before the call returns
+    TRJ_CUDA_TRY(ctx, cudaMemcpyAsync(off, group_off_host, off_need, cudaMemcpyHostToDevice, s));
+    if (n > 0)
+        phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
+                                                                       (double)box[1], (double)box[2], phase, nullptr);
+    dim3 grid((unsigned)((p->nvec + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT)), (unsigned)nsplit);
+    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(phase, off, ngroups, -1, p->vec_dev, p->plain_all_dev,
+                                                   (int)p->nvec, p->nvec, nsplit, part);
+    const int64_t tot = p->nvec * ngroups;
+    gather_plain_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, p->plain_all_dev, (int)p->nvec, p->nvec,
+                                                                      ngroups, nsplit, rho);
+    unpermute_rho_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rho, p->vec_dev, p->nvec, ngroups,
+                                                                       (double2*)rho_out);
+    ctx->launches += 4;
+    TRJ_CUDA_TRY(ctx, cudaGetLastError());
+    return TRJ_OK;
 }
 
 extern "C" int trj_sq_kernel_ms(trj_sq_plan* p, float* ms) {

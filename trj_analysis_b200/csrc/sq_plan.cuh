@@ -51,6 +51,8 @@ struct trj_sq_plan {
     int last_method = -1;
     int64_t scratch_bytes = 0;
     void* tc_state = nullptr;              // tensor-core kernel private state
+    void* groups_buf = nullptr;            // scratch of trj_sq_rho_groups (grown on demand)
+    size_t groups_bytes = 0;
     trj_kernel_timer timer;                // around the main kernel of the last accumulate
 };
 

@@ -141,6 +141,11 @@ class RdfPlan:
                                                      _ptr(hist), _ptr(edge), _ptr(gqq), _stream(stream))
         check(rc, self.ctx.h, "trj_rdf_accumulate_charged")
 
+    def set_binning(self, floor_bins: bool) -> None:
+        """Bins nint(r/deltar) (False) or int(r/deltar)+1 (True, the slab g(r))."""
+        check(self.ctx.lib.trj_rdf_plan_set_binning(self.h, 1 if floor_bins else 0), self.ctx.h,
+              "trj_rdf_plan_set_binning")
+
     def new_s2n(self):
         """(gi, g2i): uint64 [lsmax+1] sums of N_k and N_k^2 over sample points and frames."""
         dev = self.ctx.torch_device
@@ -224,6 +229,17 @@ class SqPlan:
         rc = self.ctx.lib.trj_sq_accumulate(self.h, _ptr(packed), int(n), box3(box), int(method), _ptr(out),
                                             _stream(stream))
         check(rc, self.ctx.h, "trj_sq_accumulate")
+
+    def rho_groups(self, packed: torch.Tensor, n: int, box, group_off: np.ndarray, stream=None) -> torch.Tensor:
+        """rho_g(k) over contiguous atom groups of ``packed`` (offsets ``group_off``, ngroups+1):
+        (ngroups, nvec) complex128 in the caller's vector order."""
+        off = np.ascontiguousarray(np.asarray(group_off, np.int64))
+        ng = off.shape[0] - 1
+        t = torch.empty((ng, self.kset.nvec, 2), dtype=torch.float64, device=self.ctx.torch_device)
+        rc = self.ctx.lib.trj_sq_rho_groups(self.h, _ptr(packed), int(n), box3(box), ng, off.ctypes.data_as(vp),
+                                            _ptr(t), _stream(stream))
+        check(rc, self.ctx.h, "trj_sq_rho_groups")
+        return torch.view_as_complex(t)
 
     def rho(self, stream=None) -> torch.Tensor:
         """rho_a(k) of the last accumulate, (ndens, nvec) complex128, caller vector order (charged plans:

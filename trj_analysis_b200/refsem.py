@@ -528,3 +528,54 @@ def sqw_kset(box, qw: Sequence[float], dq: float, ndim: int = 3) -> SqwSet:
     sel = (l_init >= 0) & (l_fqt >= 0)
     v = np.stack([i[sel], j[sel], k[sel]], axis=1).astype(np.int32)
     return SqwSet(qw=qw32, dq=float(dq32), vectors=v, bins=l_fqt[sel].astype(np.int32), nw=nw)
+
+
+def slab_kset(box, qmax: float, qmin: float) -> KSet:
+    """The vectors of the slab S(Q) (twoDstruc_3D; SQcalc, sq.cuf:73-85): sq_init's 2D geometry
+    (dq, lmax, nqmin, n(Q) as for ndim = 2).  sqf3xy (sq.cuf:594-674): every (kx, ky, 0) of the
+    launch grid with 0 < q2 <= qmin^2, q2 = kf1^2 + kf2^2 as the GPU contracts it, bin nint(q/dq)
+    (not sqfnD's int(q/dq + 0.501)); sqf2xy (676-771): (k, 0, 0) and (0, k, 0) for k from nqmin + 1
+    to nqmax, binned at k.  With nqmin <= 1 only sqf2xy runs, still from nqmin + 1 (sq.cuf:113-116): k = 1 is
+    skipped when nqmin = 1; the 16-alignment of lmax can make nqmin negative, and then k starts at 1."""
+    si = sq_init_params(box, qmax, qmin, 2)
+    vecs, bins = [], []
+    if si.nqmin > 1:
+        fk = si.fk
+        ext = [(si.lmax[0] // 16 + 1) * 16, (si.lmax[1] // 16 + 1) * 16]
+        kx = np.arange(ext[0])[:, None]
+        ky = np.arange(ext[1])[None, :]
+        kf1 = (kx.astype(F32) * fk[0]).astype(F32)
+        kf2 = (ky.astype(F32) * fk[1]).astype(F32)
+        q2 = _fma32(kf2, kf2, (kf1 * kf1).astype(F32))
+        qmin2 = F32(F32(si.qmin_eff) * F32(si.qmin_eff))
+        mask = (q2 > 0) & (q2.astype(np.float64) <= np.float64(qmin2))
+        idx = np.nonzero(mask)
+        q = np.sqrt(q2[idx].astype(np.float64)).astype(F32)
+        ind = nint((q / F32(si.dq)).astype(F32))
+        ind = np.atleast_1d(ind)
+        keep = ind <= si.nqmax
+        vecs.append(np.stack([idx[0][keep], idx[1][keep], np.zeros(int(keep.sum()), np.int64)], axis=1))
+        bins.append(ind[keep])
+    # sqf2xy's k starts at 1 (its thread index) or at minPts = nqmin + 1, whichever is larger
+    ks = np.arange(max(1, si.nqmin + 1), si.nqmax + 1, dtype=np.int64)
+    if ks.size:
+        z = np.zeros_like(ks)
+        vecs.append(np.stack([ks, z, z], axis=1))
+        vecs.append(np.stack([z, ks, z], axis=1))
+        bins += [ks, ks]
+    V = np.concatenate(vecs).astype(np.int32) if vecs else np.zeros((0, 3), np.int32)
+    B = np.concatenate(bins).astype(np.int32) if bins else np.zeros(0, np.int32)
+    return KSet(mode="slab", dq=si.dq, nqmax=si.nqmax, vectors=V, bins=B, weights=np.ones(V.shape[0]),
+                dense=np.zeros(V.shape[0], np.uint8), nq=reference_nq(si, 2), qmin_eff=si.qmin_eff,
+                lmax=si.lmax, nqmin=si.nqmin)
+
+
+def slab_of(z: np.ndarray, zslice: Sequence[float], zgrid: float) -> np.ndarray:
+    """Slice of each z (0-based), -1 outside: the first slice centre nearest to z (minloc of
+    |zslice - z|), kept if |zslice - z| <= zgrid/2, in FP32 (rdf.cuf:694-699, sq.cuf:633-635)."""
+    z = np.asarray(z, F32)
+    zs = np.asarray(zslice, F32)
+    d = np.abs((zs[None, :] - z[:, None]).astype(F32))
+    s = np.argmin(d, axis=1)  # first minimum, as minloc
+    ok = d[np.arange(z.shape[0]), s] <= F32(F32(zgrid) / F32(2.0))
+    return np.where(ok, s, -1).astype(np.int64)

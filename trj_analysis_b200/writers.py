@@ -220,3 +220,43 @@ def write_s2n(path_dir: str, r: np.ndarray, s2n: np.ndarray) -> str:
     with open(p, "w") as f:
         f.write("\n".join(lines) + "\n")
     return p
+
+
+def write_gxy(path_dir: str, r: np.ndarray, g: np.ndarray, nsp: int, zslice: Sequence[float]) -> List[str]:
+    """printrdf for slabs (log.f90:424-432, 546-554): gxy_<i>-<j>.dat for i <= j, header
+    '#     r        ',3x,16('g_xy(r,',f7.2,')',3x:), rows '(15f16.7)' r, g_xy(r, slice 1..nslice)."""
+    import os
+    files = []
+    labels = [f"g_xy(r,{fmt_f(z, 7, 2)})" for z in zslice]
+    for i in range(nsp):
+        for j in range(i, nsp):
+            lines = _group_header("#     r        " + " " * 3, labels, 16, " " * 3)
+            for k in range(r.shape[0]):
+                lines.extend(_records([r[k]] + list(g[k, i, j]), 15, 16, 7))
+            p = os.path.join(path_dir, f"gxy_{_i1(i + 1)}-{_i1(j + 1)}.dat")
+            with open(p, "w") as f:
+                f.write("\n".join(lines) + "\n")
+            files.append(p)
+    return files
+
+
+def write_sqxy(path_dir: str, q: np.ndarray, s_xy: np.ndarray, s_pxy: np.ndarray, zslice: Sequence[float]) -> List[str]:
+    """printSQ for slabs (log.f90:337-349, 364-376): sqxy.dat and sqpxy_<j>-<j>.dat, header
+    '#     Q        ',3x,16('S_xy(Q,',f7.2,')',3x:), rows '(15f16.7)' Q, S(Q, slice 1..nslice)."""
+    import os
+    labels = [f"S_xy(Q,{fmt_f(z, 7, 2)})" for z in zslice]
+    files = []
+
+    def emit(name, rows):
+        lines = _group_header("#     Q        " + " " * 3, labels, 16, " " * 3)
+        for k in range(q.shape[0]):
+            lines.extend(_records([q[k]] + list(rows[k]), 15, 16, 7))
+        p = os.path.join(path_dir, name)
+        with open(p, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        files.append(p)
+
+    emit("sqxy.dat", s_xy)
+    for j in range(s_pxy.shape[1]):
+        emit(f"sqpxy_{_i1(j + 1)}-{_i1(j + 1)}.dat", s_pxy[:, j, :])
+    return files
