@@ -110,6 +110,16 @@ TRJ_API int64_t trj_ctx_launches(const trj_ctx* ctx);
 TRJ_API int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev, int64_t n,
                    int nsp, const float box[3], float* packed_dev, int64_t* counts_dev,
                    void* stream);
+/* trj_frame_pack with the type-to-species numbering on the device: the species
+ * of atom i is lut_dev[types_dev[i]] (types 0 .. nlut-1; lut entries 0..nsp-1,
+ * or -1 for a type that is not selected).  A type outside the table or mapped
+ * to -1 is flagged as bad data (trj_ctx_check returns TRJ_ERR_DATA): frames
+ * whose atoms are all of selected types pass straight from the trajectory's
+ * type column to the device, with no per-atom host work.  Other arguments and
+ * results as trj_frame_pack. */
+TRJ_API int trj_frame_pack_types(trj_ctx* ctx, const float* xyz_dev, const int32_t* types_dev,
+                                 const int32_t* lut_dev, int nlut, int64_t n, int nsp, const float box[3],
+                                 float* packed_dev, int64_t* counts_dev, void* stream);
 /* trj_frame_pack for frames that carry per-atom charges (the NetCDF variable
  * "q", read as default real by src/core/netcdf.f90:404-408): the charges are
  * written in the same order as the atoms (netcdf.f90:656-658).

@@ -51,6 +51,7 @@ SIGNATURES = {
     "trj_frame_pack": (c_int, [vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp]),
     "trj_frame_pack_static": (c_int, [vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp]),
     "trj_frame_pack_charges": (c_int, [vp, vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp, vp]),
+    "trj_frame_pack_types": (c_int, [vp, vp, vp, vp, c_int, c_int64, c_int, P(c_float), vp, vp, vp]),
     "trj_rdf_plan_create": (c_int, [vp, c_int, c_float, c_float, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_create_floor": (c_int, [vp, c_int, c_float, c_int, P(c_float), c_int64, P(vp)]),
     "trj_rdf_plan_create_2d": (c_int, [vp, c_int, c_float, c_float, P(c_float), c_int64, P(vp)]),

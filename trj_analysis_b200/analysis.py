@@ -106,6 +106,8 @@ class Session:
         self.gqq = None        # FP64 [lsmax] charge-product histogram over avq2, summed over frames
         self.gi = self.g2i = None  # uint64 [lsmax+1] number-fluctuation sums (nrandom > 0)
         self.slab = None           # per-slice accumulators (SlabState) in the twoDstruc_3D analysis
+        self._lut_dev = None       # type -> species table on the device (frames with only selected types)
+        self._ntype_stale = False  # species counts of the last frame are on the device only
         self.charges = None    # charges of the last frame (FP32, selected atoms)
         self.species_q = None  # charge of each species (charge_mode "species")
 
@@ -128,8 +130,28 @@ class Session:
             raise ValueError("frame holds a type id outside the first frame's range")
         return self.species_lut[t]
 
+    def _fast_layout(self, frame: Frame) -> bool:
+        """Frames after the first whose atoms are all of selected types (as the first frame's were) go to
+        the device with their raw type column; the type-to-species table is applied there
+        (trj_frame_pack_types), and a type that is not selected is reported by the device as bad data."""
+        if self.first or self._lut_dev is None or self.cfg.ndim != 3 or frame.charges is not None or self.ex_qc:
+            return False
+        box = np.asarray(frame.box, np.float32)
+        self.box = box
+        self.volumen = refsem.volume(box)
+        self.n = self.stage.upload_and_pack_types(frame.xyz, frame.types, box, self._lut_dev, stream=self.stream)
+        self._ntype_stale = True
+        return True
+
+    def _refresh_ntype(self) -> None:
+        if self._ntype_stale:
+            self.ntype = self.stage.counts[:self.cfg.nsp].cpu().numpy().astype(np.int64)
+            self._ntype_stale = False
+
     def select_ncdfinput(self, frame: Frame) -> None:
         """Species numbering, host->device copy, fold and species-contiguous order."""
+        if self._fast_layout(frame):
+            return
         species = self._species_of(frame.types)
         keep = species >= 0
         xyz = frame.xyz if keep.all() else frame.xyz[keep]
@@ -162,7 +184,10 @@ class Session:
         self.box = box
         self.volumen = refsem.volume(self.box, self.cfg.ndim)
         self.ntype = np.bincount(species, minlength=self.cfg.nsp).astype(np.int64)
+        self._ntype_stale = False
         self.n = self.stage.upload_and_pack(xyz, species, self.box, stream=self.stream, charges=charges)
+        if self.first and keep.all() and self.cfg.ndim == 3 and not self.ex_qc and self.species_lut.size <= (1 << 20):
+            self._lut_dev = torch.from_numpy(self.species_lut.astype(np.int32)).to(self.ctx.torch_device)
 
     @property
     def device_charges(self) -> bool:
@@ -330,6 +355,7 @@ class Session:
         return float(F32(np.sum(q * q) / q.shape[0]))
 
     def rdf_results(self) -> Dict[str, np.ndarray]:
+        self._refresh_ntype()
         res = normalise_rdf(self.rdf_transfer(), self.cfg.nsp, self.rdf.lsmax, self.cfg.deltar, self.volumen,
                             self.ntype, self.nconf, gqq=self.gqq_transfer(), ndim=self.cfg.ndim)
         if self.gi is not None:
@@ -338,6 +364,7 @@ class Session:
         return res
 
     def sq_results(self) -> Dict[str, np.ndarray]:
+        self._refresh_ntype()
         if not self.ex_qc:
             return normalise_sq(self.sq_transfer_gpu_cpu(), self.kset, self.ntype, self.bsc_sp, self.nconf)
         return normalise_sq(self.sq_charged_sums(), self.kset, self.ntype, self.bsc_sp, self.nconf,
@@ -357,6 +384,7 @@ class Session:
 
     def suggested_rcl(self) -> float:
         """First minimum of the total g(r) after its first peak (rdf.cuf:313-352, 755-822)."""
+        self._refresh_ntype()
         return first_minimum(self.rdf_transfer(), self.rdf.lsmax, self.cfg.deltar, self.volumen,
                              int(self.ntype.sum()), ndim=self.cfg.ndim)
 

@@ -138,9 +138,17 @@ constexpr int kPackRounds = 4;
 constexpr int kPackChunk = kPackThreads * kPackRounds;  // atoms per block
 constexpr int kMaxSpecies = 16;
 
+// Species of atom i: sp[i], or lut[sp[i]] when a type-to-species table is given (-1: invalid).
+__device__ __forceinline__ int species_of(const int32_t* __restrict__ sp, int64_t i, const int32_t* __restrict__ lut,
+                                          int nlut) {
+    const int t = sp[i];
+    if (!lut) return t;
+    return (t >= 0 && t < nlut) ? lut[t] : -1;
+}
+
 __global__ void pack_count_kernel(const float* __restrict__ xyz, const int32_t* __restrict__ sp,
                                   int64_t n, int nsp, int32_t* __restrict__ block_counts,
-                                  unsigned* status) {
+                                  unsigned* status, const int32_t* __restrict__ lut, int nlut) {
     __shared__ int cnt[kMaxSpecies];
     if (threadIdx.x < kMaxSpecies) cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -149,7 +157,7 @@ __global__ void pack_count_kernel(const float* __restrict__ xyz, const int32_t* 
     for (int r = 0; r < kPackRounds; ++r) {
         int64_t i = base + r * kPackThreads + threadIdx.x;
         if (i < n) {
-            int s = sp[i];
+            int s = species_of(sp, i, lut, nlut);
             float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
             if (s < 0 || s >= nsp || !isfinite(x) || !isfinite(y) || !isfinite(z)) bad = true;
             if (s >= 0 && s < nsp) atomicAdd(&cnt[s], 1);
@@ -206,7 +214,7 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
                                     int64_t n, int nsp, float Lx, float Ly, float Lz,
                                     const int64_t* __restrict__ block_base,
                                     float4* __restrict__ packed, const float* __restrict__ q,
-                                    float* __restrict__ qpacked) {
+                                    float* __restrict__ qpacked, const int32_t* __restrict__ lut, int nlut) {
     __shared__ int64_t base[kMaxSpecies];
     __shared__ int warp_cnt[kPackThreads / 32][kMaxSpecies];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -220,7 +228,7 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
         int64_t i = start + r * kPackThreads + threadIdx.x;
         int s = -1;
         if (i < n) {
-            s = sp[i];
+            s = species_of(sp, i, lut, nlut);
             if (s < 0 || s >= nsp) s = -1;  // flagged by pack_count_kernel; dropped here
         }
         unsigned peers = __match_any_sync(0xffffffffu, s);
@@ -257,7 +265,8 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
 // Layout with context scratch; q/qpacked null for frames without charges.
 static int frame_pack_impl(trj_ctx* ctx, const char* name, const float* xyz_dev, const int32_t* species_dev,
                            const float* charge_dev, int64_t n, int nsp, const float box[3], float* packed_dev,
-                           float* charge_packed_dev, int64_t* counts_dev, void* stream) {
+                           float* charge_packed_dev, int64_t* counts_dev, void* stream,
+                           const int32_t* lut_dev = nullptr, int nlut = 0) {
     if (!ctx) return TRJ_ERR_INVALID;
     if (n < 0 || nsp < 1 || nsp > kMaxSpecies || !box)
         return trj_fail(ctx, TRJ_ERR_INVALID, "%s: n=%lld nsp=%d (1..%d)", name, (long long)n, nsp, kMaxSpecies);
@@ -294,11 +303,11 @@ static int frame_pack_impl(trj_ctx* ctx, const char* name, const float* xyz_dev,
     int64_t* block_base = (int64_t*)ps.ptr;
     int32_t* block_counts = (int32_t*)(block_base + nblocks * nsp);
     pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp,
-                                                                 block_counts, ctx->status_dev);
+                                                                 block_counts, ctx->status_dev, lut_dev, nlut);
     pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
     pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, box[0], box[1],
                                                                    box[2], block_base, (float4*)packed_dev,
-                                                                   charge_dev, charge_packed_dev);
+                                                                   charge_dev, charge_packed_dev, lut_dev, nlut);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
@@ -309,6 +318,15 @@ extern "C" int trj_frame_pack(trj_ctx* ctx, const float* xyz_dev, const int32_t*
                               int64_t* counts_dev, void* stream) {
     return frame_pack_impl(ctx, "trj_frame_pack", xyz_dev, species_dev, nullptr, n, nsp, box, packed_dev, nullptr,
                            counts_dev, stream);
+}
+
+extern "C" int trj_frame_pack_types(trj_ctx* ctx, const float* xyz_dev, const int32_t* types_dev,
+                                    const int32_t* lut_dev, int nlut, int64_t n, int nsp, const float box[3],
+                                    float* packed_dev, int64_t* counts_dev, void* stream) {
+    if (ctx && (!lut_dev || nlut < 1))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_frame_pack_types: null or empty type table");
+    return frame_pack_impl(ctx, "trj_frame_pack_types", xyz_dev, types_dev, nullptr, n, nsp, box, packed_dev, nullptr,
+                           counts_dev, stream, lut_dev, nlut);
 }
 
 extern "C" int trj_frame_pack_charges(trj_ctx* ctx, const float* xyz_dev, const int32_t* species_dev,
@@ -398,11 +416,11 @@ extern "C" int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const i
     int64_t* block_base = (int64_t*)scratch;
     int32_t* block_counts = (int32_t*)(block_base + nblocks * nsp);
     pack_count_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, block_counts,
-                                                                 ctx->status_dev);
+                                                                 ctx->status_dev, nullptr, 0);
     pack_scan_kernel<<<1, 1024, 0, s>>>(block_counts, nblocks, nsp, counts_dev, block_base);
     pack_scatter_kernel<<<(unsigned)nblocks, kPackThreads, 0, s>>>(xyz_dev, species_dev, n, nsp, box[0], box[1],
                                                                    box[2], block_base, (float4*)packed_dev, nullptr,
-                                                                   nullptr);
+                                                                   nullptr, nullptr, 0);
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;

@@ -344,6 +344,32 @@ class FrameStage:
         self.counts = torch.zeros((max(nsp, 1),), dtype=torch.int64, device=dev)
         self._copied = None  # event after the last host->device copy out of the pinned buffers
 
+    def upload_and_pack_types(self, xyz: np.ndarray, types: np.ndarray, box, lut: torch.Tensor, stream=None) -> int:
+        """Copies the raw coordinates and type ids and lays the frame out with the type-to-species
+        table ``lut`` (device int32) applied on the device (trj_frame_pack_types)."""
+        n = int(xyz.shape[0])
+        if n > self.n_max:
+            raise _lib.TrjError(_lib.TRJ_ERR_CAPACITY, f"frame of {n} atoms exceeds stage size {self.n_max}")
+        if self.charged:
+            raise ValueError("frame charges: use upload_and_pack")
+        if self._copied is not None:
+            self._copied.synchronize()  # pinned buffers may still feed the previous copy
+        self.h_xyz[:n].numpy()[:] = xyz
+        self.h_sp[:n].numpy()[:] = types
+        s = stream if stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self.d_xyz[:n].copy_(self.h_xyz[:n], non_blocking=True)
+            self.d_sp[:n].copy_(self.h_sp[:n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+            self._copied = ev
+        assert lut.dtype == torch.int32 and lut.is_cuda
+        rc = self.ctx.lib.trj_frame_pack_types(self.ctx.h, _ptr(self.d_xyz), _ptr(self.d_sp), _ptr(lut),
+                                               int(lut.numel()), n, self.nsp, box3(box), _ptr(self.packed),
+                                               _ptr(self.counts), _stream(s))
+        check(rc, self.ctx.h, "trj_frame_pack_types")
+        return n
+
     def upload_and_pack(self, xyz: np.ndarray, species: np.ndarray, box, stream=None,
                         charges: Optional[np.ndarray] = None) -> int:
         n = int(xyz.shape[0])
