@@ -5,7 +5,8 @@ Run in a checkout that has the reference project next to it:
     python tests/golden/make_golden.py /path/to/trj_analysis
 
 It reads ``examples/3D/<name>/{input.nml, sq.dat, sqmix.dat, gmixsim.dat}`` and
-writes ``tests/golden/examples.json``: per example, the /INPUT_RDF/ and
+writes ``tests/golden/examples.json`` (and, from the dynamics outputs of two examples,
+``tests/golden/dynamics.json``): per example, the /INPUT_RDF/ and
 /INPUT_SQ/ parameters, nsp, the header lines, the Q column (as printed), the
 n(Q) column, and the r column / row count of gmixsim.dat.  The g and S values
 themselves are not kept: the trajectories that produced them are not shipped,
@@ -61,6 +62,50 @@ def main(ref_root: str) -> None:
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "examples.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
+    print("wrote", path)
+    dynamics(ref_root)
+
+
+def _table(path):
+    lines = open(path).read().splitlines()
+    return lines[0], [r.split() for r in lines[1:] if r.strip()]
+
+
+def dynamics(ref_root: str) -> None:
+    """Known answers of the time-correlation outputs: for examples/3D/salr (F(Q,t), Fs(Q,t) and their
+    transforms) and examples/3D/meam-dyn (row count of dyn.dat), the /INPUT/ frame range and
+    /INPUT_DYN/, /INPUT_SQW/ keys, the header lines, and the printed columns.  fkt.dat and fskt.dat
+    are the inputs of the transform that wrote sqw.dat, so the transform can be checked against them;
+    C_r(t) and C_v(t) depend on the unshipped trajectory and are not kept."""
+    out = {}
+    for name in ["salr", "meam-dyn"]:
+        d = os.path.join(ref_root, "examples", "3D", name)
+        nml = open(os.path.join(d, "input.nml")).read()
+        frm = [int(x) for x in _nml_value(nml, "INPUT", "ncfs_from_to").split()]
+
+        def num(group, key, default):
+            v = _nml_value(nml, group, key)
+            return float(v.split("!")[0]) if v is not None else default
+        ex = {"ncfs_from_to": frm, "nbuffer": int(num("INPUT_DYN", "nbuffer", 2)),
+              "jump": int(num("INPUT_DYN", "jump", 1)), "tlimit": num("INPUT_DYN", "tlimit", -1.0),
+              "tmax": num("INPUT_DYN", "tmax", -1.0)}
+        head, rows = _table(os.path.join(d, "dyn.dat"))
+        ex["dyn_header"] = head
+        ex["dyn_rows"] = len(rows)
+        ex["dyn_t"] = [r[0] for r in rows]
+        if os.path.exists(os.path.join(d, "fkt.dat")):
+            ex["qw"] = [float(x) for x in _nml_value(nml, "INPUT_SQW", "qw").split("!")[0].split()]
+            for key in ("fkt", "fskt"):
+                head, rows = _table(os.path.join(d, key + ".dat"))
+                ex[key + "_header"] = head
+                ex[key] = [r[1:] for r in rows]
+            head, rows = _table(os.path.join(d, "sqw.dat"))
+            ex["sqw_header"] = head
+            ex["sqw"] = rows
+        out[name] = ex
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "dynamics.json")
+    with open(path, "w") as f:
+        json.dump(out, f)
     print("wrote", path)
 
 

@@ -174,3 +174,64 @@ def test_dynamics_files(tmp_path):
     assert open(files[0]).read().startswith("#  t(ps)         C_r(t)")
     assert open(files[3]).read().startswith("#  w(THz)       w(meV)     S(0.5000,w)")
     assert writers.fmt_f(10.0, 6, 4) == "******"  # f6.4 overflow, as Fortran prints it
+
+
+# ---- known answers from the reference's shipped dynamics outputs (tests/golden/dynamics.json) ----
+
+import json
+import os
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "dynamics.json")))
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_golden_row_counts(name):
+    """dyn.dat / fkt.dat hold itlimit rows: Nconf - (nbuffer-1)*jump with the default tlimit."""
+    g = GOLDEN[name]
+    nconf = g["ncfs_from_to"][0]
+    cfg = dynamics.DynConfig(nbuffer=g["nbuffer"], jump=g["jump"], tlimit=g["tlimit"], tmax=g["tmax"], qw=(1.0,))
+    sc = dynamics.OriginSchedule(nconf, cfg)
+    sc.schedule(1, 0.0)
+    sc.schedule(2, 0.005)
+    assert sc.itlimit == g["dyn_rows"]
+    if "fkt" in g:
+        assert len(g["fkt"]) == len(g["fskt"]) == len(g["sqw"]) == g["dyn_rows"] == sc.ndyn
+
+
+def test_golden_headers_and_time_column(tmp_path):
+    g = GOLDEN["salr"]
+    nd = g["dyn_rows"]
+    t = (np.arange(nd).astype(F32) * F32(0.005)).astype(F32)
+    res = {"t": t, "r2t": np.zeros(nd), "fkt": np.zeros((nd, 1)), "fskt": np.zeros((nd, 1)),
+           "sqw": np.zeros((nd, 1), F32), "ssqw": np.zeros((nd, 1), F32), "w": np.zeros(nd, F32),
+           "itlimit": nd, "qw": np.asarray(g["qw"], F32), "count_org": 1}
+    files = writers.write_dynamics(str(tmp_path), res, units="real")
+    got = [open(f).read().splitlines() for f in files]
+    assert g["dyn_header"].startswith(got[0][0])  # the reference adds C_v(t) when the trajectory has velocities
+    assert got[1][0] == g["fkt_header"]
+    assert got[2][0] == g["fskt_header"]
+    assert got[3][0] == g["sqw_header"]
+    assert [ln[:10].strip() for ln in got[1][1:]] == g["dyn_t"]
+
+
+@pytest.mark.parametrize("col,key", [(2, "fkt"), (3, "fskt")])
+def test_golden_transform(col, key):
+    """sqw.dat is fftw1d of fkt.dat / fskt.dat (print_rtcor, dynamics.cuf:306-313) with tmax = 2.0 from
+    /INPUT_DYN/ and dt = t(2) - t(1).  The frame times are FP32 products nstep*tstep; their difference,
+    printed as 0.005, is an FP32 difference of two times between 8 and 16 ps, i.e. a multiple of 2^-20:
+    5243 * 2^-20 = 0.0050001144 (5242 or 5244 * 2^-20 miss by 1e-2).  With it the restated transform of
+    the printed F(t) reproduces the printed S(w) to the rounding of the five printed decimals."""
+    g = GOLDEN["salr"]
+    f = np.array([float(r[0]) for r in g[key]], np.float32)
+    dt = F32(5243 * 2.0 ** -20)
+    s, w, _ = dynamics.fftw1d(f, dt, F32(g["tmax"]))
+    want = np.array([float(r[col]) for r in g["sqw"]])
+    err = np.max(np.abs(s.astype(np.float64) - want))
+    assert err <= 1e-5, err
+    s2, _, _ = dynamics.fftw1d(f, dt, F32(g["tmax"] - 0.01))  # the window position matters at this level
+    assert np.max(np.abs(s2.astype(np.float64) - want)) > 100 * err
+    twopi = F32(F32(2) * F32(3.141592653589793))
+    thz = [writers.fmt_f(F32(x / twopi), 10, 3).strip() for x in w]
+    mev = [writers.fmt_f(F32(F32(F32(4.135) * x) / twopi), 10, 3).strip() for x in w]
+    assert thz == [r[0] for r in g["sqw"]]
+    assert mev == [r[1] for r in g["sqw"]]
