@@ -36,13 +36,14 @@ def _nml_value(text: str, group: str, key: str):
 
 def main(ref_root: str) -> None:
     out = {}
-    for name in EXAMPLES:
-        d = os.path.join(ref_root, "examples", "3D", name)
+    for name in EXAMPLES + ["2D/salr"]:
+        d = os.path.join(ref_root, "examples", name if "/" in name else os.path.join("3D", name))
         nml = open(os.path.join(d, "input.nml")).read()
         ex = {
+            "ndim": int(_nml_value(nml, "INPUT", "ndim")),
             "nsp": int(_nml_value(nml, "INPUT", "nsp")),
             "deltar": float(_nml_value(nml, "INPUT_RDF", "deltar")),
-            "rcrdf": float(_nml_value(nml, "INPUT_RDF", "rcrdf")),
+            "rcrdf": float(_nml_value(nml, "INPUT_RDF", "rcrdf").split("!")[0]),
             "qmax": float(_nml_value(nml, "INPUT_SQ", "qmax")),
             "qmin": float(_nml_value(nml, "INPUT_SQ", "qmin")),
         }

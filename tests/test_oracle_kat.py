@@ -95,3 +95,21 @@ def test_meam_dyn_needs_fp32_geometry():
     L = recover_box(ex["sq_q"])
     ks = refsem.reference_kset([L, L, L], ex["qmax"], ex["qmin"])
     assert 2928 in list(ks.nq)
+
+
+def test_two_dimensional_example_columns():
+    """examples/2D/salr (ndim = 2): sq_init's 2D n(Q) (x and y only, lmax aligned to 16, loops over
+    0..lmax inclusive) reproduces every printed n(Q); the box is square, recovered from the Q column.
+    Like salr's 3D file, this sq.dat comes from an older writer: past the fully sampled region
+    (rows 1..nqmin+1 = 149) it printed every third Q of the axis region, all with n(Q) = 2."""
+    ex = GOLD["2D/salr"]
+    assert ex["ndim"] == 2
+    L = recover_box(ex["sq_q"], 50)
+    ks = refsem.reference_kset([L, L, F32(1.0)], ex["qmax"], ex["qmin"], ndim=2)
+    gold = np.array(ex["sq_nq"])
+    assert np.array_equal(ks.nq[1:1 + gold.size], gold)
+    assert ks.nqmin + 1 == 149
+    assert [f"{v:.7f}" for v in ks.q_column()[:149]] == ex["sq_q"][:149]
+    p = refsem.rdf_params(ex["nsp"], ex["deltar"], ex["rcrdf"], [L, L, F32(1.0)], ndim=2)
+    assert p.lsmax - 2 == len(ex["gmix_r"])
+    assert [f"{F32(F32(i) * F32(ex['deltar'])):.5f}" for i in range(1, p.lsmax - 1)] == ex["gmix_r"]
