@@ -59,6 +59,12 @@ def main(ref_root: str) -> None:
             g = open(gpath).read().splitlines()
             ex["gmix_header"] = g[0]
             ex["gmix_r"] = [r.split()[0] for r in g[1:] if r.strip()]
+        g1path = os.path.join(d, "gmixsim1.dat")  # nsp > 6: one file per species
+        if os.path.exists(g1path):
+            g = open(g1path).read().splitlines()
+            ex["gmix1_header"] = g[0]
+            ex["gmix1_r"] = [r.split()[0] for r in g[1:] if r.strip()]
+            ex["gmix1_ncols"] = len(g[1].split())
         out[name] = ex
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "examples.json")
     with open(path, "w") as f:

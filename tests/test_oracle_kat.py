@@ -113,3 +113,21 @@ def test_two_dimensional_example_columns():
     p = refsem.rdf_params(ex["nsp"], ex["deltar"], ex["rcrdf"], [L, L, F32(1.0)], ndim=2)
     assert p.lsmax - 2 == len(ex["gmix_r"])
     assert [f"{F32(F32(i) * F32(ex['deltar'])):.5f}" for i in range(1, p.lsmax - 1)] == ex["gmix_r"]
+
+
+@pytest.mark.parametrize("name,charged", [("Conf", False), ("RTIL+H20_rigid", True)])
+def test_seven_species_files_and_charge_columns(name, charged, tmp_path):
+    """nsp = 7 writes one gmixsim<k>.dat per species; with charges (RTIL+H20_rigid) the first file has
+    g_qq(r) after r and sq.dat has S_qq(Q) after S_NN(Q) (log.f90:353-362, 456-458, 565-567)."""
+    from trj_analysis_b200 import writers
+    ex = GOLD[name]
+    nrow = len(ex["gmix1_r"])
+    r = np.array([F32(F32(i) * F32(ex["deltar"])) for i in range(1, nrow + 1)], np.float32)
+    g = np.zeros((nrow, 7, 7))
+    files = writers.write_gmixsim(str(tmp_path), r, g, 7, g_qq=np.zeros(nrow) if charged else None)
+    lines = open(files[0]).read().splitlines()
+    assert lines[0] == ex["gmix1_header"]
+    assert len(lines[1].split()) == ex["gmix1_ncols"]
+    assert [ln.split()[0] for ln in lines[1:]] == ex["gmix1_r"]
+    head = writers.SQ_HEADER_QQ if charged else writers.SQ_HEADER
+    assert head == ex["sq_header"]
