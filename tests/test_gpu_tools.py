@@ -79,7 +79,7 @@ def test_trj_analysis_reference_outputs(traj, monkeypatch):
     from trj_analysis_b200.tools import trj_analysis as tool
     d, path, frs = traj
     nml = d / "input.nml"
-    nml.write_text("&INPUT\n trj_input_file='run.nc'\n nsp=2\n ncfs_from_to=2 1 1\n"
+    nml.write_text("&INPUT\n trj_input_file='run.nc'\n nsp=2\n ncfs_from_to=2 1 2\n"
                    " rdf_sq_cl_dyn_sqw_conf_ord=T T F F F F F\n/\n&INPUT_SP\n sp_types_selected=1 2\n/\n"
                    "&INPUT_RDF\n deltar=0.05\n rcrdf=5.0\n/\n&INPUT_SQ\n qmax=4.0\n qmin=2.0\n/\n")
     monkeypatch.chdir(d)
@@ -105,3 +105,36 @@ def test_trj_analysis_reference_outputs(traj, monkeypatch):
     ref = normalise_rdf(H.astype(np.uint64), 2, p.lsmax, 0.05, refsem.volume(frs[0].box), nt, 2)
     got = np.array([[float(x) for x in r.split()] for r in g[1:]])
     assert np.allclose(got[:, 1], ref["g"][:, 0, 0], atol=6e-6)
+
+
+def test_trj_analysis_dynamics_charges_s2n(tmp_path, monkeypatch):
+    """The namelist driver with time correlations (/INPUT_DYN/, /INPUT_SQW/), number fluctuations
+    (nrandom) and a trajectory that carries charges and times: every output file of the reference."""
+    from trj_analysis_b200.tools import trj_analysis as tool
+    spec = frames.FCCSpec(cells=(5, 5, 5), sigma=0.1, fractions=(0.5, 0.5), seed=44, charges=(1.0, -1.0))
+    frs = []
+    for f in frames.random_walk_frames(spec, 12, 0.1):
+        f.time = f.time + 1.0  # no step 0 (the reference skips it)
+        frs.append(f)
+    frames.write_netcdf_trajectory(str(tmp_path / "run.nc"), frs)
+    nml = tmp_path / "input.nml"
+    nml.write_text("&INPUT\n trj_input_file='run.nc'\n nsp=2\n ncfs_from_to=12 1 12\n"
+                   " rdf_sq_cl_dyn_sqw_conf_ord=T T F T T F F\n/\n&INPUT_SP\n sp_types_selected=1 2\n/\n"
+                   "&INPUT_RDF\n deltar=0.05\n rcrdf=3.0\n nrandom=8\n/\n&INPUT_SQ\n qmax=4.0\n qmin=2.0\n/\n"
+                   "&INPUT_DYN\n nbuffer=2\n tmax=3.0\n/\n&INPUT_SQW\n qw=1.5 3.0\n/\n")
+    monkeypatch.chdir(tmp_path)
+    assert tool.main([str(nml), "0"]) == 0
+    g = open(tmp_path / "gmixsim.dat").read().splitlines()
+    assert "g_qq(r)" in g[0]
+    assert open(tmp_path / "sq.dat").readline().startswith("#           Q        S_NN(Q)          S_qq(Q)")
+    assert open(tmp_path / "s2n.dat").readline().strip().endswith("s2n")
+    fkt = open(tmp_path / "fkt.dat").read().splitlines()
+    assert fkt[0] == "#  t(ps)         F(1.5000,t)    F(3.0000,t)"
+    assert len(fkt) - 1 == 11  # itlimit = Nconf - (nbuffer-1)*jump
+    row = [float(x) for x in fkt[1].split()]
+    assert row[0] == 0.0 and all(np.isfinite(row))
+    fs = [float(x) for x in open(tmp_path / "fskt.dat").read().splitlines()[1].split()]
+    assert abs(fs[1] - 1.0) < 1e-5 and abs(fs[2] - 1.0) < 1e-5  # Fs(Q, 0) = 1
+    dyn = open(tmp_path / "dyn.dat").read().splitlines()
+    assert dyn[0] == "#  t(ps)         C_r(t)" and float(dyn[1].split()[1]) == 0.0 and float(dyn[3].split()[1]) > 0
+    assert len(open(tmp_path / "sqw.dat").read().splitlines()) == 1 + 11

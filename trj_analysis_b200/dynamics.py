@@ -137,9 +137,13 @@ class Dynamics:
         self.cfg = cfg
         self.sched = OriginSchedule(nconf, cfg)
         self.ndyn = self.sched.ndyn
-        if dq is None:
-            dq = refsem.sq_init_params(box, max(cfg.qw), max(cfg.qw), ndim).dq
-        self.sqw = refsem.sqw_kset(box, cfg.qw, dq, ndim)
+        if len(cfg.qw) == 0:  # C_r(t) only (run_dyn without run_sqw)
+            self.sqw = refsem.SqwSet(qw=np.zeros(0, np.float32), dq=0.0, vectors=np.zeros((0, 3), np.int32),
+                                     bins=np.zeros(0, np.int32), nw=np.zeros(0, np.int64))
+        else:
+            if dq is None:
+                dq = refsem.sq_init_params(box, max(cfg.qw), max(cfg.qw), ndim).dq
+            self.sqw = refsem.sqw_kset(box, cfg.qw, dq, ndim)
         self.n = int(n)
         self.plan = engine.DynPlan(ctx, nsp, n, cfg.nbuffer, self.ndyn, self.sqw, bsc)
         self.fkt, self.fskt, self.r2t = self.plan.new_totals()
@@ -155,12 +159,13 @@ class Dynamics:
         """print_rtcor's arrays (dynamics.cuf:278-315): t from 0, C_r = r2t/count_org,
         F = fkt/(N count_org nw), Fs likewise, and their transforms."""
         sc = self.sched
+        nq_ = self.sqw.qw.size
         t = (sc.t - sc.t[0]).astype(F32)
         with np.errstate(divide="ignore", invalid="ignore"):
             r2t = self.r2t.cpu().numpy() / sc.count_org
             den = self.n * sc.count_org * self.sqw.nw.astype(np.float64)
-            fkt = self.fkt.cpu().numpy() / den[None, :]
-            fskt = self.fskt.cpu().numpy() / den[None, :]
+            fkt = self.fkt.cpu().numpy()[:, :nq_] / den[None, :]
+            fskt = self.fskt.cpu().numpy()[:, :nq_] / den[None, :]
         dt = F32(t[1] - t[0]) if t.shape[0] > 1 else F32(1)
         nq = self.sqw.qw.size
         sqw = np.zeros((self.ndyn, nq), F32)

@@ -266,7 +266,7 @@ class DynPlan:
     def __init__(self, ctx: Context, nsp: int, n: int, nbuffer: int, ndyn: int, sqw, bsc):
         self.ctx = ctx
         self.nsp, self.n, self.nbuffer, self.ndyn = nsp, int(n), int(nbuffer), int(ndyn)
-        self.nbins = int(sqw.qw.size)
+        self.nbins = max(1, int(sqw.qw.size))  # one unused bin when only C_r(t) is wanted
         self._vec = np.ascontiguousarray(sqw.vectors.astype(np.int32))
         self._bin = np.ascontiguousarray(sqw.bins.astype(np.int32))
         self._bsc = np.ascontiguousarray(np.asarray(bsc, np.float32))

@@ -168,7 +168,10 @@ def _frame_charges(var, f: int) -> Optional[np.ndarray]:
 
 class NpzTrajectory:
     """Frames stored as ``coordinates`` (F, N, 3), ``cell_lengths`` (F, 3), ``type`` (F, N) or (N,),
-    and optionally ``q`` (F, N) or (N,) charges."""
+    and optionally ``q`` (F, N) or (N,) charges and ``time`` (F,)."""
+
+    time_units = "lj"
+    time_scale = 1.0
 
     def __init__(self, path: str):
         self._z = np.load(path)
@@ -176,20 +179,25 @@ class NpzTrajectory:
     def __len__(self) -> int:
         return int(self._z["coordinates"].shape[0])
 
+    def frame(self, f: int) -> Frame:
+        """Frame f (0-based)."""
+        z = self._z
+        types = z["type"] if "type" in z else None
+        t = np.ones(z["coordinates"].shape[1], np.int32) if types is None else (
+            types[f] if types.ndim == 2 else types)
+        return Frame(xyz=np.asarray(z["coordinates"][f], np.float32), types=np.asarray(t, np.int32),
+                     box=np.asarray(z["cell_lengths"][f], np.float32),
+                     charges=_frame_charges(z["q"] if "q" in z else None, f),
+                     time=float(z["time"][f]) if "time" in z else None)
+
     def __iter__(self) -> Iterator[Frame]:
-        coords = self._z["coordinates"]
-        cells = self._z["cell_lengths"]
-        types = self._z["type"] if "type" in self._z else None
-        q = self._z["q"] if "q" in self._z else None
-        for f in range(coords.shape[0]):
-            t = np.ones(coords.shape[1], np.int32) if types is None else (
-                types[f] if types.ndim == 2 else types)
-            yield Frame(xyz=np.asarray(coords[f], np.float32), types=np.asarray(t, np.int32),
-                        box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f))
+        for f in range(len(self)):
+            yield self.frame(f)
 
 
 class NetCDFTrajectory:
-    """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type`` and ``q``).
+    """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type``, ``q`` and
+    ``time`` with its ``units`` and ``scale_factor`` attributes, read as netcdf.f90:432-448 does).
 
     Uses netCDF4 when importable, else scipy's reader for classic CDF-1/2 files.
     """
@@ -204,22 +212,36 @@ class NetCDFTrajectory:
             from scipy.io import netcdf_file
             self._ds = netcdf_file(path, "r", mmap=False)
             self._v = self._ds.variables
+        self.time_units, self.time_scale = "lj", 1.0
+        if "time" in self._v:
+            tv = self._v["time"]
+            u = getattr(tv, "units", b"lj")
+            self.time_units = (u.decode() if isinstance(u, bytes) else str(u)).strip()
+            self.time_scale = float(getattr(tv, "scale_factor", 1.0))
 
     def __len__(self) -> int:
         return int(self._v["coordinates"].shape[0])
 
+    def frame(self, f: int) -> Frame:
+        """Frame f (0-based)."""
+        v = self._v
+        xyz = np.asarray(v["coordinates"][f], dtype=np.float32)
+        t = np.asarray(v["type"][f], np.int32) if "type" in v else np.ones(xyz.shape[0], np.int32)
+        return Frame(xyz=xyz, types=t, box=np.asarray(v["cell_lengths"][f], np.float32),
+                     charges=_frame_charges(v["q"] if "q" in v else None, f),
+                     time=float(v["time"][f]) if "time" in v else None)
+
     def __iter__(self) -> Iterator[Frame]:
-        coords = self._v["coordinates"]
-        cells = self._v["cell_lengths"]
-        has_type = "type" in self._v
-        q = self._v["q"] if "q" in self._v else None
-        tv = self._v["time"] if "time" in self._v else None
-        for f in range(coords.shape[0]):
-            xyz = np.asarray(coords[f], dtype=np.float32)
-            t = (np.asarray(self._v["type"][f], np.int32) if has_type
-                 else np.ones(xyz.shape[0], np.int32))
-            yield Frame(xyz=xyz, types=t, box=np.asarray(cells[f], np.float32), charges=_frame_charges(q, f),
-                        time=None if tv is None else float(tv[f]))
+        for f in range(len(self)):
+            yield self.frame(f)
+
+
+def tstep_of(traj) -> float:
+    """Time per unit of the trajectory's time variable, in ps for real/metal units (common.cuf:399-412):
+    scale_factor * 0.001 for femtoseconds, scale_factor for picoseconds, scale_factor otherwise."""
+    if traj.time_units == "femtosecond":
+        return traj.time_scale * 0.001
+    return traj.time_scale
 
 
 def open_trajectory(path: str):

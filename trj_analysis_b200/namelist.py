@@ -90,7 +90,8 @@ def _list(v) -> List:
 
 def config_from_namelist(groups: Dict[str, Dict[str, Value]]):
     """Config of the g(r)/S(Q) path from /INPUT/, /INPUT_SP/, /INPUT_RDF/, /INPUT_SQ/ (input.f90:78-217)."""
-    from .analysis import Config
+    from .analysis import Config, SlabConfig
+    from .dynamics import DynConfig
     inp = groups.get("INPUT", {})
     sp = groups.get("INPUT_SP", {})
     rdf = groups.get("INPUT_RDF", {})
@@ -104,6 +105,44 @@ def config_from_namelist(groups: Dict[str, Dict[str, Value]]):
     bsc = sq.get("bsc")
     bsc = [float(x) for x in _list(bsc)] if bsc is not None else [1.0] * nsp
     bsc = (bsc + [1.0] * nsp)[:nsp]
-    return Config(nsp=nsp, sp_types_selected=sel[:nsp], run_rdf=flags[0], run_sq=flags[1],
-                  deltar=float(rdf.get("deltar", 0.02)), rcrdf=float(rdf.get("rcrdf", 0.0)),
-                  qmax=float(sq.get("qmax", -1.0)), qmin=float(sq.get("qmin", 0.0)), bsc=bsc, kset="ref")
+    cfg = Config(nsp=nsp, sp_types_selected=sel[:nsp], run_rdf=flags[0], run_sq=flags[1],
+                 deltar=float(rdf.get("deltar", 0.02)), rcrdf=float(rdf.get("rcrdf", 0.0)),
+                 qmax=float(sq.get("qmax", -1.0)), qmin=float(sq.get("qmin", 0.0)), bsc=bsc, kset="ref",
+                 ndim=int(inp.get("ndim", 3)), nrandom=int(rdf.get("nrandom", 0)))
+    # /INPUT_CONF/ with the confinement switch and g(r) or S(Q): the slab analysis (input.f90:171-191)
+    if flags[5] and (flags[0] or flags[1]):
+        conf = groups.get("INPUT_CONF", {})
+        nslice = int(inp.get("nslice", 1))
+        zs = [float(x) for x in _list(conf.get("zslice", [0.0]))][:max(1, nslice)]
+        cfg.slab = SlabConfig(zslice=tuple(zs), zgrid=float(conf.get("zgrid", 1.0)))
+    # /INPUT_DYN/, /INPUT_SQW/: time correlations (flags 4 and 5, util.f90:175-180)
+    if flags[3] or flags[4]:
+        dyn = groups.get("INPUT_DYN", {})
+        sqw = groups.get("INPUT_SQW", {})
+        qw = [float(x) for x in _list(sqw.get("qw", []))] if flags[4] else []
+        cfg.run_sqw = True
+        cfg.dyn = DynConfig(nbuffer=int(dyn.get("nbuffer", 2)), jump=int(dyn.get("jump", 1)),
+                            tlimit=float(dyn.get("tlimit", -1.0)), tmax=float(dyn.get("tmax", -1.0)),
+                            qw=tuple(qw))
+    return cfg
+
+
+def frame_schedule(ncfs_from_to, nframes: int, first_step_is_zero: bool = False) -> List[int]:
+    """0-based trajectory frames the reference reads for ncfs_from_to = (count, from, to)
+    (trj_analysis.f90:173-183 with reset_confs, util.f90:128-145): count = 0 means every frame;
+    ``to`` is increased by one; frame i (1..count) is from + (i-1)*(to-from)/count in integer
+    arithmetic, one later when the ``from`` frame is step 0 and from = 1; reading stops at the end
+    of the file."""
+    v = (list(ncfs_from_to) + [0, 0, 0])[:3]
+    count, frm, to = int(v[0]), int(v[1]), int(v[2])
+    if count == 0:
+        count, frm, to = nframes, 1, nframes
+    to += 1
+    shift = 1 if (first_step_is_zero and frm == 1) else 0
+    out = []
+    for i in range(1, count + 1):
+        ncstart = frm + (i - 1) * (to - frm) // count + shift
+        if ncstart < 1 or ncstart > nframes:
+            break
+        out.append(ncstart - 1)
+    return out

@@ -188,6 +188,8 @@ def write_dynamics(path_dir: str, res: dict, units: str = "lj") -> List[str]:
 
     emit("dyn.dat", ["#  " + tl + " " * 9 + "C_r(t)"] +
          [ln for i in rows_t for ln in format_record([t[i], res["r2t"][i]], ROW_T8)])
+    if len(qw) == 0:  # run_dyn without run_sqw: C_r(t) only
+        return files
     for name, key, lab in (("fkt.dat", "fkt", "F("), ("fskt.dat", "fskt", "Fs(")):
         head = _group_header("#  " + tl + " " * 9, [f"{lab}{fmt_f(q, 6, 4)},t)" for q in qw], 8, " " * 4)
         emit(name, head + [ln for i in rows_t for ln in format_record([t[i]] + list(res[key][i]), ROW_T8)])
