@@ -63,9 +63,10 @@ def merge(hist: Optional[torch.Tensor] = None, sq_sums: Optional[torch.Tensor] =
 def run_sharded(session, frames: Iterable, rank: int, world: int, group=None) -> Dict[str, object]:
     """Analyse this rank's frames with an `analysis.Session`, then merge over the group.
 
-    Afterwards the session's device accumulators (counts, edge statistics, S sums, g_qq sums) and its frame
+    Afterwards the session's device accumulators (counts, edge statistics, S sums, g_qq and s2n sums) and its frame
     count hold the whole trajectory on every rank, so its printrdf/printSQ give the one-GPU result.
-    Needs at least one frame per rank (the plans are sized from a rank's first frame).
+    Needs at least one frame per rank (the plans are sized from a rank's first frame).  Time
+    correlations need consecutive frames on one rank and are not sharded.
     """
     frames = list(frames)
     if len(frames) < world:
@@ -80,5 +81,8 @@ def run_sharded(session, frames: Iterable, rank: int, world: int, group=None) ->
     gqq = getattr(session, "gqq", None)
     if gqq is not None:  # charge-product histogram over avq2: a per-frame sum like the counts
         dist.all_reduce(gqq, op=dist.ReduceOp.SUM, group=group)
+    for t in (getattr(session, "gi", None), getattr(session, "g2i", None)):  # s2n sums over frames
+        if t is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     session.nconf = int(out["nframes"])
     return out
