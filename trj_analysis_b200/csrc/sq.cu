@@ -46,19 +46,20 @@ __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n
     if (q) out[n + i] = make_uint4(u[0], u[1], u[2], __float_as_uint(q[i]));
 }
 
-// Direct sum: thread owns kPlainVPT vectors; block y-index selects a slice of every species.
+// Direct sum: thread owns VPT vectors; block y-index selects a slice of every species.
 // Species qsp (if any) is the charge species: each term is weighted by the charge in the entry's w.
+template <int VPT>
 __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
     const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp, int qsp,
     const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
     int nsplit, double2* __restrict__ part) {
     __shared__ uint4 atoms[kPlainChunk];
     const int tid = threadIdx.x;
-    const int64_t vbase = (int64_t)blockIdx.x * kPlainThreads * kPlainVPT;
-    unsigned nx[kPlainVPT], ny[kPlainVPT], nz[kPlainVPT];
-    int vidx[kPlainVPT];
+    const int64_t vbase = (int64_t)blockIdx.x * kPlainThreads * VPT;
+    unsigned nx[VPT], ny[VPT], nz[VPT];
+    int vidx[VPT];
 #pragma unroll
-    for (int q = 0; q < kPlainVPT; ++q) {
+    for (int q = 0; q < VPT; ++q) {
         int64_t s = vbase + q * kPlainThreads + tid;
         vidx[q] = s < nsub ? subset[s] : -1;
         int4 v = vidx[q] >= 0 ? vecs[vidx[q]] : make_int4(0, 0, 0, 0);
@@ -71,9 +72,9 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
         int64_t a0 = sp_off[a], a1 = sp_off[a + 1];
         int64_t len = a1 - a0;
         int64_t s0 = a0 + len * blockIdx.y / nsplit, s1 = a0 + len * (blockIdx.y + 1) / nsplit;
-        double accr[kPlainVPT], acci[kPlainVPT];
+        double accr[VPT], acci[VPT];
 #pragma unroll
-        for (int q = 0; q < kPlainVPT; ++q) accr[q] = acci[q] = 0.0;
+        for (int q = 0; q < VPT; ++q) accr[q] = acci[q] = 0.0;
         const bool weighted = a == qsp;
         for (int64_t c0 = s0; c0 < s1; c0 += kPlainChunk) {
             int cnt = (int)((s1 - c0) < (int64_t)kPlainChunk ? (s1 - c0) : (int64_t)kPlainChunk);
@@ -82,14 +83,14 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
             __syncthreads();
             for (int j0 = 0; j0 < cnt; j0 += kPlainSub) {
                 int j1 = min(cnt, j0 + kPlainSub);
-                float fr[kPlainVPT], fi[kPlainVPT];
+                float fr[VPT], fi[VPT];
 #pragma unroll
-                for (int q = 0; q < kPlainVPT; ++q) fr[q] = fi[q] = 0.f;
+                for (int q = 0; q < VPT; ++q) fr[q] = fi[q] = 0.f;
                 for (int j = j0; j < j1; ++j) {
                     uint4 u = atoms[j];
                     const float w = weighted ? __uint_as_float(u.w) : 1.0f;  // fma with 1: the plain sum
 #pragma unroll
-                    for (int q = 0; q < kPlainVPT; ++q) {
+                    for (int q = 0; q < VPT; ++q) {
                         unsigned ph = nx[q] * u.x + ny[q] * u.y + nz[q] * u.z;
                         float ang = __int2float_rn((int)ph) * kScale;
                         float sn, cs;
@@ -99,16 +100,17 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < kPlainVPT; ++q) {
+                for (int q = 0; q < VPT; ++q) {
                     accr[q] += (double)fr[q];
                     acci[q] += (double)fi[q];
                 }
             }
         }
 #pragma unroll
-        for (int q = 0; q < kPlainVPT; ++q)
-            if (vidx[q] >= 0)
-                part[((int64_t)blockIdx.y * nsp + a) * nvec + vidx[q]] = make_double2(accr[q], acci[q]);
+        for (int q = 0; q < VPT; ++q)
+            if (vidx[q] >= 0)  // partials by position in the subset: [split][species][nsub]
+                part[((int64_t)blockIdx.y * nsp + a) * nsub + vbase + q * kPlainThreads + tid] =
+                    make_double2(accr[q], acci[q]);
     }
 }
 
@@ -118,10 +120,11 @@ __global__ void gather_plain_kernel(const double2* __restrict__ part, const int3
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)nsub * nsp) return;
     int a = (int)(t / nsub);
-    int v = subset[t % nsub];
+    const int64_t pos = t % nsub;
+    int v = subset[pos];
     double re = 0.0, im = 0.0;
     for (int s = 0; s < nsplit; ++s) {
-        double2 p = part[((int64_t)s * nsp + a) * nvec + v];
+        double2 p = part[((int64_t)s * nsp + a) * nsub + pos];
         re += p.x;
         im += p.y;
     }
@@ -189,14 +192,21 @@ __global__ void check_counts_kernel(const uint4* __restrict__ phase, const int64
     if (s < 0 || s >= nsp || i < sp_off[s] || i >= sp_off[s + 1]) trj_raise(status, TRJ_DEV_COUNT_MISMATCH);
 }
 
+// Vectors per thread: 4 for large vector sets; 1 when 4 per thread would leave most lanes idle
+// (the few hundred axis vectors next to the tensor tiles).
+int plain_vpt(int64_t nsub) { return nsub < (int64_t)kPlainThreads * kPlainVPT * 32 ? 1 : kPlainVPT; }
+
 int plain_nsplit(const trj_ctx* ctx, int64_t nsub, int64_t n_total) {
-    int64_t blocks_v = (nsub + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT);
+    const int vpt = plain_vpt(nsub);
+    int64_t blocks_v = (nsub + kPlainThreads * vpt - 1) / (kPlainThreads * vpt);
     if (blocks_v <= 0) return 1;
     int64_t target = (int64_t)ctx->sm_count * 8;
     int64_t ns = (target + blocks_v - 1) / blocks_v;
-    int64_t by_atoms = std::max<int64_t>(1, n_total / (4 * kPlainChunk));
+    int64_t by_atoms = std::max<int64_t>(1, n_total / (2 * kPlainChunk));
     ns = std::min<int64_t>(ns, by_atoms);
-    ns = std::max<int64_t>(1, std::min<int64_t>(ns, 128));
+    // partials are nsplit x species x vectors x 16 bytes: allow more splits for small vector sets
+    const int64_t cap = nsub <= 32768 ? 1024 : 128;
+    ns = std::max<int64_t>(1, std::min<int64_t>(ns, cap));
     return (int)ns;
 }
 
@@ -381,8 +391,9 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     p->nsplit_all = plain_nsplit(ctx, nvec, p->n_total);
     p->nsplit_sparse = plain_nsplit(ctx, p->n_sparse, p->n_total);
     size_t phase_b = sizeof(uint4) * (size_t)std::max<int64_t>(1, p->n_total);
-    size_t part_b = sizeof(double2) * (size_t)std::max(p->nsplit_all, p->nsplit_sparse) * nsp *
-                    (size_t)std::max<int64_t>(1, nvec);
+    size_t part_b = sizeof(double2) * (size_t)nsp *
+                    std::max<size_t>((size_t)p->nsplit_all * std::max<int64_t>(1, nvec),
+                                     (size_t)p->nsplit_sparse * std::max<int64_t>(1, p->n_sparse));
     size_t rho_b = sizeof(double2) * (size_t)nsp * (size_t)std::max<int64_t>(1, nvec);
     if (trj_dev_alloc(ctx, (void**)&p->phase_dev, phase_b) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&p->part_dev, part_b) != cudaSuccess ||
@@ -439,10 +450,16 @@ extern "C" int trj_sq_plan_info(const trj_sq_plan* p, int64_t* n_dense, int64_t*
 static int run_plain(trj_sq_plan* p, const int32_t* subset, int64_t nsub, int nsplit, cudaStream_t s,
                      bool timed) {
     if (nsub <= 0) return TRJ_OK;
-    dim3 grid((unsigned)((nsub + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT)), (unsigned)nsplit);
+    const int vpt = plain_vpt(nsub);
+    dim3 grid((unsigned)((nsub + kPlainThreads * vpt - 1) / (kPlainThreads * vpt)), (unsigned)nsplit);
     if (timed) p->timer.begin(p->ctx, s);
-    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->qsp, p->vec_dev, subset,
-                                                   (int)nsub, p->nvec, nsplit, p->part_dev);
+    if (vpt == 1)
+        sq_plain_kernel<1><<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->qsp, p->vec_dev,
+                                                          subset, (int)nsub, p->nvec, nsplit, p->part_dev);
+    else
+        sq_plain_kernel<kPlainVPT><<<grid, kPlainThreads, 0, s>>>(p->phase_dev, p->species_off_dev, p->nsp, p->qsp,
+                                                                  p->vec_dev, subset, (int)nsub, p->nvec, nsplit,
+                                                                  p->part_dev);
     if (timed) p->timer.end(p->ctx, s);
     int64_t tot = nsub * p->nsp;
     gather_plain_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(p->part_dev, subset, (int)nsub, p->nvec,
@@ -561,9 +578,14 @@ extern "C" int trj_sq_rho_groups(trj_sq_plan* p, const float* packed_dev, int64_
     if (n > 0)
         phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
                                                                        (double)box[1], (double)box[2], phase, nullptr);
-    dim3 grid((unsigned)((p->nvec + kPlainThreads * kPlainVPT - 1) / (kPlainThreads * kPlainVPT)), (unsigned)nsplit);
-    sq_plain_kernel<<<grid, kPlainThreads, 0, s>>>(phase, off, ngroups, -1, p->vec_dev, p->plain_all_dev,
-                                                   (int)p->nvec, p->nvec, nsplit, part);
+    const int vpt = plain_vpt(p->nvec);
+    dim3 grid((unsigned)((p->nvec + kPlainThreads * vpt - 1) / (kPlainThreads * vpt)), (unsigned)nsplit);
+    if (vpt == 1)
+        sq_plain_kernel<1><<<grid, kPlainThreads, 0, s>>>(phase, off, ngroups, -1, p->vec_dev, p->plain_all_dev,
+                                                          (int)p->nvec, p->nvec, nsplit, part);
+    else
+        sq_plain_kernel<kPlainVPT><<<grid, kPlainThreads, 0, s>>>(phase, off, ngroups, -1, p->vec_dev,
+                                                                  p->plain_all_dev, (int)p->nvec, p->nvec, nsplit, part);
     const int64_t tot = p->nvec * ngroups;
     gather_plain_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(part, p->plain_all_dev, (int)p->nvec, p->nvec,
                                                                       ngroups, nsplit, rho);
