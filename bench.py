@@ -67,9 +67,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--serving", type=int, default=200, help="requests in the serving run (0: skip)")
-    ap.add_argument("--row", default="main", choices=["main", "charges", "dyn"],
+    ap.add_argument("--row", default="main", choices=["main", "charges", "dyn", "extras"],
                     help="main: the g(r)+S(Q) frame rate; charges: the same frames with per-atom charges "
-                         "(g_qq, S_qq); dyn: F(Q,t)/Fs(Q,t)/MSD over time origins")
+                         "(g_qq, S_qq); dyn: F(Q,t)/Fs(Q,t)/MSD over time origins; extras: number "
+                         "fluctuations, a two-dimensional frame and the slab analysis")
     return ap.parse_args()
 
 
@@ -579,10 +580,73 @@ def run_dyn(args):
                             "terms_per_clk_per_sm": self_tps / (ctx.sm_count * 1.9e9)}}
 
 
+def run_extras(args):
+    """Timings of the remaining analyses on the benchmark frame's scale:
+    s2n: trj_rdf_s2n with 4096 sample points after the c3 frame's pair pass;
+    2d: a two-dimensional frame of 1,000,000 atoms (square lattice with noise, 2 species) through the 2D
+        pair plan (deltar 0.01, rcrdf 8) and the 2D reference vector set (qmax 10, qmin 3, direct sum);
+    slab: the c3 frame in three z slices (g_xy and S_xy, host-orchestrated per slice)."""
+    import torch
+    from trj_analysis_b200 import analysis, engine, frames, refsem
+    out = {}
+    wl = WORKLOADS["c3"]
+    spec = frames.c3_spec()
+    fr = spec.frame(0)
+    n, box = fr.n, fr.box
+    ctx = engine.Context(0)
+    stage = engine.FrameStage(ctx, n, 3)
+    nn = stage.upload_and_pack(fr.xyz, fr.types - 1, box)
+    rdf = engine.RdfPlan(ctx, 3, wl["deltar"], wl["rcrdf"], box, n)
+    hist = rdf.new_hist()
+    gi, g2i = rdf.new_s2n()
+    rdf.accumulate(stage.packed, nn, box, hist)
+    ms = _events(lambda i: rdf.s2n(4096, gi, g2i), args.warmup + args.steps, None)[args.warmup:]
+    out["s2n"] = {"points": 4096, "ms": statistics.median(ms), "workload": "c3 frame, 13^3 cells"}
+    ctx.check()
+    # two-dimensional frame
+    rng = np.random.default_rng(7)
+    side = 1000
+    a = 1.1
+    gx, gy = np.meshgrid(np.arange(side), np.arange(side), indexing="ij")
+    xy = np.stack([gx.ravel(), gy.ravel()], axis=1) * a + rng.normal(0, 0.12 * a, size=(side * side, 2))
+    xyz = np.concatenate([xy, np.zeros((side * side, 1))], axis=1).astype(np.float32)
+    types = rng.permutation(np.repeat(np.array([1, 2], np.int32), [side * side // 2, side * side // 2]))
+    f2 = frames.Frame(xyz=xyz, types=types, box=np.array([side * a, side * a, 1.0], np.float32))
+    cfg = analysis.Config(nsp=2, ndim=2, sp_types_selected=(1, 2), deltar=0.01, rcrdf=8.0, qmax=10.0, qmin=3.0,
+                          method="plain", kset="ref")
+    sess = analysis.Session(cfg, ctx=ctx)
+    sess.add_frame(f2)
+    torch.cuda.synchronize()
+    ms = _events(lambda i: (sess.RDFcomp(), sess.SQcalc()), args.warmup + args.steps, None)[args.warmup:]
+    out["2d"] = {"n_atoms": side * side, "n_kvec": int(sess.kset.nvec), "frame_ms": statistics.median(ms),
+                 "frames_per_s": 1000.0 / statistics.median(ms)}
+    sess.ctx.check()
+    sess.close()
+    # slab analysis of the c3 frame in three slices
+    zmax = float(box[2])
+    cfg = analysis.Config(nsp=3, sp_types_selected=(1, 2, 3), deltar=wl["deltar"], rcrdf=wl["rcrdf"], qmax=6.0,
+                          qmin=3.0, slab=analysis.SlabConfig(zslice=(0.25 * zmax, 0.5 * zmax, 0.75 * zmax),
+                                                             zgrid=0.1 * zmax))
+    sess = analysis.Session(cfg, ctx=ctx)
+    sess.add_frame(fr)
+    t = []
+    for i in range(max(2, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sess.add_frame(fr)
+        torch.cuda.synchronize()
+        t.append((time.perf_counter() - t0) * 1000.0)
+    out["slab"] = {"slices": 3, "frame_ms_wall": statistics.median(t), "workload": "c3 frame, 3 slices of 0.1 L"}
+    sess.close()
+    ctx.check()
+    return {"metric": "secondary analyses: s2n, 2D frame, slabs", "unit": "ms", "n_gpus": 1, "data": "synthetic",
+            "detail": out}
+
+
 def main():
     args = parse()
     if args.row != "main":
-        res = run_charges(args) if args.row == "charges" else run_dyn(args)
+        res = {"charges": run_charges, "dyn": run_dyn, "extras": run_extras}[args.row](args)
         print(json.dumps(res), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
