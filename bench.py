@@ -612,16 +612,18 @@ def run_extras(args):
     xyz = np.concatenate([xy, np.zeros((side * side, 1))], axis=1).astype(np.float32)
     types = rng.permutation(np.repeat(np.array([1, 2], np.int32), [side * side // 2, side * side // 2]))
     f2 = frames.Frame(xyz=xyz, types=types, box=np.array([side * a, side * a, 1.0], np.float32))
-    cfg = analysis.Config(nsp=2, ndim=2, sp_types_selected=(1, 2), deltar=0.01, rcrdf=8.0, qmax=10.0, qmin=3.0,
-                          method="plain", kset="ref")
-    sess = analysis.Session(cfg, ctx=ctx)
-    sess.add_frame(f2)
-    torch.cuda.synchronize()
-    ms = _events(lambda i: (sess.RDFcomp(), sess.SQcalc()), args.warmup + args.steps, None)[args.warmup:]
-    out["2d"] = {"n_atoms": side * side, "n_kvec": int(sess.kset.nvec), "frame_ms": statistics.median(ms),
-                 "frames_per_s": 1000.0 / statistics.median(ms)}
-    sess.ctx.check()
-    sess.close()
+    out["2d"] = {"n_atoms": side * side}
+    for method in ("split", "plain"):  # split: the planar tile form on the tensor cores
+        cfg = analysis.Config(nsp=2, ndim=2, sp_types_selected=(1, 2), deltar=0.01, rcrdf=8.0, qmax=10.0, qmin=3.0,
+                              method=method, kset="ref")
+        sess = analysis.Session(cfg, ctx=ctx)
+        sess.add_frame(f2)
+        torch.cuda.synchronize()
+        ms = _events(lambda i: (sess.RDFcomp(), sess.SQcalc()), args.warmup + args.steps, None)[args.warmup:]
+        out["2d"]["n_kvec"] = int(sess.kset.nvec)
+        out["2d"][method] = {"frame_ms": statistics.median(ms), "frames_per_s": 1000.0 / statistics.median(ms)}
+        sess.ctx.check()
+        sess.close()
     # slab analysis of the c3 frame in three slices
     zmax = float(box[2])
     cfg = analysis.Config(nsp=3, sp_types_selected=(1, 2, 3), deltar=wl["deltar"], rcrdf=wl["rcrdf"], qmax=6.0,

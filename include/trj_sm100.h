@@ -262,6 +262,12 @@ TRJ_API int trj_sq_plan_create_charged(trj_ctx* ctx, int nsp, int64_t nvec, cons
  * trj_frame_pack_charges.  A charged plan accepts only this call. */
 TRJ_API int trj_sq_accumulate_charged(trj_sq_plan* plan, const float* packed_dev, const float* charge_packed_dev,
                                       int64_t n, const float box[3], int method, double* out_dev, void* stream);
+/* Planar frames in tile form (mul > 0): every atom's third phase coordinate is
+ * taken as mul * (its second) mod 1, exactly in 32-bit fixed point, instead of
+ * its z.  A plan whose vectors are (nx, ny mod mul, ny div mul) then evaluates
+ * the in-plane vectors (nx, ny) of a z = 0 frame, and 16 x 8 x nz tensor tiles
+ * fill with them (ndim = 2 S(Q) on the tensor path).  0 turns it off. */
+TRJ_API int trj_sq_plan_set_z_from_y(trj_sq_plan* plan, int mul);
 /* Direct sums over caller-defined atom groups, for the plan's vectors:
  * rho_g(k) = sum over atoms j in group g of exp(i k.r_j), FP64 [ngroups][nvec][2]
  * in the caller's vector order.  packed_dev holds n atoms (x, y, z; w unused)

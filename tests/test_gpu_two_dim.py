@@ -26,10 +26,11 @@ def _frames_2d(nx, ny, a, nframes, seed):
     return out
 
 
-def test_session_2d_matches_oracle():
+@pytest.mark.parametrize("method", ["plain", "split"])  # split: the planar tile form on the tensor cores
+def test_session_2d_matches_oracle(method):
     frs = _frames_2d(60, 48, 1.1, 2, seed=12)
     cfg = analysis.Config(nsp=2, ndim=2, sp_types_selected=(1, 2), deltar=0.05, rcrdf=6.0, qmax=6.0, qmin=2.5,
-                          method="plain", kset="ref", nrandom=20)
+                          method=method, kset="ref", nrandom=20)
     s = analysis.Session(cfg)
     hist_want = None
     gi_w = g2i_w = None
@@ -50,9 +51,14 @@ def test_session_2d_matches_oracle():
         gi_w = a if gi_w is None else gi_w + a
         g2i_w = b if g2i_w is None else g2i_w + b
         rho = s.sq.rho().cpu().numpy()
-        rho_o = orc.rho_fp64(pos, off, box, s.kset.vectors)
+        v = s.kset.vectors.astype(np.int64)
+        if method == "split":  # planar tile form (nx, ny mod 8, ny div 8) -> in-plane (nx, ny, 0)
+            assert s.sq.n_tiles > 0
+            v = np.stack([v[:, 0], v[:, 1] + 8 * v[:, 2], 0 * v[:, 2]], axis=1)
+        rho_o = orc.rho_fp64(pos, off, box, v.astype(np.int32))
+        per, floor = (2e-6, 1e-6) if method == "plain" else (3e-5, 1e-5)
         for k in range(2):
-            assert np.abs(rho[k] - rho_o[k]).max() <= 2e-6 * (off[k + 1] - off[k]) + 1e-6
+            assert np.abs(rho[k] - rho_o[k]).max() <= per * (off[k + 1] - off[k]) + floor
     s.ctx.check()
     np.testing.assert_array_equal(s.rdf_transfer(), hist_want)
     np.testing.assert_array_equal(s.gi.cpu().numpy(), gi_w)

@@ -85,7 +85,11 @@ def test_sq_init_2d(box, qmax, qmin):
         assert si.lmax[:2] == tuple(lm) and si.nqmin == min(lm)
     ks = refsem.make_kset("ref", b, qmax, qmin, ndim=2)
     assert np.all(ks.vectors[:, 2] == 0)
-    assert not ks.dense.any()
+    pt = refsem.planar_tiles(ks, 8)
+    v = ks.vectors.astype(np.int64)
+    np.testing.assert_array_equal(pt.vectors[:, 1] + 8 * pt.vectors[:, 2], v[:, 1])
+    np.testing.assert_array_equal(pt.vectors[:, 0], v[:, 0])
+    assert np.all((pt.vectors[:, 1] >= 0) & (pt.vectors[:, 1] < 8))
     if si.nqmin > 1:
         np.testing.assert_array_equal(ks.nq, _nq2_loops(si))
         # sqfnD, dim = 2: every (kx, ky) of the launch grid with 0 < q2 <= qmin^2, q2 = fma(kf2, kf2, kf1*kf1)

@@ -233,7 +233,14 @@ class Session:
     def sq_init(self) -> None:
         c = self.cfg
         self.kset = refsem.make_kset(c.kset, self.box, c.qmax, c.qmin, seed=c.seed, per_shell=c.per_shell, ndim=c.ndim)
+        planar = c.ndim == 2 and c.method in ("split", "split_bf16x3")
+        if planar:  # in-plane vectors as (nx, ny mod 8, ny div 8) so that they fill tensor tiles
+            self.kset = refsem.planar_tiles(self.kset, 8)
+        elif c.ndim == 2:
+            self.kset = dataclasses.replace(self.kset, dense=np.zeros_like(self.kset.dense))
         self.sq = engine.SqPlan(self.ctx, c.nsp, self.kset, self.ntype, charged=self.device_charges)
+        if planar:
+            self.sq.set_z_from_y(8)
         self.sq_out = self.sq.new_out()
 
     def SQcalc(self) -> None:

@@ -30,8 +30,11 @@ constexpr int kPlainSub = 64;          // FP32 partial-sum length before the FP6
 // Fixed-point phase coordinates of every atom.  With charges (q non-null) every atom is written a
 // second time at n + i as a member of the charge species qsp, its charge (FP32 bits) in place of the
 // species index: rho_q(k) = sum_j q_j exp(i k.r_j) (sq.cuf:569-573) is then the sum of that species.
+// zmul != 0 (planar frames in tile form): the third phase is zmul * u_y mod 2^32, exactly, so that
+// lattice vector (nx, ny mod zmul, ny div zmul) has the phase of (nx, ny) in the plane.
 __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n, double Lx, double Ly,
-                                    double Lz, uint4* __restrict__ out, const float* __restrict__ q) {
+                                    double Lz, uint4* __restrict__ out, const float* __restrict__ q,
+                                    unsigned zmul) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 v = packed[i];
@@ -42,6 +45,7 @@ __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n
         double f = s[d] - floor(s[d]);             // [0, 1]
         u[d] = (unsigned)(long long)rint(f * 4294967296.0);  // 2^32 wraps to 0
     }
+    if (zmul) u[2] = u[1] * zmul;
     out[i] = make_uint4(u[0], u[1], u[2], (unsigned)__float_as_int(v.w));
     if (q) out[n + i] = make_uint4(u[0], u[1], u[2], __float_as_uint(q[i]));
 }
@@ -487,7 +491,7 @@ static int sq_accumulate_impl(trj_sq_plan* p, const float* packed_dev, const flo
     if (n > 0) {
         phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
                                                                        (double)box[1], (double)box[2], p->phase_dev,
-                                                                       charge_dev);
+                                                                       charge_dev, p->z_from_y);
         // the charge entries (n .. 2n-1) are the same atoms: only the first n carry species to check
         check_counts_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->phase_dev, p->species_off_dev,
                                                                         p->qsp >= 0 ? p->qsp : p->nsp, n,
@@ -577,7 +581,8 @@ extern "C" int trj_sq_rho_groups(trj_sq_plan* p, const float* packed_dev, int64_
     TRJ_CUDA_TRY(ctx, cudaMemcpyAsync(off, group_off_host, off_need, cudaMemcpyHostToDevice, s));
     if (n > 0)
         phase_coords_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const float4*)packed_dev, n, (double)box[0],
-                                                                       (double)box[1], (double)box[2], phase, nullptr);
+                                                                       (double)box[1], (double)box[2], phase, nullptr,
+                                                                       p->z_from_y);
     const int vpt = plain_vpt(p->nvec);
     dim3 grid((unsigned)((p->nvec + kPlainThreads * vpt - 1) / (kPlainThreads * vpt)), (unsigned)nsplit);
     if (vpt == 1)
@@ -611,5 +616,12 @@ extern "C" int trj_sq_rho(trj_sq_plan* p, double* rho_out, void* stream) {
     unpermute_rho_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
         p->rho_dev, p->vec_dev, p->nvec, p->nsp, (double2*)rho_out);
     TRJ_CUDA_TRY(p->ctx, cudaGetLastError());
+    return TRJ_OK;
+}
+
+extern "C" int trj_sq_plan_set_z_from_y(trj_sq_plan* p, int mul) {
+    if (!p) return TRJ_ERR_INVALID;
+    if (mul < 0 || mul > 1024) return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq plan: z-from-y multiplier %d", mul);
+    p->z_from_y = (unsigned)mul;
     return TRJ_OK;
 }

@@ -24,6 +24,7 @@ struct trj_sq_plan {
     int64_t n_total = 0;                   // phase entries: atoms, plus the charge species' copies
     int64_t n_atoms = 0;                   // atoms per frame
     int qsp = -1;                          // index of the charge species (charged plans), else -1
+    unsigned z_from_y = 0;                 // planar tile form: third phase = z_from_y * u_y (0: off)
     std::vector<int64_t> species_counts;   // host
     std::vector<int64_t> species_off;      // host, nsp+1
     // vectors in plan order (sorted by bin); perm[plan_index] = caller index

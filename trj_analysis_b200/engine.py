@@ -211,6 +211,10 @@ class SqPlan:
         """Atoms the tensor cores accumulate in one FP32 run before it is added into the running sum."""
         check(self.ctx.lib.trj_sq_plan_set_flush(self.h, int(atoms)), self.ctx.h, "trj_sq_plan_set_flush")
 
+    def set_z_from_y(self, mul: int) -> None:
+        """Planar tile form: third phase = mul * second phase (exact); vectors (nx, ny % mul, ny // mul)."""
+        check(self.ctx.lib.trj_sq_plan_set_z_from_y(self.h, int(mul)), self.ctx.h, "trj_sq_plan_set_z_from_y")
+
     def set_pairs(self, enable: bool) -> None:
         """Tensor-core tiles in CTA pairs (one M = 256 contraction per two tiles) or one per CTA."""
         check(self.ctx.lib.trj_sq_plan_set_pairs(self.h, 1 if enable else 0), self.ctx.h, "trj_sq_plan_set_pairs")

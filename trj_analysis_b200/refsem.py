@@ -290,8 +290,7 @@ def reference_kset(box, qmax: float, qmin: float, ndim: int = 3) -> KSet:
     V = np.concatenate(vecs).astype(np.int32) if vecs else np.zeros((0, 3), np.int32)
     B = np.concatenate(bins).astype(np.int32) if bins else np.zeros(0, np.int32)
     dense = np.zeros(V.shape[0], np.uint8)
-    if ndim == 3:  # 2D vectors (nz = 0 only) fill one column of a tensor tile: direct sum only
-        dense[:nd] = 1
+    dense[:nd] = 1  # 2D: tensor tiles only in the planar tile form (planar_tiles)
     return KSet(mode="ref", dq=si.dq, nqmax=si.nqmax, vectors=V, bins=B,
                 weights=np.ones(V.shape[0]), dense=dense, nq=reference_nq(si, ndim),
                 qmin_eff=si.qmin_eff, lmax=si.lmax, nqmin=si.nqmin)
@@ -579,3 +578,16 @@ def slab_of(z: np.ndarray, zslice: Sequence[float], zgrid: float) -> np.ndarray:
     s = np.argmin(d, axis=1)  # first minimum, as minloc
     ok = d[np.arange(z.shape[0]), s] <= F32(F32(zgrid) / F32(2.0))
     return np.where(ok, s, -1).astype(np.int64)
+
+
+def planar_tiles(ks: KSet, mul: int = 8) -> KSet:
+    """The vectors of a two-dimensional k-set in the planar tile form: (nx, ny, 0) becomes
+    (nx, ny mod mul, ny div mul), to be evaluated with the third phase taken as mul times the second
+    (trj_sq_plan_set_z_from_y), which gives it exactly the phase of (nx, ny).  Tensor tiles of 16 nx x
+    8 ny rows then fill with in-plane vectors (ny mod 8 over the rows, ny div 8 over the columns).
+    Bins, weights and n(Q) are unchanged."""
+    v = ks.vectors.astype(np.int64)
+    if np.any(v[:, 2] != 0) or np.any(v[:, 1] < 0):
+        raise ValueError("planar tile form: vectors must be (nx, ny >= 0, 0)")
+    t = np.stack([v[:, 0], v[:, 1] % mul, v[:, 1] // mul], axis=1).astype(np.int32)
+    return dataclasses.replace(ks, vectors=t)
