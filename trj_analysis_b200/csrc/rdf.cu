@@ -13,6 +13,12 @@
 // the counts equal the all-pairs sweep exactly.  Axes with fewer than 3 cells are not split
 // (one cell along that axis); a frame with no split axis is the all-pairs case.
 //
+// Within a cell, atoms are ordered along a Morton curve over S^3 sub-cells, so the 64 home atoms of
+// a warp (two per lane, consecutive in that order) fill a small box.  Each warp tests 32 staged
+// neighbour atoms at a time against that box grown by the cutoff (one ballot) and runs the exact
+// pair test only for the neighbours that can be in range: a conservative cull, the counts are
+// those of the full stencil.
+//
 // Neighbour-cell atoms are staged into shared memory with 1-D TMA bulk copies
 // (cp.async.bulk, no multicast), double-buffered on mbarriers; each warp counts into its own
 // uint32 shared histogram replica; replicas are merged with 64-bit global atomics at exit.
@@ -27,9 +33,9 @@
 namespace {
 
 constexpr int kThreads = 256;       // threads per CTA
-constexpr int kHome = 2;            // home atoms per thread
-constexpr int kHomeChunk = kThreads * kHome;
+constexpr int kHomeChunk = 2 * kThreads;  // two home atoms per thread: a warp holds 64 consecutive atoms
 constexpr int kJChunk = 512;        // neighbour atoms per staged buffer (8 KB)
+constexpr int kSlots = 2;           // staged buffers (tasks in flight per CTA)
 constexpr int kMaxOffsets = 14;
 
 struct RdfParams {
@@ -45,6 +51,8 @@ struct RdfParams {
     int hsplit, jsplit;
     int nrep;
     int fast_ok;                // every axis split into >= 5 cells
+    float cull2;                // (cutoff * (1 + 2^-10))^2: neighbours farther from a warp's box are skipped
+    float cull_pad;             // added to the box half-widths: covers the FP32 rounding of the cull test
     int off[kMaxOffsets][3];
     int64_t nitems;
 };
@@ -57,6 +65,8 @@ struct TaskInfo {
     int hc;            // home chunk
     int self;          // home cell == neighbour cell
     int fast;          // no minimum image needed for any pair of the task
+    int cull;          // both cells hold only coordinates in [0, L): the box cull applies
+    float img[3];      // periodic image of the neighbour cell: 0 or -+L per axis
     int valid;         // 0 = no more tasks
 };
 
@@ -144,6 +154,10 @@ __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restr
             t.hc = g.hc;
             t.self = self;
             t.fast = p.fast_ok && !wraps && !cflag[c] && !cflag[c2];
+            t.cull = !cflag[c] && !cflag[c2];
+            t.img[0] = ex < 0 ? -p.L[0] : (ex >= p.nc[0] ? p.L[0] : 0.f);
+            t.img[1] = ey < 0 ? -p.L[1] : (ey >= p.nc[1] ? p.L[1] : 0.f);
+            t.img[2] = ez < 0 ? -p.L[2] : (ez >= p.nc[2] ? p.L[2] : 0.f);
             t.valid = 1;
             g.jc += 1;
             return true;
@@ -217,21 +231,97 @@ __device__ __forceinline__ void pair(const float4& a, const float4& b, bool vali
     }
 }
 
+// Box of the warp's home atoms, centred on the neighbour cell's periodic image: a neighbour b can be
+// within the cutoff of some home atom only if |b - c| - h, clipped at 0 per axis, has squared length
+// <= cull2.  Unsplit axes (one cell) get an infinite half-width: no cull along them.
+struct WarpBox {
+    float4 c, h;  // centre (x, y, z) and half-widths (x, y, z); .w unused
+};
+
+__device__ __forceinline__ void axis_box(float v0, bool has0, float v1, bool has1, bool split, float img, float pad,
+                                         float& c, float& h) {
+    // Coordinates of cull tasks lie in [0, L): their bit patterns order like the values (+0 for -0).
+    const unsigned b0 = __float_as_uint(v0 + 0.0f), b1 = __float_as_uint(v1 + 0.0f);
+    const unsigned lo = min(has0 ? b0 : 0x7f800000u, has1 ? b1 : 0x7f800000u);
+    const unsigned hi = max(has0 ? b0 : 0u, has1 ? b1 : 0u);
+    const float mn = __uint_as_float(__reduce_min_sync(0xffffffffu, lo));
+    const float mx = __uint_as_float(__reduce_max_sync(0xffffffffu, hi));
+    c = 0.5f * (mn + mx) - img;
+    h = split ? 0.5f * (mx - mn) + pad : INFINITY;
+}
+
+__device__ __forceinline__ bool maybe_near(const float4& b, const float4& c, const float4& h, float cull2) {
+    const float gx = fmaxf(fabsf(b.x - c.x) - h.x, 0.f);
+    const float gy = fmaxf(fabsf(b.y - c.y) - h.y, 0.f);
+    const float gz = fmaxf(fabsf(b.z - c.z) - h.z, 0.f);
+    return fmaf(gz, gz, fmaf(gy, gy, gx * gx)) <= cull2;
+}
+
+// One task for one warp: its 64 home atoms (a0 = atom il0, a1 = atom il0 + 32 per lane) against the
+// staged neighbour chunk.  Blocks of 32 neighbours are culled against the warp's box (kept in shared
+// memory, `wb`) with one ballot; the survivors are tested exactly.  Returns the candidate pairs tested.
 template <bool FAST, bool QMODE>
-__device__ __forceinline__ void run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
-                                         const float4& a1, bool h0, bool h1, int il0, int il1, int s0, int s1,
-                                         const RdfParams& p, const int* rowtab, unsigned* myhist, PairCounters& pc,
-                                         double* myq, float qa0, float qa1, const float* qj) {
-    int jbeg = 0;
-    if (ti.self) jbeg = max(0, il0 + 1 - ti.jlocal0);  // il0 < il1: a0 starts earlier
-    if (!h0 && !h1) jbeg = ti.jcount;
-    if (!h0 && h1) jbeg = ti.self ? max(0, il1 + 1 - ti.jlocal0) : 0;
-    const int lim1 = ti.self ? il1 - ti.jlocal0 : -1;  // a1 pairs need jj > lim1
-#pragma unroll 2
-    for (int jj = jbeg; jj < ti.jcount; ++jj) {
-        const float4 b = bj[jj];
-        pair<FAST, QMODE>(a0, b, h0, s0, p, rowtab, myhist, pc, myq, qa0, qj + jj);
-        pair<FAST, QMODE>(a1, b, h1 && jj > lim1, s1, p, rowtab, myhist, pc, myq, qa1, qj + jj);
+__device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
+                                             const float4& a1, bool h0, bool h1, int il0, int s0, int s1,
+                                             unsigned lane, const RdfParams& p, const int* rowtab, unsigned* myhist,
+                                             PairCounters& pc, double* myq, float qa0, float qa1, const float* qj,
+                                             WarpBox* wb) {
+    const int il0w = il0 - (int)lane;  // the warp's first home atom
+    if (il0w >= ti.na) return 0u;
+    if (ti.cull) {
+        float cx, cy, cz, hx, hy, hz;
+        axis_box(a0.x, h0, a1.x, h1, p.nc[0] > 1, ti.img[0], p.cull_pad, cx, hx);
+        axis_box(a0.y, h0, a1.y, h1, p.nc[1] > 1, ti.img[1], p.cull_pad, cy, hy);
+        axis_box(a0.z, h0, a1.z, h1, p.nc[2] > 1, ti.img[2], p.cull_pad, cz, hz);
+        if (lane == 0) {
+            wb->c = make_float4(cx, cy, cz, 0.f);
+            wb->h = make_float4(hx, hy, hz, 0.f);
+        }
+        __syncwarp();
+    }
+    const int jbeg = ti.self ? max(0, il0w + 1 - ti.jlocal0) : 0;
+    const int lim0 = ti.self ? il0 - ti.jlocal0 : -1;  // a0 pairs need jj > lim0
+    const int lim1 = ti.self ? lim0 + 32 : -1;           // a1 pairs need jj > lim1
+    unsigned tested = 0;
+    for (int jj0 = jbeg; jj0 < ti.jcount; jj0 += 32) {
+        const int jl = jj0 + (int)lane;
+        bool keep = jl < ti.jcount;
+        if (ti.cull && keep) keep = maybe_near(bj[jl], wb->c, wb->h, p.cull2);
+        unsigned m = __ballot_sync(0xffffffffu, keep);
+        while (m) {
+            const int k0 = __ffs(m) - 1;
+            m &= m - 1u;
+            const int j0 = jj0 + k0;
+            const float4 b0 = bj[j0];
+            const bool v0 = h0 && j0 > lim0;
+            const bool v1 = h1 && j0 > lim1;
+            pair<FAST, QMODE>(a0, b0, v0, s0, p, rowtab, myhist, pc, myq, qa0, qj + j0);
+            pair<FAST, QMODE>(a1, b0, v1, s1, p, rowtab, myhist, pc, myq, qa1, qj + j0);
+            tested += (unsigned)v0 + (unsigned)v1;
+        }
+    }
+    return tested;
+}
+
+// Arms the next phase of a staging slot: the next task's neighbour chunk by bulk copy, or a plain
+// arrival with valid = 0 when the work is exhausted (readers of that phase leave the task loop).
+__device__ __forceinline__ void refill_slot(int slot, TaskGen& gen, const RdfParams& p,
+                                            const int32_t* __restrict__ cstart, const int32_t* __restrict__ ccount,
+                                            const int32_t* __restrict__ cflag, unsigned long long* work,
+                                            const float4* __restrict__ sorted, TaskInfo* tinfo, uint64_t* bars,
+                                            unsigned* phases, float4* buf) {
+    TaskInfo nx;
+    const bool ok = next_task(gen, p, cstart, ccount, cflag, work, nx);
+    tinfo[slot] = nx;
+    phases[slot] += 1u;
+    if (ok) {
+        // The slot's previous contents were read through the generic proxy; order those reads before
+        // the bulk copy (async proxy) overwrites them.
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        trj_mbar_arrive_expect_tx(&bars[slot], nx.jcount * 16u);
+        trj_bulk_g2s(buf + slot * kJChunk, sorted + nx.sb, nx.jcount * 16u, &bars[slot]);
+    } else {
+        trj_mbar_arrive(&bars[slot]);
     }
 }
 
@@ -250,14 +340,19 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
                                                              const float* __restrict__ sorted_q,
                                                              double* __restrict__ gqq_frame) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float4* buf = reinterpret_cast<float4*>(smem);                       // [2][kJChunk]
-    unsigned* hist = reinterpret_cast<unsigned*>(smem + 2 * kJChunk * sizeof(float4));
-    __shared__ __align__(8) uint64_t bars[2];
-    __shared__ TaskInfo tinfo[2];
+    float4* buf = reinterpret_cast<float4*>(smem);                       // [kSlots][kJChunk]
+    unsigned* hist = reinterpret_cast<unsigned*>(smem + kSlots * kJChunk * sizeof(float4));
+    __shared__ __align__(8) uint64_t bars[kSlots];
+    __shared__ TaskInfo tinfo[kSlots];
+    __shared__ unsigned released[kSlots];  // warps done with the slot's task
+    __shared__ unsigned phases[kSlots];    // phases armed per slot
+    __shared__ TaskGen gen;                // task iterator, used by one refilling thread at a time
     __shared__ int rowtab[16 * 16];
     __shared__ int abort_flag;
+    __shared__ WarpBox wboxes[kThreads / 32];
 
     const int tid = threadIdx.x, warp = tid / 32;
+    const unsigned lane = (unsigned)tid & 31u;
     const int hsz = p.nit * p.lsmax;
     unsigned* myhist = hist + (size_t)(warp % p.nrep) * hsz;
     for (int k = tid; k < p.nrep * hsz; k += blockDim.x) hist[k] = 0u;
@@ -269,38 +364,37 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         for (int k = tid; k < p.nrep * p.lsmax; k += blockDim.x) qhist[k] = 0.0;
     }
     for (int k = tid; k < p.nsp * p.nsp; k += blockDim.x) rowtab[k] = trj_pair_row(k / p.nsp, k % p.nsp, p.nsp);
-    TaskGen gen;
-    gen.started = 0;
-    unsigned issued[2] = {0u, 0u};  // copies issued per staging slot (thread 0)
     if (tid == 0) {
+        gen.started = 0;
         abort_flag = 0;
-        trj_mbar_init(&bars[0], 1);
-        trj_mbar_init(&bars[1], 1);
-        trj_fence_mbar_init();
-        if (next_task(gen, p, cstart, ccount, cflag, work, tinfo[0])) {
-            trj_mbar_arrive_expect_tx(&bars[0], tinfo[0].jcount * 16u);
-            trj_bulk_g2s(buf, sorted + tinfo[0].sb, tinfo[0].jcount * 16u, &bars[0]);
-            issued[0] = 1;
+        for (int sl = 0; sl < kSlots; ++sl) {
+            trj_mbar_init(&bars[sl], 1);
+            released[sl] = 0u;
+            phases[sl] = 0u;
         }
+        trj_fence_mbar_init();
+        for (int sl = 0; sl < kSlots; ++sl) refill_slot(sl, gen, p, cstart, ccount, cflag, work, sorted, tinfo, bars, phases, buf);
     }
+    __syncthreads();
     PairCounters pc;
     unsigned long long n_tested = 0;
+    // Warps walk the task sequence independently: task t sits in slot t % kSlots; the last warp to
+    // release a slot refills it with the next task, so a warp may run up to kSlots - 1 tasks ahead of
+    // the slowest one instead of meeting it at a CTA barrier after every task.
     for (int t = 0;; ++t) {
-        __syncthreads();
-        const int slot = t & 1;
-        const TaskInfo ti = tinfo[slot];
-        if (!ti.valid || abort_flag) break;
-        if (tid == 0) {
-            TaskInfo nx;
-            if (next_task(gen, p, cstart, ccount, cflag, work, nx)) {
-                trj_mbar_arrive_expect_tx(&bars[slot ^ 1], nx.jcount * 16u);
-                trj_bulk_g2s(buf + (slot ^ 1) * kJChunk, sorted + nx.sb, nx.jcount * 16u, &bars[slot ^ 1]);
-                issued[slot ^ 1] += 1;
+        const int slot = t % kSlots;
+        if (__shfl_sync(0xffffffffu, *(volatile int*)&abort_flag, 0)) break;  // warp-uniform
+        // Warp-uniform outcome: the task loop below uses full-warp ballots.
+        if (!__all_sync(0xffffffffu, trj_mbar_wait(&bars[slot], (unsigned)(t / kSlots) & 1u))) {
+            if (lane == 0) {
+                trj_raise(status, TRJ_DEV_TIMEOUT);
+                *(volatile int*)&abort_flag = 1;
             }
-            tinfo[slot ^ 1] = nx;
+            break;
         }
-        // home atoms of this task (loaded before the wait to overlap the copy)
-        const int il0 = ti.hc * kHomeChunk + tid, il1 = il0 + kThreads;
+        const TaskInfo ti = tinfo[slot];
+        if (!ti.valid) break;
+        const int il0 = ti.hc * kHomeChunk + 64 * warp + (int)lane, il1 = il0 + 32;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 a0 = il0 < ti.na ? sorted[ti.sa + il0] : z4;
         const float4 a1 = il1 < ti.na ? sorted[ti.sa + il1] : z4;
@@ -308,34 +402,34 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
         const bool h0 = il0 < ti.na && (unsigned)s0 < (unsigned)p.nsp;
         const bool h1 = il1 < ti.na && (unsigned)s1 < (unsigned)p.nsp;
-        float qa0 = 0.f, qa1 = 0.f;
-        if (QMODE) {
-            qa0 = il0 < ti.na ? sorted_q[ti.sa + il0] : 0.f;
-            qa1 = il1 < ti.na ? sorted_q[ti.sa + il1] : 0.f;
-        }
+        const float qa0 = (QMODE && il0 < ti.na) ? sorted_q[ti.sa + il0] : 0.f;
+        const float qa1 = (QMODE && il1 < ti.na) ? sorted_q[ti.sa + il1] : 0.f;
         const float* qj = QMODE ? sorted_q + ti.sb : nullptr;
-        if (!trj_mbar_wait(&bars[slot], (t >> 1) & 1)) {
-            trj_raise(status, TRJ_DEV_TIMEOUT);
-            abort_flag = 1;
-            continue;  // the barrier at the loop head sees the flag
-        }
         const float4* bj = buf + slot * kJChunk;
-        if (ti.self) {
-            n_tested += (unsigned long long)(h0 ? max(0, ti.jcount - max(0, il0 + 1 - ti.jlocal0)) : 0);
-            n_tested += (unsigned long long)(h1 ? max(0, ti.jcount - max(0, il1 + 1 - ti.jlocal0)) : 0);
-        } else {
-            n_tested += (unsigned long long)((h0 ? ti.jcount : 0) + (h1 ? ti.jcount : 0));
-        }
+        WarpBox* wb = &wboxes[warp];
         if (ti.fast)
-            run_task<true, QMODE>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc, myq, qa0, qa1, qj);
+            n_tested += run_task<true, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
+                                              qa0, qa1, qj, wb);
         else
-            run_task<false, QMODE>(ti, bj, a0, a1, h0, h1, il0, il1, s0, s1, p, rowtab, myhist, pc, myq, qa0, qa1,
-                                   qj);
+            n_tested += run_task<false, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
+                                               qa0, qa1, qj, wb);
+        // Release the slot; the last warp refills it.
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&released[slot], 1u) == kThreads / 32 - 1) {
+                released[slot] = 0u;
+                __threadfence_block();
+                refill_slot(slot, gen, p, cstart, ccount, cflag, work, sorted, tinfo, bars, phases, buf);
+            }
+        }
+        __syncwarp();
     }
+    __syncthreads();
     if (tid == 0 && abort_flag) {
         // Let copies still in flight land before the CTA exits (bounded).
-        for (int sl = 0; sl < 2; ++sl)
-            if (issued[sl]) trj_mbar_wait(&bars[sl], (issued[sl] - 1) & 1);
+        for (int sl = 0; sl < kSlots; ++sl)
+            if (phases[sl]) trj_mbar_wait(&bars[sl], (phases[sl] - 1) & 1);
     }
     __syncthreads();
     // Merge replicas into the global uint64 histogram (their total is the counted pairs).
@@ -369,10 +463,13 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
     }
 }
 
-// Cell of each atom from its wrapped coordinate; per-cell counts and slots.
+// Cell of each atom from its wrapped coordinate, and its sub-cell: the cell is split into
+// 2^sbits parts per axis and the parts are numbered along a Morton curve (bits interleaved x, y, z
+// from the lowest), so atoms sorted by key = cell * 8^sbits + sub-cell are cell-contiguous and
+// spatially ordered inside each cell.  Per-key counts and slots.
 __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n, float Lx, float Ly,
-                                   float Lz, int ncx, int ncy, int ncz, int32_t* __restrict__ ccount,
-                                   int32_t* __restrict__ cflag, int32_t* __restrict__ acell,
+                                   float Lz, int ncx, int ncy, int ncz, int sbits, int32_t* __restrict__ fcount,
+                                   int32_t* __restrict__ cflag, int32_t* __restrict__ akey,
                                    int32_t* __restrict__ aslot) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -380,29 +477,48 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     float L[3] = {Lx, Ly, Lz};
     int nc[3] = {ncx, ncy, ncz};
     float r[3] = {v.x, v.y, v.z};
-    int k[3];
+    int k[3], sub[3];
+    const int S = 1 << sbits;
     bool outside = false;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         outside |= !(r[d] >= 0.0f && r[d] < L[d]);
         float w = r[d] - L[d] * floorf(r[d] / L[d]);
-        int c = (int)(w * ((float)nc[d] / L[d]));
+        float t = w * ((float)nc[d] / L[d]);
+        int c = (int)t;
         c = c < 0 ? 0 : (c >= nc[d] ? nc[d] - 1 : c);
         k[d] = c;
+        int sc = (int)((t - (float)c) * (float)S);
+        sub[d] = sc < 0 ? 0 : (sc >= S ? S - 1 : sc);  // also catches NaN coordinates (sc = 0)
     }
+    int m = 0;
+    for (int b = 0; b < sbits; ++b)
+        m |= (((sub[0] >> b) & 1) << (3 * b)) | (((sub[1] >> b) & 1) << (3 * b + 1)) |
+             (((sub[2] >> b) & 1) << (3 * b + 2));
     int c = (k[0] * ncy + k[1]) * ncz + k[2];
-    acell[i] = c;
-    aslot[i] = atomicAdd(&ccount[c], 1);
+    const int key = (c << (3 * sbits)) | m;
+    akey[i] = key;
+    aslot[i] = atomicAdd(&fcount[key], 1);
     if (outside) cflag[c] = 1;
 }
 
+// Cell start and count from the exclusive scan of the per-key counts.
+__global__ void cell_ranges_kernel(const int32_t* __restrict__ fstart, int ncell, int sbits,
+                                   int32_t* __restrict__ cstart, int32_t* __restrict__ ccount) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > ncell) return;
+    const int a = fstart[c << (3 * sbits)];
+    cstart[c] = a;
+    if (c < ncell) ccount[c] = fstart[(c + 1) << (3 * sbits)] - a;
+}
+
 __global__ void cell_scatter_kernel(const float4* __restrict__ packed, int64_t n,
-                                    const int32_t* __restrict__ acell, const int32_t* __restrict__ aslot,
-                                    const int32_t* __restrict__ cstart, float4* __restrict__ sorted,
+                                    const int32_t* __restrict__ akey, const int32_t* __restrict__ aslot,
+                                    const int32_t* __restrict__ fstart, float4* __restrict__ sorted,
                                     const float* __restrict__ q, float* __restrict__ sorted_q) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int64_t d = cstart[acell[i]] + aslot[i];
+    const int64_t d = fstart[akey[i]] + aslot[i];
     sorted[d] = packed[i];
     if (q) sorted_q[d] = q[i];
 }
@@ -538,7 +654,10 @@ struct trj_rdf_plan {
     int32_t* cflag = nullptr;   // ncell_cap: cell holds a coordinate outside [0, L)
     unsigned long long* work = nullptr;  // item counter of the pair kernel
     int32_t* cstart = nullptr;  // ncell_cap + 1
-    int32_t* acell = nullptr;   // n_max
+    int64_t fine_cap = 0;       // capacity of the per-(cell, sub-cell) arrays
+    int32_t* fcount = nullptr;  // fine_cap
+    int32_t* fstart = nullptr;  // fine_cap + 1
+    int32_t* akey = nullptr;    // n_max: (cell, sub-cell) key per atom
     int32_t* aslot = nullptr;   // n_max
     float4* sorted = nullptr;   // n_max
     float* sorted_q = nullptr;  // n_max charges in cell order (first charged call)
@@ -598,7 +717,7 @@ static int rdf_plan_create_impl(trj_ctx* ctx, int nsp, float deltar, float rcrdf
     p->lsmax = nint_host(rc / deltar) + 1;
     p->n_max = n_max;
     size_t hist_bytes = (size_t)p->nit * p->lsmax * 4;
-    size_t budget = ctx->smem_optin - 2 * kJChunk * sizeof(float4) - 4096;
+    size_t budget = ctx->smem_optin - kSlots * kJChunk * sizeof(float4) - 4096;
     if (hist_bytes > budget) {
         delete p;
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED,
@@ -610,7 +729,10 @@ static int rdf_plan_create_impl(trj_ctx* ctx, int nsp, float deltar, float rcrdf
     // Room for a box up to 25% smaller per axis (more cells) without re-planning.
     p->ncell_cap = std::max(ncell * 2 + 64, 64);
     trj_device_guard g(ctx->device);
+    // Sub-cell keys: up to 64 per cell, never more entries than atoms (or cells).
+    p->fine_cap = std::max<int64_t>(p->ncell_cap, std::min<int64_t>((int64_t)p->ncell_cap * 64, n_max));
     size_t bytes = 64 + sizeof(int32_t) * (size_t)(3 * p->ncell_cap + 1) +
+                   sizeof(int32_t) * (size_t)(2 * p->fine_cap + 1) +
                    (sizeof(int32_t) * 2 + sizeof(float4)) * (size_t)std::max<int64_t>(n_max, 1);
     char* base = nullptr;
     if (trj_dev_alloc(ctx, (void**)&base, bytes + 256) != cudaSuccess) {
@@ -618,13 +740,15 @@ static int rdf_plan_create_impl(trj_ctx* ctx, int nsp, float deltar, float rcrdf
         return trj_fail(ctx, TRJ_ERR_NOMEM, "rdf plan: %zu bytes of scratch", bytes);
     }
     p->sorted = reinterpret_cast<float4*>(base);
-    p->acell = reinterpret_cast<int32_t*>(p->sorted + std::max<int64_t>(n_max, 1));
-    p->aslot = p->acell + std::max<int64_t>(n_max, 1);
+    p->akey = reinterpret_cast<int32_t*>(p->sorted + std::max<int64_t>(n_max, 1));
+    p->aslot = p->akey + std::max<int64_t>(n_max, 1);
     p->ccount = p->aslot + std::max<int64_t>(n_max, 1);
     p->cstart = p->ccount + p->ncell_cap;
     p->cflag = p->cstart + p->ncell_cap + 1;
+    p->fcount = p->cflag + p->ncell_cap;
+    p->fstart = p->fcount + p->fine_cap;
     p->work = reinterpret_cast<unsigned long long*>(
-        (reinterpret_cast<uintptr_t>(p->cflag + p->ncell_cap) + 15) & ~(uintptr_t)15);
+        (reinterpret_cast<uintptr_t>(p->fstart + p->fine_cap + 1) + 15) & ~(uintptr_t)15);
     p->scratch_bytes = (int64_t)bytes;
     *out = p;
     return TRJ_OK;
@@ -781,6 +905,11 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     P.hsplit = std::max(1, (int)ceil(avg / kHomeChunk));
     // No minimum image needed away from the wrap (2D: z differences are 0, z is never wrapped).
     P.fast_ok = P.nc[0] >= 5 && P.nc[1] >= 5 && (P.nc[2] >= 5 || plan->dim == 2);
+    // Cull radius 2^-10 above the cutoff (the exact test needs rr2 < side2*(1 + 2^-20)); the pad,
+    // 2^-16 of the largest edge, exceeds the rounding of the box and gap arithmetic (a few ulps of
+    // coordinates below 2L).
+    P.cull2 = (float)((double)plan->side2 * (1.0 + 1.0 / 1024.0) * (1.0 + 1.0 / 1024.0));
+    P.cull_pad = (float)((double)std::max(box[0], std::max(box[1], box[2])) / 65536.0);
     // Split neighbour ranges when there are too few (cell, offset, home chunk) items to fill the GPU.
     int64_t base_items = (int64_t)P.ncell * P.noff * P.hsplit;
     int64_t want = (int64_t)ctx->sm_count * 4;
@@ -789,14 +918,14 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
 
     // Shared memory: two staging buffers + histogram replicas (+ FP64 charge replicas).
     size_t hist_bytes = (size_t)P.nit * P.lsmax * 4 + (charged ? (size_t)P.lsmax * 8 + 8 : 0);
-    size_t stage = 2 * kJChunk * sizeof(float4);
+    size_t stage = kSlots * kJChunk * sizeof(float4);
     size_t optin = ctx->smem_optin;
     // Most CTAs per SM (up to 4, i.e. 32 warps) that still hold >= 2 histogram replicas each;
     // a single CTA per SM otherwise.
     const size_t sm_smem = optin + 1024;  // per-SM shared memory (the opt-in limit plus the driver's block reserve)
     int ctas_per_sm = 1, nrep = 0;
     for (int k = 4; k >= 2; --k) {
-        size_t per_cta = sm_smem / k - 1024 - 1280;  // driver reserve + static shared memory
+        size_t per_cta = sm_smem / k - 1024 - 2048;  // driver reserve + static shared memory
         int r = per_cta > stage ? (int)std::min<size_t>(8, (per_cta - stage) / hist_bytes) : 0;
         if (r >= 2) {
             ctas_per_sm = k;
@@ -811,15 +940,25 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(charged ? rdf_pairs_kernel<true> : rdf_pairs_kernel<false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
+    // Sub-cells per cell axis: 4 (64 per cell) from 128 atoms per cell on, 2 from 16 on, within the
+    // key capacity.
+    const double per_cell = (double)n / P.ncell;
+    int sbits = per_cell >= 128.0 ? 2 : (per_cell >= 16.0 ? 1 : 0);
+    while (sbits > 0 && ((int64_t)P.ncell << (3 * sbits)) > plan->fine_cap) --sbits;
+    const int nkey = P.ncell << (3 * sbits);
+
     // Cell binning: count, scan, scatter.
-    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->ccount, 0, sizeof(int32_t) * P.ncell, s));
+    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->fcount, 0, sizeof(int32_t) * nkey, s));
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->cflag, 0, sizeof(int32_t) * P.ncell, s));
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->work, 0, sizeof(unsigned long long), s));
     unsigned nb = (unsigned)((n + 255) / 256);
     cell_assign_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, box[0], box[1], box[2], P.nc[0],
-                                          P.nc[1], P.nc[2], plan->ccount, plan->cflag, plan->acell, plan->aslot);
-    scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->ccount, plan->cstart, P.ncell);
-    cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->acell, plan->aslot, plan->cstart,
+                                          P.nc[1], P.nc[2], sbits, plan->fcount, plan->cflag, plan->akey,
+                                          plan->aslot);
+    scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->fcount, plan->fstart, nkey);
+    cell_ranges_kernel<<<(unsigned)((P.ncell + 256) / 256), 256, 0, s>>>(plan->fstart, P.ncell, sbits, plan->cstart,
+                                                                        plan->ccount);
+    cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->akey, plan->aslot, plan->fstart,
                                            plan->sorted, charged ? charge_dev : nullptr, plan->sorted_q);
     if (charged) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
     int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
@@ -834,7 +973,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
             (unsigned long long*)edge_dev, ctx->status_dev, nullptr, nullptr);
     plan->timer.end(ctx, s);
     plan->cells_valid = 1;
-    ctx->launches += 4;
+    ctx->launches += 5;
     if (charged) {
         gqq_finish_kernel<<<1, 1024, 0, s>>>(charge_dev, n, plan->gqq_frame, plan->lsmax, gqq_dev);
         ctx->launches += 1;
