@@ -188,20 +188,26 @@ __device__ __noinline__ int exact_bin(float rr2, float x2, float dy, float dz, c
 
 // QMODE: also adds the charge product q_a*q_b of every counted pair to the bin (FP64; the product
 // of two FP32 charges is exact in FP64).  rdf.cuf:469-472.
-template <bool QMODE>
+// FLOOR: bins floor(r/deltar)+1 (rdfxy) instead of nint(r/deltar).
+template <bool FLOOR, bool QMODE>
 __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz, int row, const RdfParams& p,
                                          unsigned* myhist, PairCounters& pc, double* myq, float qa,
                                          const float* qbp) {
     const float q = rr2 * rsqrtf(rr2) * p.inv_deltar;
-    const float fq = q - floorf(q);
+    // Nearest integer of q by adding and removing 1.5*2^23 (q < 2^22): qb holds it in its low
+    // mantissa bits; d = q - r in [-1/2, 1/2] exactly.
+    const float qb = __fadd_rn(q, 12582912.0f);
+    const float d = __fsub_rn(q, __fsub_rn(qb, 12582912.0f));
     const float win = fmaf(q, 1.9073486e-6f, 9.5367432e-7f);  // q*2^-19 + 2^-20
-    // distance of q from the nearest bin edge: half-integers (nint bins) or integers (floor bins)
-    const float edge = p.floor_bins ? fminf(fq, 1.0f - fq) : fabsf(fq - 0.5f);
+    // distance of q from the nearest bin edge: integers (floor bins) or half-integers (nint bins)
+    const float edge = FLOOR ? fabsf(d) : 0.5f - fabsf(d);
     int ind;
     if (rr2 >= p.side2_lo || !(edge > win)) {  // NaN (rr2 == 0) takes this path too
         ind = exact_bin(rr2, x2, dy, dz, p, pc);
     } else {
-        ind = p.floor_bins ? (int)floorf(q) + 1 : __float2int_rn(q);
+        // Away from an edge, round-to-nearest-even and NINT agree, and floor(q) = r - (d < 0).
+        const int r = __float_as_int(qb) - 0x4B400000;
+        ind = FLOOR ? r + (d > 0.f ? 1 : 0) : r;
         if (ind > p.lsmax) ind = 0;
     }
     if (ind > 0) {
@@ -210,7 +216,7 @@ __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz
     }
 }
 
-template <bool FAST, bool QMODE>
+template <bool FAST, bool FLOOR, bool QMODE>
 __device__ __forceinline__ void pair(const float4& a, const float4& b, bool valid, int si, const RdfParams& p,
                                      const int* rowtab, unsigned* myhist, PairCounters& pc, double* myq,
                                      float qa, const float* qbp) {
@@ -227,7 +233,7 @@ __device__ __forceinline__ void pair(const float4& a, const float4& b, bool vali
     if (valid && rr2 < p.side2_hi) {
         const int sj = __float_as_int(b.w);
         if ((unsigned)sj < (unsigned)p.nsp)
-            bin_pair<QMODE>(rr2, x2, dy, dz, rowtab[si * p.nsp + sj], p, myhist, pc, myq, qa, qbp);
+            bin_pair<FLOOR, QMODE>(rr2, x2, dy, dz, rowtab[si * p.nsp + sj], p, myhist, pc, myq, qa, qbp);
     }
 }
 
@@ -260,7 +266,7 @@ __device__ __forceinline__ bool maybe_near(const float4& b, const float4& c, con
 // One task for one warp: its 64 home atoms (a0 = atom il0, a1 = atom il0 + 32 per lane) against the
 // staged neighbour chunk.  Blocks of 32 neighbours are culled against the warp's box (kept in shared
 // memory, `wb`) with one ballot; the survivors are tested exactly.  Returns the candidate pairs tested.
-template <bool FAST, bool QMODE>
+template <bool FAST, bool FLOOR, bool QMODE>
 __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
                                              const float4& a1, bool h0, bool h1, int il0, int s0, int s1,
                                              unsigned lane, const RdfParams& p, const int* rowtab, unsigned* myhist,
@@ -295,8 +301,8 @@ __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* _
             const float4 b0 = bj[j0];
             const bool v0 = h0 && j0 > lim0;
             const bool v1 = h1 && j0 > lim1;
-            pair<FAST, QMODE>(a0, b0, v0, s0, p, rowtab, myhist, pc, myq, qa0, qj + j0);
-            pair<FAST, QMODE>(a1, b0, v1, s1, p, rowtab, myhist, pc, myq, qa1, qj + j0);
+            pair<FAST, FLOOR, QMODE>(a0, b0, v0, s0, p, rowtab, myhist, pc, myq, qa0, qj + j0);
+            pair<FAST, FLOOR, QMODE>(a1, b0, v1, s1, p, rowtab, myhist, pc, myq, qa1, qj + j0);
             tested += (unsigned)v0 + (unsigned)v1;
         }
     }
@@ -328,7 +334,7 @@ __device__ __forceinline__ void refill_slot(int slot, TaskGen& gen, const RdfPar
 // QMODE: sorted_q holds the charges in cell order and gqq_frame (lsmax doubles) receives this
 // frame's sum of q_a*q_b per bin; each warp's charge replica (lsmax doubles) follows the count
 // replicas in shared memory.
-template <bool QMODE>
+template <bool FLOOR, bool QMODE>
 __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
                                                              const int32_t* __restrict__ cstart,
                                                              const int32_t* __restrict__ ccount,
@@ -408,10 +414,10 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         const float4* bj = buf + slot * kJChunk;
         WarpBox* wb = &wboxes[warp];
         if (ti.fast)
-            n_tested += run_task<true, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
+            n_tested += run_task<true, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
                                               qa0, qa1, qj, wb);
         else
-            n_tested += run_task<false, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
+            n_tested += run_task<false, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
                                                qa0, qa1, qj, wb);
         // Release the slot; the last warp refills it.
         __syncwarp();
@@ -937,8 +943,11 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     if (nrep < 1) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf accumulate: histogram too large");
     P.nrep = nrep;
     size_t smem = stage + (size_t)nrep * hist_bytes;
-    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(charged ? rdf_pairs_kernel<true> : rdf_pairs_kernel<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void (*kern)(RdfParams, const float4*, const int32_t*, const int32_t*, const int32_t*, unsigned long long*,
+                 unsigned long long*, unsigned long long*, unsigned*, const float*, double*) =
+        plan->floor_bins ? (charged ? rdf_pairs_kernel<true, true> : rdf_pairs_kernel<true, false>)
+                         : (charged ? rdf_pairs_kernel<false, true> : rdf_pairs_kernel<false, false>);
+    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     // Sub-cells per cell axis: 4 (64 per cell) from 128 atoms per cell on, 2 from 16 on, within the
     // key capacity.
@@ -963,14 +972,10 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     if (charged) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
     int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
     plan->timer.begin(ctx, s);
-    if (charged)
-        rdf_pairs_kernel<true><<<(unsigned)grid, kThreads, smem, s>>>(
-            P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work, (unsigned long long*)hist_dev,
-            (unsigned long long*)edge_dev, ctx->status_dev, plan->sorted_q, plan->gqq_frame);
-    else
-        rdf_pairs_kernel<false><<<(unsigned)grid, kThreads, smem, s>>>(
-            P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work, (unsigned long long*)hist_dev,
-            (unsigned long long*)edge_dev, ctx->status_dev, nullptr, nullptr);
+    kern<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work,
+                                                (unsigned long long*)hist_dev, (unsigned long long*)edge_dev,
+                                                ctx->status_dev, charged ? plan->sorted_q : nullptr,
+                                                charged ? plan->gqq_frame : nullptr);
     plan->timer.end(ctx, s);
     plan->cells_valid = 1;
     ctx->launches += 5;
