@@ -472,11 +472,11 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
 // Cell of each atom from its wrapped coordinate, and its sub-cell: the cell is split into
 // 2^sbits parts per axis and the parts are numbered along a Morton curve (bits interleaved x, y, z
 // from the lowest), so atoms sorted by key = cell * 8^sbits + sub-cell are cell-contiguous and
-// spatially ordered inside each cell.  Per-key counts and slots.
+// spatially ordered inside each cell.  Per-key and per-cell counts, per-key slots.
 __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n, float Lx, float Ly,
                                    float Lz, int ncx, int ncy, int ncz, int sbits, int32_t* __restrict__ fcount,
-                                   int32_t* __restrict__ cflag, int32_t* __restrict__ akey,
-                                   int32_t* __restrict__ aslot) {
+                                   int32_t* __restrict__ ccount, int32_t* __restrict__ cflag,
+                                   int32_t* __restrict__ akey, int32_t* __restrict__ aslot) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 v = packed[i];
@@ -505,17 +505,32 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     const int key = (c << (3 * sbits)) | m;
     akey[i] = key;
     aslot[i] = atomicAdd(&fcount[key], 1);
+    atomicAdd(&ccount[c], 1);
     if (outside) cflag[c] = 1;
 }
 
-// Cell start and count from the exclusive scan of the per-key counts.
-__global__ void cell_ranges_kernel(const int32_t* __restrict__ fstart, int ncell, int sbits,
-                                   int32_t* __restrict__ cstart, int32_t* __restrict__ ccount) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > ncell) return;
-    const int a = fstart[c << (3 * sbits)];
-    cstart[c] = a;
-    if (c < ncell) ccount[c] = fstart[(c + 1) << (3 * sbits)] - a;
+// Start of every (cell, sub-cell) key: the cell's start plus the exclusive prefix of its sub-cell
+// counts.  One warp per cell.
+__global__ void sub_offsets_kernel(const int32_t* __restrict__ fcount, const int32_t* __restrict__ cstart, int ncell,
+                                   int sbits, int32_t* __restrict__ fstart) {
+    const int c = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const unsigned lane = threadIdx.x & 31u;
+    if (c >= ncell) return;
+    const int nsub = 1 << (3 * sbits);
+    const int64_t base = (int64_t)c << (3 * sbits);
+    int carry = cstart[c];
+    for (int s0 = 0; s0 < nsub; s0 += 32) {
+        const int s = s0 + (int)lane;
+        const int v = s < nsub ? fcount[base + s] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if ((int)lane >= o) x += y;
+        }
+        if (s < nsub) fstart[base + s] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
 }
 
 __global__ void cell_scatter_kernel(const float4* __restrict__ packed, int64_t n,
@@ -956,17 +971,18 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     while (sbits > 0 && ((int64_t)P.ncell << (3 * sbits)) > plan->fine_cap) --sbits;
     const int nkey = P.ncell << (3 * sbits);
 
-    // Cell binning: count, scan, scatter.
+    // Cell binning: count, scan over cells, sub-cell offsets, scatter.
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->fcount, 0, sizeof(int32_t) * nkey, s));
+    TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->ccount, 0, sizeof(int32_t) * P.ncell, s));
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->cflag, 0, sizeof(int32_t) * P.ncell, s));
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->work, 0, sizeof(unsigned long long), s));
     unsigned nb = (unsigned)((n + 255) / 256);
     cell_assign_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, box[0], box[1], box[2], P.nc[0],
-                                          P.nc[1], P.nc[2], sbits, plan->fcount, plan->cflag, plan->akey,
-                                          plan->aslot);
-    scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->fcount, plan->fstart, nkey);
-    cell_ranges_kernel<<<(unsigned)((P.ncell + 256) / 256), 256, 0, s>>>(plan->fstart, P.ncell, sbits, plan->cstart,
-                                                                        plan->ccount);
+                                          P.nc[1], P.nc[2], sbits, plan->fcount, plan->ccount, plan->cflag,
+                                          plan->akey, plan->aslot);
+    scan_exclusive_kernel<<<1, 1024, 0, s>>>(plan->ccount, plan->cstart, P.ncell);
+    sub_offsets_kernel<<<(unsigned)((P.ncell + 7) / 8), 256, 0, s>>>(plan->fcount, plan->cstart, P.ncell, sbits,
+                                                                    plan->fstart);
     cell_scatter_kernel<<<nb, 256, 0, s>>>((const float4*)packed_dev, n, plan->akey, plan->aslot, plan->fstart,
                                            plan->sorted, charged ? charge_dev : nullptr, plan->sorted_q);
     if (charged) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
