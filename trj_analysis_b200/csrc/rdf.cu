@@ -83,12 +83,13 @@ __device__ __forceinline__ float min_image(float d, float L, float t0, float t1,
     return min_image_exact(d, L);
 }
 
-__device__ __forceinline__ int outcome(float rr2, const RdfParams& p) {
-    if (!(rr2 < p.side2)) return 0;
+// Bin of a pair by the reference's arithmetic (0: not counted).
+__device__ __forceinline__ int outcome(float rr2, float side2, float deltar, int lsmax, int floor_bins) {
+    if (!(rr2 < side2)) return 0;
     float rr = __fsqrt_rn(rr2);
-    float q = __fdiv_rn(rr, p.deltar);
-    int ind = p.floor_bins ? (int)floorf(q) + 1 : (int)roundf(q);
-    return (ind <= p.lsmax && ind > 0) ? ind : 0;
+    float q = __fdiv_rn(rr, deltar);
+    int ind = floor_bins ? (int)floorf(q) + 1 : (int)roundf(q);
+    return (ind <= lsmax && ind > 0) ? ind : 0;
 }
 
 // Task iterator run by thread 0: items are taken from a global counter (dynamic balance);
@@ -171,19 +172,17 @@ struct PairCounters {
     unsigned long long ulp = 0, fma = 0, counted = 0;
 };
 
-// Bin of one candidate pair (rr2 < side2_hi): approximate bin from rsqrt, exact reference
-// arithmetic (and edge statistics) whenever the approximation is within a window of a bin edge
-// or of the cutoff, so the result always equals outcome(rr2).
-// Exact reference outcome of a pair near a bin edge or the cutoff, with its edge statistics.
-__device__ __noinline__ int exact_bin(float rr2, float x2, float dy, float dz, const RdfParams& p,
-                                      PairCounters& pc) {
-    const int ind = outcome(rr2, p);
-    const int olo = outcome(nextafterf(rr2, -INFINITY), p);
-    const int ohi = outcome(nextafterf(rr2, INFINITY), p);
-    pc.ulp += (olo != ind || ohi != ind);
+// Exact reference outcome of a pair near a bin edge or the cutoff, with its edge statistics:
+// returns the bin | 2^29 if a one-ulp change of rr2 changes it | 2^30 if the FMA-contracted rr2
+// does.  Scalars by value: nothing of the caller's needs an address (no local-memory copies).
+__device__ __noinline__ int exact_bin(float rr2, float x2, float dy, float dz, float side2, float deltar, int lsmax,
+                                      int floor_bins) {
+    const int ind = outcome(rr2, side2, deltar, lsmax, floor_bins);
+    const int olo = outcome(nextafterf(rr2, -INFINITY), side2, deltar, lsmax, floor_bins);
+    const int ohi = outcome(nextafterf(rr2, INFINITY), side2, deltar, lsmax, floor_bins);
     const float rr2f = fmaf(dz, dz, fmaf(dy, dy, x2));
-    pc.fma += (outcome(rr2f, p) != ind);
-    return ind;
+    const int fma = outcome(rr2f, side2, deltar, lsmax, floor_bins) != ind;
+    return ind | ((olo != ind || ohi != ind) ? (1 << 29) : 0) | (fma ? (1 << 30) : 0);
 }
 
 // QMODE: also adds the charge product q_a*q_b of every counted pair to the bin (FP64; the product
@@ -203,7 +202,10 @@ __device__ __forceinline__ void bin_pair(float rr2, float x2, float dy, float dz
     const float edge = FLOOR ? fabsf(d) : 0.5f - fabsf(d);
     int ind;
     if (rr2 >= p.side2_lo || !(edge > win)) {  // NaN (rr2 == 0) takes this path too
-        ind = exact_bin(rr2, x2, dy, dz, p, pc);
+        const int e = exact_bin(rr2, x2, dy, dz, p.side2, p.deltar, p.lsmax, p.floor_bins);
+        pc.ulp += (e >> 29) & 1;
+        pc.fma += (e >> 30) & 1;
+        ind = e & ((1 << 29) - 1);
     } else {
         // Away from an edge, round-to-nearest-even and NINT agree, and floor(q) = r - (d < 0).
         const int r = __float_as_int(qb) - 0x4B400000;
@@ -266,7 +268,14 @@ __device__ __forceinline__ bool maybe_near(const float4& b, const float4& c, con
 // One task for one warp: its 64 home atoms (a0 = atom il0, a1 = atom il0 + 32 per lane) against the
 // staged neighbour chunk.  Blocks of 32 neighbours are culled against the warp's box (kept in shared
 // memory, `wb`) with one ballot; the survivors are tested exactly.  Returns the candidate pairs tested.
-template <bool FAST, bool FLOOR, bool QMODE>
+// Lanes whose bit index k has jj0 + k > lim: the neighbours of a block that pair with a home.
+__device__ __forceinline__ unsigned after_mask(int lim, int jj0) {
+    const int s = lim - jj0;
+    return s < 0 ? 0xffffffffu : (s >= 31 ? 0u : (0xffffffffu << (s + 1)));
+}
+
+// SELF: home and neighbour cell are the same cell (pairs need j > i within it).
+template <bool FAST, bool SELF, bool FLOOR, bool QMODE>
 __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
                                              const float4& a1, bool h0, bool h1, int il0, int s0, int s1,
                                              unsigned lane, const RdfParams& p, const int* rowtab, unsigned* myhist,
@@ -285,25 +294,28 @@ __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* _
         }
         __syncwarp();
     }
-    const int jbeg = ti.self ? max(0, il0w + 1 - ti.jlocal0) : 0;
-    const int lim0 = ti.self ? il0 - ti.jlocal0 : -1;  // a0 pairs need jj > lim0
-    const int lim1 = ti.self ? lim0 + 32 : -1;           // a1 pairs need jj > lim1
+    const int jbeg = SELF ? max(0, il0w + 1 - ti.jlocal0) : 0;
+    const int lim0 = SELF ? il0 - ti.jlocal0 : -1;  // a0 pairs need jj > lim0
+    const int lim1 = SELF ? lim0 + 32 : -1;         // a1 pairs need jj > lim1
     unsigned tested = 0;
     for (int jj0 = jbeg; jj0 < ti.jcount; jj0 += 32) {
         const int jl = jj0 + (int)lane;
         bool keep = jl < ti.jcount;
         if (ti.cull && keep) keep = maybe_near(bj[jl], wb->c, wb->h, p.cull2);
         unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (SELF)
+            tested += (h0 ? __popc(m & after_mask(lim0, jj0)) : 0) + (h1 ? __popc(m & after_mask(lim1, jj0)) : 0);
+        else
+            tested += __popc(m) * ((unsigned)h0 + (unsigned)h1);
         while (m) {
             const int k0 = __ffs(m) - 1;
             m &= m - 1u;
             const int j0 = jj0 + k0;
             const float4 b0 = bj[j0];
-            const bool v0 = h0 && j0 > lim0;
-            const bool v1 = h1 && j0 > lim1;
-            pair<FAST, FLOOR, QMODE>(a0, b0, v0, s0, p, rowtab, myhist, pc, myq, qa0, qj + j0);
-            pair<FAST, FLOOR, QMODE>(a1, b0, v1, s1, p, rowtab, myhist, pc, myq, qa1, qj + j0);
-            tested += (unsigned)v0 + (unsigned)v1;
+            pair<FAST, FLOOR, QMODE>(a0, b0, SELF ? (h0 && j0 > lim0) : h0, s0, p, rowtab, myhist, pc, myq, qa0,
+                                     qj + j0);
+            pair<FAST, FLOOR, QMODE>(a1, b0, SELF ? (h1 && j0 > lim1) : h1, s1, p, rowtab, myhist, pc, myq, qa1,
+                                     qj + j0);
         }
     }
     return tested;
@@ -413,12 +425,14 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         const float* qj = QMODE ? sorted_q + ti.sb : nullptr;
         const float4* bj = buf + slot * kJChunk;
         WarpBox* wb = &wboxes[warp];
+#define TRJ_RUN(F, S)                                                                                       \
+    run_task<F, S, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq, qa0, qa1, qj, \
+                                 wb)
         if (ti.fast)
-            n_tested += run_task<true, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
-                                              qa0, qa1, qj, wb);
+            n_tested += ti.self ? TRJ_RUN(true, true) : TRJ_RUN(true, false);
         else
-            n_tested += run_task<false, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq,
-                                               qa0, qa1, qj, wb);
+            n_tested += ti.self ? TRJ_RUN(false, true) : TRJ_RUN(false, false);
+#undef TRJ_RUN
         // Release the slot; the last warp refills it.
         __syncwarp();
         if (lane == 0) {
