@@ -11,7 +11,8 @@
 //
 // Operands: A is built by the producer warps straight into tensor memory (the tcgen05.mma form
 // with A in TMEM), in two alternating half-stage buffers of 16 atoms, so shared-memory bandwidth
-// goes to the B operand only.  B (the split Z factors) is a per-frame table read with 2-D TMA loads
+// goes to the B operand only.  B (the split Z factors) is a per-frame table, blocked by 32-atom stage
+// ([stage][row][32 atoms x (re, im)], so one stage's rows are contiguous), read with 2-D TMA loads
 // (128-byte swizzle, no multicast) through a ring of 32-atom stages; each stage also carries the
 // atoms' x/y phases, from which the producers evaluate the X and Y factors of the tile in shared
 // memory before forming the products.  Tiles are up to 224 columns wide: one tcgen05.mma costs at
@@ -96,6 +97,7 @@ struct TcParams {
     int flush_stages;
     int stage_bytes;
     int bmax;  // B rows of a stage buffer
+    int table_rows;  // Z-table rows per 32-slot block
     unsigned* status;
 };
 
@@ -123,6 +125,7 @@ struct Tc2Params {
     int flush_stages;
     int stage_bytes;
     int bhalf;  // B rows per CTA of a stage buffer
+    int table_rows;  // Z-table rows per 32-slot block
     unsigned* status;
 };
 
@@ -304,7 +307,7 @@ __device__ __forceinline__ bool slot_atom(int64_t slot, const int64_t* pad_off, 
 // x/y phase fractions of every slot (zero for padding slots, whose Z rows are zero).
 __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
                                  const int64_t* __restrict__ pad_off, int nsp, int64_t total_slots, int nz_min,
-                                 int nz_count, int64_t kdim, __nv_bfloat16* __restrict__ tab_hi,
+                                 int nz_count, int64_t table_rows, __nv_bfloat16* __restrict__ tab_hi,
                                  __nv_bfloat16* __restrict__ tab_lo, uint2* __restrict__ uxy, int64_t qbase) {
     int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= total_slots) return;
@@ -325,8 +328,9 @@ __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t*
             split2(z.x, -z.y, h0, l0);
             split2(z.y, z.x, h1, l1);
         }
-        const int64_t w0 = (int64_t)(2 * t) * (kdim / 2) + slot;
-        const int64_t w1 = w0 + kdim / 2;
+        // blocked layout [slot / 32][row][32 slots x (re, im)]: a stage's rows are contiguous
+        const int64_t w0 = ((slot / kStageSlots) * table_rows + 2 * t) * kStageSlots + (slot % kStageSlots);
+        const int64_t w1 = w0 + kStageSlots;
         hi[w0] = h0;
         lo[w0] = l0;
         hi[w1] = h1;
@@ -407,15 +411,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     uint8_t* ux = bl + p.bmax * 128;
                     trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
-                    const int k0 = 2 * slot0;
+                    // rows of this stage's 32-slot block: contiguous 128-byte rows from row0
+                    const int row0 = (slot0 / kStageSlots) * p.table_rows + T.brow;
                     int r = 0;
                     for (int b = 0; b < n64; ++b, r += 64) {
-                        tma_load_2d(bh + r * 128, &map_hi64, k0, T.brow + r, &full_b[slot]);
-                        tma_load_2d(bl + r * 128, &map_lo64, k0, T.brow + r, &full_b[slot]);
+                        tma_load_2d(bh + r * 128, &map_hi64, 0, row0 + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo64, 0, row0 + r, &full_b[slot]);
                     }
                     for (; r < T.ncols; r += 16) {
-                        tma_load_2d(bh + r * 128, &map_hi, k0, T.brow + r, &full_b[slot]);
-                        tma_load_2d(bl + r * 128, &map_lo, k0, T.brow + r, &full_b[slot]);
+                        tma_load_2d(bh + r * 128, &map_hi, 0, row0 + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo, 0, row0 + r, &full_b[slot]);
                     }
                     trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
                     ++issued;
@@ -825,15 +830,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     if (leader) trj_mbar_arrive_expect_tx(&full_b[slot], (unsigned)(P.ncols * 256));
                     trj_mbar_arrive_expect_tx(&full_u[slot], (unsigned)kUxyBytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
-                    const int k0 = 2 * slot0;
+                    const int rowb = (slot0 / kStageSlots) * p.table_rows + row0;  // this stage's block
                     int r = 0;
                     for (int b = 0; b < n64; ++b, r += 64) {
-                        tma_load_2d_pair(bh + r * 128, &map_hi64, k0, row0 + r, lead_full);
-                        tma_load_2d_pair(bl + r * 128, &map_lo64, k0, row0 + r, lead_full);
+                        tma_load_2d_pair(bh + r * 128, &map_hi64, 0, rowb + r, lead_full);
+                        tma_load_2d_pair(bl + r * 128, &map_lo64, 0, rowb + r, lead_full);
                     }
                     for (; r < half; r += 16) {
-                        tma_load_2d_pair(bh + r * 128, &map_hi, k0, row0 + r, lead_full);
-                        tma_load_2d_pair(bl + r * 128, &map_lo, k0, row0 + r, lead_full);
+                        tma_load_2d_pair(bh + r * 128, &map_hi, 0, rowb + r, lead_full);
+                        tma_load_2d_pair(bl + r * 128, &map_lo, 0, rowb + r, lead_full);
                     }
                     trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_u[slot]);
                     ++issued;
@@ -1395,17 +1400,19 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->sched_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
     plan->scratch_bytes += (int64_t)(2 * tab_bytes + uxy_bytes + part_bytes);
-    int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
-                        16, CU_TENSOR_MAP_SWIZZLE_128B);
+    // Blocked table: [total_slots / 32][table_rows][64 bf16] as a 2-D map of 128-byte rows.
+    const int64_t brows = (st->total_slots / kStageSlots) * (int64_t)st->table_rows;
+    int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 64, brows, 64, 16,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc == TRJ_OK)
-        rc = encode_map(ctx, &st->map_lo, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
-                        16, CU_TENSOR_MAP_SWIZZLE_128B);
+        rc = encode_map(ctx, &st->map_lo, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 64, brows, 64, 16,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc == TRJ_OK)
-        rc = encode_map(ctx, &st->map_hi64, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
-                        64, CU_TENSOR_MAP_SWIZZLE_128B);
+        rc = encode_map(ctx, &st->map_hi64, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 64, brows, 64, 64,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc == TRJ_OK)
-        rc = encode_map(ctx, &st->map_lo64, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, kdim, st->table_rows, 64,
-                        64, CU_TENSOR_MAP_SWIZZLE_128B);
+        rc = encode_map(ctx, &st->map_lo64, st->tab_lo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 64, brows, 64, 64,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
@@ -1418,11 +1425,11 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     TcState* st = reinterpret_cast<TcState*>(plan->tc_state);
     if (!st || !st->tab_hi)
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor-core S(Q) path was not prepared for this plan");
-    const int64_t kdim = 2 * st->total_slots;
     const int nz_count = st->table_rows / 2;
     dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 32));
     tc_ztable_kernel<<<zg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
-                                        st->total_slots, st->nz_min, nz_count, kdim, st->tab_hi, st->tab_lo, st->uxy,
+                                        st->total_slots, st->nz_min, nz_count, (int64_t)st->table_rows, st->tab_hi,
+                                        st->tab_lo, st->uxy,
                                         plan->qsp >= 0 ? plan->n_atoms : INT64_MAX);
     TcParams P;
     P.tiles = st->tiles_dev;
@@ -1438,6 +1445,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.flush_stages = st->flush_stages;
     P.stage_bytes = st->stage_bytes;
     P.bmax = st->bmax;
+    P.table_rows = st->table_rows;
     P.status = ctx->status_dev;
     // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1458,6 +1466,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         Q.flush_stages = st->flush_stages;
         Q.stage_bytes = st->stage_bytes2;
         Q.bhalf = st->bhalf;
+        Q.table_rows = st->table_rows;
         Q.status = ctx->status_dev;
         TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                st->smem_bytes2));
