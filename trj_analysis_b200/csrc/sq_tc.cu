@@ -1426,7 +1426,10 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     if (!st || !st->tab_hi)
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor-core S(Q) path was not prepared for this plan");
     const int nz_count = st->table_rows / 2;
-    dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 32));
+    // Four row groups per slot: each thread walks a quarter of the nz rows, so the slot -> atom
+    // mapping (a 64-bit modulo) and the phase load are done 4 times per slot, not once per row group
+    // of 32.
+    dim3 zg((unsigned)((st->total_slots + 255) / 256), (unsigned)std::min(nz_count, 4));
     tc_ztable_kernel<<<zg, 256, 0, s>>>(plan->phase_dev, plan->species_off_dev, st->pad_off_dev, plan->nsp,
                                         st->total_slots, st->nz_min, nz_count, (int64_t)st->table_rows, st->tab_hi,
                                         st->tab_lo, st->uxy,
