@@ -52,6 +52,10 @@ CASES = [
     ("cells_mixed_axes", frames.FCCSpec(cells=(3, 12, 12), sigma=0.1, fractions=(0.7, 0.3), seed=5), 0.02, 2.4,
      True),
     ("cells_3_per_axis", frames.FCCSpec(cells=(7, 7, 7), sigma=0.1, seed=6), 0.02, 3.9, True),
+    # 5 cells per axis (no minimum image inside the box) with ~562 atoms per cell: two home rounds of
+    # 512 and self tasks whose neighbours span two staged chunks, with the box cull active.
+    ("cells_fast_rounds", frames.FCCSpec(cells=(26, 26, 26), density=1.0, sigma=0.1, fractions=(0.5, 0.5),
+                                         seed=9), 0.02, 8.2, True),
 ]
 
 
