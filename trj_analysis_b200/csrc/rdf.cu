@@ -20,8 +20,10 @@
 // those of the full stencil.
 //
 // Neighbour-cell atoms are staged into shared memory with 1-D TMA bulk copies
-// (cp.async.bulk, no multicast), double-buffered on mbarriers; each warp counts into its own
-// uint32 shared histogram replica; replicas are merged with 64-bit global atomics at exit.
+// (cp.async.bulk, no multicast) into two slots, each on its own mbarrier.  Warps walk the task
+// sequence independently: the last warp to release a slot refills it with the next task, so there
+// is no CTA barrier per task.  Warps count into uint32 shared histogram replicas (warp w uses
+// replica w mod nrep); replicas are merged with 64-bit global atomics at exit.
 #include <curand_kernel.h>
 #include <math.h>
 
@@ -92,8 +94,9 @@ __device__ __forceinline__ int outcome(float rr2, float side2, float deltar, int
     return (ind <= lsmax && ind > 0) ? ind : 0;
 }
 
-// Task iterator run by thread 0: items are taken from a global counter (dynamic balance);
-// item = (cell, offset, home split, neighbour segment); tasks = (home chunk, neighbour chunk).
+// Task iterator, run by one thread at a time (the thread that refills a slot): items are taken from
+// a global counter (dynamic balance); item = (cell, offset, home round, neighbour segment);
+// tasks = (home round of up to 512 atoms, neighbour chunk of up to 512 atoms).
 struct TaskGen {
     int64_t w;
     int hc, jc;
@@ -344,8 +347,8 @@ __device__ __forceinline__ void refill_slot(int slot, TaskGen& gen, const RdfPar
 }
 
 // QMODE: sorted_q holds the charges in cell order and gqq_frame (lsmax doubles) receives this
-// frame's sum of q_a*q_b per bin; each warp's charge replica (lsmax doubles) follows the count
-// replicas in shared memory.
+// frame's sum of q_a*q_b per bin; the charge replicas (lsmax doubles each, warp w uses w mod nrep)
+// follow the count replicas in shared memory.
 template <bool FLOOR, bool QMODE>
 __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, const float4* __restrict__ sorted,
                                                              const int32_t* __restrict__ cstart,
