@@ -141,6 +141,8 @@ TRJ_API int trj_frame_pack_charges(trj_ctx* ctx, const float* xyz_dev, const int
  * Every GPU that loads the library keeps that array until the process exits.
  * The first call on a device resolves the array's address on that device
  * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The address is kept for the life of the process: resetting the device
+ * (cudaDeviceReset) after that first call is not supported.
  * All calls share the array and overwrite what they use: calls whose work
  * overlaps on the GPU (other streams or host threads) race on it.
  * Arguments and results are those of trj_frame_pack. */

@@ -284,9 +284,12 @@ static void rdf_cells_impl(const float* pos, const int32_t* sp, const float* q, 
  * pos: N x 3 FP32 species-contiguous; sp_off: nsp+1 offsets; vec: nvec x 3 ints.
  * rho: nsp x nvec x 2 doubles (re, im), overwritten.
  *
- * Separable evaluation: per atom, e^{i 2 pi n s} for every needed n on each
- * axis is computed by a direct FP64 sincos of the reduced fraction, and the
- * 3-factor product is taken in FP64.
+ * Separable evaluation: per block of atoms, e^{i 2 pi n s} for every needed n on
+ * each axis is a direct FP64 cos/sin of the reduced fraction n s - nint(n s),
+ * stored per axis value as contiguous runs over the block's atoms.  Vectors are
+ * grouped by (nx, ny): the FP64 product X Y of a group is formed once per atom
+ * and multiplied by Z for each nz of the group.  Sums are FP64 (four partial
+ * sums per vector inside a block, then per block and per thread).
  */
 static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int64_t* sp_off, int nsp,
                           const float box[3], int64_t nvec, const int32_t* vec, double* rho);
@@ -303,27 +306,52 @@ ORC_EXPORT void orc_rho_fp64_w(const float* pos, const float* w, int64_t n, cons
     rho_fp64_impl(pos, w, n, sp_off, nsp, box, nvec, vec, rho);
 }
 
+#define ORC_BLK 256                                   /* atoms per block */
+typedef double orc_v4 __attribute__((vector_size(32)));  /* four doubles (plain SIMD pairs on SSE2) */
+
+static const int32_t* g_sort_vec;
+static int cmp_xy(const void* pa, const void* pb) {
+    const int64_t a = *(const int64_t*)pa, b = *(const int64_t*)pb;
+    const int32_t* va = g_sort_vec + 3 * a;
+    const int32_t* vb = g_sort_vec + 3 * b;
+    if (va[0] != vb[0]) return va[0] < vb[0] ? -1 : 1;
+    if (va[1] != vb[1]) return va[1] < vb[1] ? -1 : 1;
+    return a < b ? -1 : (a > b);
+}
+
 static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int64_t* sp_off, int nsp,
                           const float box[3], int64_t nvec, const int32_t* vec, double* rho) {
     (void)n;
+    memset(rho, 0, sizeof(double) * 2 * (size_t)nsp * nvec);
+    if (nvec == 0) return;
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     for (int64_t v = 0; v < nvec; ++v)
         for (int d = 0; d < 3; ++d) {
             if (vec[3 * v + d] < lo[d]) lo[d] = vec[3 * v + d];
             if (vec[3 * v + d] > hi[d]) hi[d] = vec[3 * v + d];
         }
-    int span[3], off[3];
-    for (int d = 0; d < 3; ++d) { span[d] = hi[d] - lo[d] + 1; off[d] = -lo[d]; }
-    int tsz = span[0] + span[1] + span[2];
-    memset(rho, 0, sizeof(double) * 2 * (size_t)nsp * nvec);
-    const int B = 64;
-    for (int a = 0; a < nsp; ++a) {
-        int64_t j0 = sp_off[a], j1 = sp_off[a + 1];
-        int64_t nblk = (j1 - j0 + B - 1) / B;
-        int nthr = 1;
+    int span[3];
+    for (int d = 0; d < 3; ++d) span[d] = hi[d] - lo[d] + 1;
+    const int tsz = span[0] + span[1] + span[2];
+    /* vectors sorted by (nx, ny); groups of equal (nx, ny) */
+    int64_t* ord = (int64_t*)malloc(sizeof(int64_t) * (size_t)nvec);
+    for (int64_t v = 0; v < nvec; ++v) ord[v] = v;
+    g_sort_vec = vec;
+    qsort(ord, (size_t)nvec, sizeof(int64_t), cmp_xy);
+    int64_t* gstart = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nvec + 1));
+    int64_t ng = 0;
+    for (int64_t k = 0; k < nvec; ++k) {
+        const int32_t* a = vec + 3 * ord[k];
+        if (k == 0 || a[0] != vec[3 * ord[k - 1]] || a[1] != vec[3 * ord[k - 1] + 1]) gstart[ng++] = k;
+    }
+    gstart[ng] = nvec;
+    int nthr = 1;
 #ifdef _OPENMP
-        nthr = omp_get_max_threads();
+    nthr = omp_get_max_threads();
 #endif
+    for (int a = 0; a < nsp; ++a) {
+        const int64_t j0 = sp_off[a], j1 = sp_off[a + 1];
+        const int64_t nblk = (j1 - j0 + ORC_BLK - 1) / ORC_BLK;
         double* acc = (double*)calloc((size_t)nthr * nvec * 2, sizeof(double));
 #pragma omp parallel
         {
@@ -332,47 +360,69 @@ static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int
             t = omp_get_thread_num();
 #endif
             double* my = acc + (size_t)t * nvec * 2;
-            double* tab = (double*)malloc(sizeof(double) * 2 * (size_t)tsz * B);
+            /* table [axis value][re/im][ORC_BLK], zero past the block's atoms */
+            double* tab = (double*)aligned_alloc(64, sizeof(double) * 2 * (size_t)tsz * ORC_BLK);
+            double* ar = (double*)aligned_alloc(64, sizeof(double) * ORC_BLK);
+            double* ai = (double*)aligned_alloc(64, sizeof(double) * ORC_BLK);
 #pragma omp for schedule(dynamic, 1)
             for (int64_t b = 0; b < nblk; ++b) {
-                int64_t jb = j0 + b * B, je = jb + B < j1 ? jb + B : j1;
-                int cnt = (int)(je - jb);
-                for (int q = 0; q < cnt; ++q) {
-                    const float* r = pos + 3 * (jb + q);
-                    double* tq = tab + (size_t)2 * tsz * q;
-                    int base = 0;
-                    for (int d = 0; d < 3; ++d) {
-                        double s = (double)r[d] / (double)box[d];
-                        for (int m = 0; m < span[d]; ++m) {
-                            double t2 = (double)(m - off[d]) * s;
-                            t2 -= nearbyint(t2);
-                            double ang = 2.0 * M_PI * t2;
-                            tq[2 * (base + m)] = cos(ang);
-                            tq[2 * (base + m) + 1] = sin(ang);
+                const int64_t jb = j0 + b * ORC_BLK, je = jb + ORC_BLK < j1 ? jb + ORC_BLK : j1;
+                const int cnt = (int)(je - jb);
+                int base = 0;
+                for (int d = 0; d < 3; ++d) {
+                    for (int m = 0; m < span[d]; ++m) {
+                        double* re = tab + (size_t)(base + m) * 2 * ORC_BLK;
+                        double* im = re + ORC_BLK;
+                        for (int q = 0; q < ORC_BLK; ++q) {
+                            if (q < cnt) {
+                                const double s = (double)pos[3 * (jb + q) + d] / (double)box[d];
+                                double t2 = (double)(m + lo[d]) * s;
+                                t2 -= nearbyint(t2);
+                                const double ang = 2.0 * M_PI * t2;
+                                /* the weight rides on the z factor */
+                                const double wq = (d == 2 && w) ? (double)w[jb + q] : 1.0;
+                                re[q] = wq * cos(ang);
+                                im[q] = wq * sin(ang);
+                            } else {
+                                re[q] = 0.0;
+                                im[q] = 0.0;
+                            }
                         }
-                        base += span[d];
                     }
+                    base += span[d];
                 }
-                for (int64_t v = 0; v < nvec; ++v) {
-                    int ix = vec[3 * v] + off[0];
-                    int iy = span[0] + vec[3 * v + 1] + off[1];
-                    int iz = span[0] + span[1] + vec[3 * v + 2] + off[2];
-                    double sr = 0.0, si = 0.0;
-                    for (int q = 0; q < cnt; ++q) {
-                        const double* tq = tab + (size_t)2 * tsz * q;
-                        double xr = tq[2 * ix], xi = tq[2 * ix + 1];
-                        double yr = tq[2 * iy], yi = tq[2 * iy + 1];
-                        double zr = tq[2 * iz], zi = tq[2 * iz + 1];
-                        double pr = xr * yr - xi * yi, pi2 = xr * yi + xi * yr;
-                        const double wq = w ? (double)w[jb + q] : 1.0;
-                        sr += wq * (pr * zr - pi2 * zi);
-                        si += wq * (pr * zi + pi2 * zr);
+                for (int64_t g = 0; g < ng; ++g) {
+                    const int32_t* v0 = vec + 3 * ord[gstart[g]];
+                    const double* xr = tab + (size_t)(v0[0] - lo[0]) * 2 * ORC_BLK;
+                    const double* xi = xr + ORC_BLK;
+                    const double* yr = tab + (size_t)(span[0] + v0[1] - lo[1]) * 2 * ORC_BLK;
+                    const double* yi = yr + ORC_BLK;
+                    for (int q = 0; q < ORC_BLK; ++q) {
+                        ar[q] = xr[q] * yr[q] - xi[q] * yi[q];
+                        ai[q] = xr[q] * yi[q] + xi[q] * yr[q];
                     }
-                    my[2 * v] += sr;
-                    my[2 * v + 1] += si;
+                    for (int64_t k = gstart[g]; k < gstart[g + 1]; ++k) {
+                        const int64_t v = ord[k];
+                        const double* zr = tab + (size_t)(span[0] + span[1] + vec[3 * v + 2] - lo[2]) * 2 * ORC_BLK;
+                        const double* zi = zr + ORC_BLK;
+                        orc_v4 sr = {0, 0, 0, 0}, si = {0, 0, 0, 0};
+                        for (int q = 0; q < ORC_BLK; q += 4) {
+                            orc_v4 a_r, a_i, z_r, z_i;
+                            memcpy(&a_r, ar + q, 32);
+                            memcpy(&a_i, ai + q, 32);
+                            memcpy(&z_r, zr + q, 32);
+                            memcpy(&z_i, zi + q, 32);
+                            sr += a_r * z_r - a_i * z_i;
+                            si += a_r * z_i + a_i * z_r;
+                        }
+                        my[2 * v] += (sr[0] + sr[1]) + (sr[2] + sr[3]);
+                        my[2 * v + 1] += (si[0] + si[1]) + (si[2] + si[3]);
+                    }
                 }
             }
             free(tab);
+            free(ar);
+            free(ai);
         }
         for (int t = 0; t < nthr; ++t)
             for (int64_t v = 0; v < nvec; ++v) {
@@ -381,6 +431,8 @@ static void rho_fp64_impl(const float* pos, const float* w, int64_t n, const int
             }
         free(acc);
     }
+    free(ord);
+    free(gstart);
 }
 
 /*

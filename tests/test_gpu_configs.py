@@ -1,0 +1,284 @@
+"""The benchmark configurations at their stated sizes, on the GPU, against the CPU oracle.
+
+* c3, N = 1,000,188, three species, L = 107.73 (13^3 cells): the g(r) pair histogram of three
+  frames bit for bit against the oracle's linked-cell restatement of rdf_sh (rdf.cuf:449-475),
+  edge counters included; S(Q) on every shell (all dense shells below qmin = 3 and every axis
+  shell up to nqmax = 171) against the exact FP64 oracle, for the split-BF16 tensor path in both
+  tile forms and the plain FP32 direct sum.
+* c2, N = 62,500 binary 80:20: the precision configuration (deltar 0.01, rcrdf 10; full grid below
+  qmin = 5 and 200 sampled lattice vectors per shell up to qmax = 15) over ten frames, plain and
+  split against FP64 per shell.
+* c1, N = 4,000 single species, rcrdf = L/2 (fewer than 3 cells per axis: the all-pairs route of
+  rdf_sh) and the full grid |k| <= 20, ten frames.
+* c4, N = 4,000,000 in a 1:1:4 slab: g(r) of one frame bit-exact, S(Q) with per-axis phase tables
+  of different lengths (nx, ny <= 34, nz <= 137) on selected dense shells and every axis shell,
+  in the corrected k-set and in the reference k-set (quirk Q4: axis vectors binned at integer k,
+  sq.cuf:372-454), and the plans' device footprint.
+
+Shell bar, as in the other S(Q) tests: |sum_gpu - sum_fp64| <= 1e-5 * sqrt(sum_aa * sum_bb) per
+shell and species pair.  With TRJ_SHELL_TABLE_DIR set, each S(Q) test writes its per-shell error
+table there as JSON (shell index, Q, vectors, max error over the species pairs).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import orc
+from trj_analysis_b200 import frames, refsem
+
+pytestmark = pytest.mark.gpu
+
+REL_SHELL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from trj_analysis_b200 import engine
+    c = engine.Context(0)
+    yield c
+    c.close()
+
+
+def _layout(fr, nsp):
+    return orc.layout(fr.xyz, fr.types - 1, fr.box, nsp)
+
+
+def gpu_hist(ctx, frs, nsp, deltar, rcrdf):
+    from trj_analysis_b200 import engine
+    stage = engine.FrameStage(ctx, frs[0].n, nsp)
+    rdf = engine.RdfPlan(ctx, nsp, deltar, rcrdf, frs[0].box, frs[0].n)
+    hist = rdf.new_hist()
+    edge = torch.zeros(4, dtype=torch.int64, device=ctx.torch_device)
+    for fr in frs:
+        n = stage.upload_and_pack(fr.xyz, fr.types - 1, fr.box)
+        rdf.accumulate(stage.packed, n, fr.box, hist, edge)
+    ctx.check()
+    out = hist.cpu().numpy().astype(np.uint64), edge.cpu().numpy().astype(np.uint64), rdf.cells, rdf.scratch_bytes
+    rdf.close()
+    del stage
+    return out
+
+
+def oracle_hist(frs, nsp, deltar, rcrdf, cells):
+    p = refsem.rdf_params(nsp, deltar, rcrdf, frs[0].box)
+    h = np.zeros((p.nit, p.lsmax), np.uint64)
+    e = np.zeros(3, np.uint64)
+    for fr in frs:
+        pos, sp, _ = _layout(fr, nsp)
+        hh, ee = orc.rdf_counts(pos, sp, fr.box, p.side2, p.deltar, p.lsmax, nsp, cells=cells)
+        h += hh
+        e += ee
+    return h, e, p
+
+
+def gpu_sq(ctx, frs, nsp, ks, method, pairs=False):
+    """Accumulated [nbins][nit] shell sums over the frames and rho of the last frame."""
+    from trj_analysis_b200 import engine
+    stage = engine.FrameStage(ctx, frs[0].n, nsp)
+    plan = engine.SqPlan(ctx, nsp, ks, np.bincount(frs[0].types - 1, minlength=nsp))
+    plan.set_pairs(pairs)
+    out = plan.new_out()
+    for fr in frs:
+        n = stage.upload_and_pack(fr.xyz, fr.types - 1, fr.box)
+        plan.accumulate(stage.packed, n, fr.box, out, engine.METHODS[method])
+    ctx.check()
+    res = out.cpu().numpy()
+    rho = plan.rho().cpu().numpy()
+    scratch = plan.scratch_bytes
+    plan.close()
+    del stage
+    return res, rho, scratch
+
+
+def oracle_sq(frs, nsp, ks, vectors=None):
+    """FP64 shell sums over the frames (w Re(rho_a conj rho_b) per vector)."""
+    ref = np.zeros((ks.nbins, nsp * (nsp + 1) // 2))
+    rho = None
+    for fr in frs:
+        pos, _, off = _layout(fr, nsp)
+        rho = orc.rho_fp64(pos, off, fr.box, ks.vectors if vectors is None else vectors)
+        ref += orc.bin_sums(rho, ks.bins, ks.weights, ks.nbins)
+    return ref, rho
+
+
+def shell_errors(res, ref, nsp):
+    """Per shell: max over species pairs of |res - ref| / sqrt(ref_aa ref_bb); NaN for empty shells."""
+    rows = refsem.pair_rows(nsp)
+    diag = {a: ref[:, refsem.pair_row(a, a, nsp)] for a in range(nsp)}
+    scale = np.stack([np.sqrt(np.abs(diag[a] * diag[b])) for a, b in rows], axis=1)
+    live = scale > 0
+    rel = np.where(live, np.abs(res - ref) / np.where(live, scale, 1.0), 0.0)
+    err = rel.max(axis=1)
+    err[~live.any(axis=1)] = np.nan
+    assert np.all(res[~live] == 0), "a shell without vectors has a nonzero sum"
+    return err
+
+
+def write_table(name, ks, errs: dict):
+    d = os.environ.get("TRJ_SHELL_TABLE_DIR")
+    if not d:
+        return
+    os.makedirs(d, exist_ok=True)
+    nvec = np.bincount(ks.bins, minlength=ks.nbins)
+    rows = []
+    for b in range(ks.nbins):
+        if nvec[b] == 0:
+            continue
+        row = {"shell": b, "Q": float(b * ks.dq), "vectors": int(nvec[b]), "dense": bool(ks.dense[ks.bins == b].any())}
+        for k, e in errs.items():
+            row[k] = None if np.isnan(e[b]) else float(e[b])
+        rows.append(row)
+    with open(os.path.join(d, f"shells_{name}.json"), "w") as f:
+        json.dump({"config": name, "rows": rows,
+                   "max": {k: float(np.nanmax(e)) for k, e in errs.items()}}, f, indent=1)
+
+
+# ---- c3: N = 1,000,188 ----------------------------------------------------------
+
+@pytest.fixture(scope="module")
+def c3_frames():
+    spec = frames.c3_spec()
+    return [spec.frame(i) for i in range(3)]
+
+
+def test_c3_pair_counts_bit_exact_three_frames(ctx, c3_frames):
+    h_g, e_g, cells, _ = gpu_hist(ctx, c3_frames, 3, 0.01, 8.0)
+    h_o, e_o, p = oracle_hist(c3_frames, 3, 0.01, 8.0, cells=True)
+    assert cells == (13, 13, 13) and p.lsmax == 801 and h_o.shape == (6, 801)
+    assert np.array_equal(h_g, h_o)
+    assert int(e_g[2]) == int(e_o[2]) == int(h_o.sum())
+    assert int(e_g[0]) == int(e_o[0]) and int(e_g[1]) == int(e_o[1])
+    assert 8.4e8 * 3 < int(h_o.sum()) < 8.7e8 * 3
+
+
+@pytest.fixture(scope="module")
+def c3_sq(c3_frames):
+    fr = c3_frames[0]
+    ks = refsem.make_kset("full+axes", fr.box, 10.0, 3.0)
+    ref, rho = oracle_sq([fr], 3, ks)
+    return fr, ks, ref, rho
+
+
+def test_c3_sq_every_shell_within_1e5(ctx, c3_sq):
+    fr, ks, ref, rho_o = c3_sq
+    assert ks.nqmax == 171 and ks.nvec == 270419
+    errs = {}
+    for name, method, pairs in (("split", "split", False), ("split_pairs", "split", True), ("plain", "plain", False)):
+        res, rho_g, _ = gpu_sq(ctx, [fr], 3, ks, method, pairs)
+        errs[name] = shell_errors(res, ref, 3)
+        # per vector (tensor path: hi+lo BF16 keeps ~16 significant bits per factor)
+        off = np.bincount(fr.types - 1, minlength=3)
+        tol = (3e-5 if method == "split" else 2e-6) * off[:, None] + 1e-5
+        assert np.all(np.abs(rho_g - rho_o) <= tol), name
+    write_table("c3", ks, errs)
+    live = ~np.isnan(errs["split"])
+    assert live.sum() == 171  # shells 1..171 all carry vectors
+    for name, e in errs.items():
+        assert np.nanmax(e) <= REL_SHELL, (name, np.nanargmax(e), np.nanmax(e))
+
+
+# ---- c2: N = 62,500, the precision configuration --------------------------------
+
+def test_c2_precision_config_ten_frames(ctx):
+    spec = frames.c2_spec()
+    frs = [spec.frame(i) for i in range(10)]
+    ks = refsem.make_kset("full+sampled", frs[0].box, 15.0, 5.0, seed=0, per_shell=200)
+    assert ks.nqmax == 102 and ks.nvec == 92581
+    ref, _ = oracle_sq(frs, 2, ks)
+    errs = {}
+    for method in ("split", "plain"):
+        res, _, _ = gpu_sq(ctx, frs, 2, ks, method)
+        errs[method] = shell_errors(res, ref, 2)
+    write_table("c2", ks, errs)
+    for name, e in errs.items():
+        assert np.nanmax(e) <= REL_SHELL, (name, np.nanargmax(e), np.nanmax(e))
+    # pair counts of the same frames: deltar 0.01, rcrdf 10 (4 cells per axis)
+    h_g, e_g, cells, _ = gpu_hist(ctx, frs[:3], 2, 0.01, 10.0)
+    h_o, e_o, p = oracle_hist(frs[:3], 2, 0.01, 10.0, cells=True)
+    assert cells == (4, 4, 4) and p.lsmax == 1001
+    assert np.array_equal(h_g, h_o) and np.array_equal(e_g[:3], e_o)
+
+
+# ---- c1: N = 4,000, rcrdf = L/2, full grid |k| <= 20 -------------------------------
+
+def test_c1_as_configured_ten_frames(ctx):
+    spec = frames.c1_spec()
+    frs = [spec.frame(i) for i in range(10)]
+    h_g, e_g, cells, _ = gpu_hist(ctx, frs, 1, 0.02, 1e9)
+    h_o, e_o, p = oracle_hist(frs, 1, 0.02, 1e9, cells=False)  # rdf_sh's all-pairs loop
+    assert p.lsmax == 428 and abs(p.rcrdf - float(frs[0].box[0]) / 2) < 1e-5
+    assert min(cells) < 3  # the all-pairs route, not the cell stencil
+    assert np.array_equal(h_g, h_o) and np.array_equal(e_g[:3], e_o)
+    ks = refsem.make_kset("full", frs[0].box, 20.0, None)
+    assert ks.nvec == 339250 and ks.nbins == 55
+    ref, _ = oracle_sq(frs, 1, ks)
+    errs = {}
+    for method in ("plain", "split"):
+        res, _, _ = gpu_sq(ctx, frs, 1, ks, method)
+        errs[method] = shell_errors(res, ref, 1)
+    write_table("c1", ks, errs)
+    for name, e in errs.items():
+        assert np.nanmax(e) <= REL_SHELL, (name, np.nanargmax(e), np.nanmax(e))
+
+
+# ---- c4: N = 4,000,000 slab 1:1:4 -------------------------------------------------
+
+@pytest.fixture(scope="module")
+def c4_frame():
+    return frames.c4_spec().frame(0)
+
+
+def test_c4_pair_counts_bit_exact(ctx, c4_frame):
+    fr = c4_frame
+    assert fr.n == 4_000_000
+    h_g, e_g, cells, scratch = gpu_hist(ctx, [fr], 2, 0.02, 6.0)
+    h_o, e_o, p = oracle_hist([fr], 2, 0.02, 6.0, cells=True)
+    assert p.lsmax == 301 and p.rcrdf == 6.0
+    assert cells[0] == cells[1] and cells[2] >= 4 * cells[0] - 1
+    assert np.array_equal(h_g, h_o)
+    assert int(e_g[2]) == int(e_o[2]) and int(e_g[0]) == int(e_o[0]) and int(e_g[1]) == int(e_o[1])
+    assert 1.3e9 < int(h_o.sum()) < 1.6e9
+
+
+# dense shells checked at c4 (every shell's vectors at 4e6 atoms would take minutes of FP64 on the host)
+C4_DENSE = [1, 2, 3, 4, 5, 8, 13, 21, 34, 55, 89, 136]
+
+
+@pytest.mark.parametrize("mode", ["full+axes", "ref"])
+def test_c4_sq_per_axis_tables(ctx, c4_frame, mode):
+    fr = c4_frame
+    ks = refsem.make_kset(mode, fr.box, 8.0, 2.0)
+    assert ks.nqmax == 549
+    dense = ks.dense.astype(bool)
+    if mode == "ref":
+        # quirk Q4: an axis vector k along x or y is binned at k although |q| = k * fk_x = 4 k dq
+        ax = ~dense & (ks.vectors[:, 1] == 0) & (ks.vectors[:, 2] == 0)
+        assert np.array_equal(ks.bins[ax], ks.vectors[ax, 0])
+        assert ks.nqmin == 32
+        sel_dense = np.isin(ks.bins, [1, 2, 3, 5, 8, 13, 21, 34, 55, 89, 128]) & dense
+    else:
+        assert ks.nqmin == 136
+        sel_dense = np.isin(ks.bins, C4_DENSE) & dense
+    sel = sel_dense | ~dense
+    # shells whose every vector is in the subset (the plan's own sums compare there)
+    shells = np.flatnonzero((np.bincount(ks.bins[sel], minlength=ks.nbins) == np.bincount(ks.bins, minlength=ks.nbins))
+                            & (np.bincount(ks.bins, minlength=ks.nbins) > 0))
+    assert shells.size >= 100
+    sub = refsem.KSet(mode=ks.mode, dq=ks.dq, nqmax=ks.nqmax, vectors=ks.vectors[sel], bins=ks.bins[sel],
+                      weights=ks.weights[sel], dense=ks.dense[sel], nq=ks.nq, qmin_eff=ks.qmin_eff, lmax=ks.lmax,
+                      nqmin=ks.nqmin)
+    # the plan holds the whole k-set (the per-axis Z tables span nz up to 137); the check reads the subset
+    ref_sub, rho_o = oracle_sq([fr], 2, sub)
+    res, rho_g, scratch = gpu_sq(ctx, [fr], 2, ks, "split")
+    got = orc.bin_sums(rho_g[:, sel], ks.bins[sel], ks.weights[sel], ks.nbins)
+    err = shell_errors(got, ref_sub, 2)
+    # the plan's shell sums on the checked shells are the per-vector sums
+    assert np.allclose(res[shells], got[shells], rtol=1e-12, atol=1e-9 * np.abs(got).max())
+    write_table("c4_" + mode.replace("+", "_"), sub, {"split": err})
+    assert np.nanmax(err) <= REL_SHELL, (np.nanargmax(err), np.nanmax(err))
+    # footprint: the plan's own scratch fits a small share of the device
+    free, total = torch.cuda.mem_get_info()
+    assert 0 < scratch < 0.25 * total

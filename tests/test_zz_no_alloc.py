@@ -72,3 +72,40 @@ def test_static_pack_rejects_oversized_frame(ctx):
                                    vp(packed.data_ptr()), vp(counts.data_ptr()), vp(0))
     assert rc == _lib.TRJ_ERR_CAPACITY
     assert b"fixed array" in lib.trj_ctx_last_error(h)
+
+
+def test_static_pack_at_the_exact_limit(ctx):
+    """ceil(n/1024) * nsp == 87381 (nsp 9, n = 9709 * 1024) is the largest frame the fixed array takes:
+    it is laid out exactly as trj_frame_pack does; one atom more is refused before any launch."""
+    lib, h = ctx
+    nsp, n = 9, 9709 * 1024
+    assert -(-n // 1024) * nsp == 87381
+    g = torch.Generator(device="cuda").manual_seed(5)
+    box = np.array([300.0, 310.0, 320.0], np.float32)
+    xyz = (torch.rand((n, 3), device="cuda", generator=g) * 1.2 - 0.1) * torch.from_numpy(box).cuda()
+    sp = torch.randint(0, nsp, (n,), device="cuda", dtype=torch.int32, generator=g)
+    ref_p = torch.full((n, 4), -7.0, device="cuda")
+    ref_c = torch.zeros(nsp, dtype=torch.int64, device="cuda")
+    got_p = torch.full((n, 4), 3.0, device="cuda")
+    got_c = torch.full((nsp,), 99, dtype=torch.int64, device="cuda")
+    assert _pack(lib, "trj_frame_pack", h, xyz, sp, nsp, box, ref_p, ref_c) == 0
+    assert _pack(lib, "trj_frame_pack_static", h, xyz, sp, nsp, box, got_p, got_c) == 0
+    assert lib.trj_ctx_check(h, vp(torch.cuda.current_stream().cuda_stream)) == 0
+    assert torch.equal(got_c, ref_c) and int(got_c.sum()) == n
+    assert torch.equal(got_p.view(torch.int32), ref_p.view(torch.int32))
+    del xyz, sp, ref_p, got_p
+    small = torch.zeros((4, 4), device="cuda")
+    rc = lib.trj_frame_pack_static(h, vp(small.data_ptr()), vp(small.data_ptr()), n + 1, nsp, _lib.box3(box),
+                                   vp(small.data_ptr()), vp(got_c.data_ptr()), vp(0))
+    assert rc == _lib.TRJ_ERR_CAPACITY
+
+
+def test_static_pack_empty_frame_zeroes_counts(ctx):
+    lib, h = ctx
+    counts = torch.full((3,), 99, dtype=torch.int64, device="cuda")
+    packed = torch.zeros((1, 4), device="cuda")
+    rc = lib.trj_frame_pack_static(h, vp(0), vp(0), 0, 3, _lib.box3([5, 5, 5]), vp(packed.data_ptr()),
+                                   vp(counts.data_ptr()), vp(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    assert lib.trj_ctx_check(h, vp(torch.cuda.current_stream().cuda_stream)) == 0
+    assert counts.cpu().tolist() == [0, 0, 0]

@@ -65,6 +65,8 @@ extern "C" int trj_ctx_destroy(trj_ctx* ctx) {
         trj_device_guard g(ctx->device);
         if (ctx->status_dev) cudaFree(ctx->status_dev);
         if (ctx->status_host) cudaFreeHost(ctx->status_host);
+        // a caller allocator's free callback takes no stream: layout kernels still in flight finish first
+        if (ctx->alloc && !ctx->pack_scratch.empty()) cudaDeviceSynchronize();
         for (auto& kv : ctx->pack_scratch) trj_dev_free(ctx, kv.second.ptr);
         ctx->pack_scratch.clear();
     }
@@ -82,6 +84,12 @@ extern "C" int trj_ctx_set_allocator(trj_ctx* ctx, trj_alloc_fn alloc, trj_free_
     if (!ctx) return TRJ_ERR_INVALID;
     if ((alloc == nullptr) != (free_fn == nullptr))
         return trj_fail(ctx, TRJ_ERR_INVALID, "trj_ctx_set_allocator: give both callbacks or neither");
+    if (!ctx->pack_scratch.empty()) {
+        // Layout kernels on any stream may still use the scratch; the caller's free callback takes no
+        // stream, so nothing may be handed back to it before they finish.
+        trj_device_guard g(ctx->device);
+        TRJ_CUDA_TRY(ctx, cudaDeviceSynchronize());
+    }
     for (auto& kv : ctx->pack_scratch) trj_dev_free(ctx, kv.second.ptr);  // with the allocator that made it
     ctx->pack_scratch.clear();
     ctx->alloc = alloc;
@@ -290,9 +298,10 @@ static int frame_pack_impl(trj_ctx* ctx, const char* name, const float* xyz_dev,
     size_t need = (size_t)nblocks * nsp * (sizeof(int32_t) + sizeof(int64_t)) + 256;
     trj_ctx::PackScratch& ps = ctx->pack_scratch[stream];
     if (need > ps.bytes) {
-        // Earlier work of this stream may still read the old buffer; cudaFree waits for it, and a
-        // caller allocator receives the release from the thread that issued that work.
-        if (ps.ptr && !ctx->alloc) TRJ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+        // Earlier layout kernels of this stream may still use the old buffer, and neither cudaFree's
+        // implicit synchronisation nor a caller's free callback (which takes no stream) orders the
+        // release after them: wait for the stream first.
+        if (ps.ptr) TRJ_CUDA_TRY(ctx, cudaStreamSynchronize(s));
         trj_dev_free(ctx, ps.ptr);
         ps.ptr = nullptr;
         ps.bytes = 0;
@@ -351,7 +360,9 @@ extern "C" int trj_frame_pack_charges(trj_ctx* ctx, const float* xyz_dev, const 
 //
 // Limit: ceil(n / 1024) * nsp * 12 bytes must fit in kPackStaticBytes (1 MiB), i.e.
 // ceil(n / 1024) * nsp <= 87381 (about 29.8 million atoms for 3 species, 5.5 million for 16).
-// Every GPU that loads this library holds the 1 MiB array until the process exits.  All calls
+// Every GPU that loads this library holds the 1 MiB array until the process exits.  The array's
+// address is resolved once per device and kept for the life of the process, so resetting a device
+// (cudaDeviceReset) after the first call on it is not supported.  All calls
 // share it: each call overwrites every word it reads (nothing has to start at zero), and calls
 // whose kernels overlap on the GPU (different streams, other host threads) race on it.
 // ---------------------------------------------------------------------------
