@@ -167,6 +167,16 @@ TRJ_API int trj_rdf_plan_create_2d(trj_ctx* ctx, int nsp, float deltar, float rc
 /* Bin rule of the plan's counts: 0 = nint(r/deltar) (rdf_sh), 1 = int(r/deltar)+1
  * (rdfxy, rdf.cuf:722, the slab g(r)); bins 1..lsmax either way. */
 TRJ_API int trj_rdf_plan_set_binning(trj_rdf_plan* plan, int floor_bins);
+/* Failure handling of the pair kernel (the reference prints the CUDA error and
+ * stops, rdf.cuf:241-242; here a device wait that runs out sets TRJ_DEV_TIMEOUT,
+ * the kernel lets its copies in flight land and returns, and trj_ctx_check then
+ * reports TRJ_ERR_TIMEOUT with the context still usable).  clocks: limit of a
+ * warp's wait for a staged neighbour chunk, in SM clocks, 1000..2^32 (0 = the
+ * default 2^32, about 2 s).  stall_test = 1 makes each warp's first wait target a
+ * barrier that nothing arrives on, so that every launch of the plan runs out after
+ * `clocks`: a way to exercise the timeout path without a fault.  Copies in flight
+ * are always waited for with the default limit. */
+TRJ_API int trj_rdf_plan_set_wait(trj_rdf_plan* plan, int64_t clocks, int stall_test);
 /* Plan with nbins bins of width r_max/nbins covering [0, r_max): bin k (1-based)
  * holds r in [(k-1) dr, k dr), i.e. index floor(r/dr)+1, pairs counted for
  * rr2 < r_max^2 (FP32).  This is the binning of the freud RDF used by the

@@ -60,3 +60,28 @@ def test_served_counts_match_oracle(workload):
             h, _ = orc.rdf_counts(pos, sps, fr.box, p.side2, p.deltar, p.lsmax, req.nsp, cells=True)
             H = H + h
         assert np.array_equal(res[req.rid].hist, H)
+
+
+def test_cancel_running_and_queued_requests(workload):
+    """A request cancelled while it runs stops after the frames already on its stream and releases its
+    slot and budget; one cancelled while queued never starts; the others are unchanged."""
+    from trj_analysis_b200.serve import Server
+    reqs = sorted(workload, key=lambda r: -len(r.frames))[:6]
+    assert len(reqs[0].frames) >= 4
+    running, queued = reqs[0].rid, reqs[-1].rid
+
+    def hook(srv, turn):
+        if turn == 1:
+            srv.cancel(running)
+            srv.cancel(queued)
+
+    srv = Server(slots=2, n_max=1 << 14, method="split")
+    res = {r.rid: r for r in srv.run(reqs, realtime=False, on_turn=hook)}
+    assert sorted(srv.cancelled) == sorted([running, queued])
+    assert set(res) == {r.rid for r in reqs} - {running, queued}
+    assert srv.in_use == 0 and all(s.req is None for s in srv.slots)
+    for req in reqs:
+        if req.rid in res:
+            _, alone = _run([req], slots=1, method="split")
+            assert np.array_equal(alone[req.rid].hist, res[req.rid].hist)
+            assert np.array_equal(alone[req.rid].sq_sums, res[req.rid].sq_sums)

@@ -71,6 +71,7 @@ SIGNATURES = {
     "trj_sq_rho_groups": (c_int, [vp, vp, c_int64, P(c_float), c_int, vp, vp, vp]),
     "trj_sq_plan_set_z_from_y": (c_int, [vp, c_int]),
     "trj_rdf_plan_set_binning": (c_int, [vp, c_int]),
+    "trj_rdf_plan_set_wait": (c_int, [vp, c_int64, c_int]),
     "trj_sq_plan_destroy": (c_int, [vp]),
     "trj_dyn_plan_create": (c_int, [vp, c_int, c_int64, c_int, c_int, c_int64, vp, vp, c_int, vp, P(vp)]),
     "trj_dyn_plan_info": (c_int, [vp, P(c_int64)]),

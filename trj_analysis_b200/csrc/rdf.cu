@@ -55,6 +55,8 @@ struct RdfParams {
     int fast_ok;                // every axis split into >= 5 cells
     float cull2;                // (cutoff * (1 + 2^-10))^2: neighbours farther from a warp's box are skipped
     float cull_pad;             // added to the box half-widths: covers the FP32 rounding of the cull test
+    long long wait_clocks;      // limit of a warp's wait for a staged neighbour chunk
+    int stall_test;             // 1: each warp's first wait is on a barrier nothing arrives on (timeout test)
     int off[kMaxOffsets][3];
     int64_t nitems;
 };
@@ -67,7 +69,7 @@ struct TaskInfo {
     int hc;            // home chunk
     int self;          // home cell == neighbour cell
     int fast;          // no minimum image needed for any pair of the task
-    int cull;          // both cells hold only coordinates in [0, L): the box cull applies
+    int cull;          // both cells hold only coordinates in [-L, L): the box cull applies (wrapped values)
     float img[3];      // periodic image of the neighbour cell: 0 or -+L per axis
     int valid;         // 0 = no more tasks
 };
@@ -158,7 +160,7 @@ __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restr
             t.hc = g.hc;
             t.self = self;
             t.fast = p.fast_ok && !wraps && !cflag[c] && !cflag[c2];
-            t.cull = !cflag[c] && !cflag[c2];
+            t.cull = !((cflag[c] | cflag[c2]) & 2);
             t.img[0] = ex < 0 ? -p.L[0] : (ex >= p.nc[0] ? p.L[0] : 0.f);
             t.img[1] = ey < 0 ? -p.L[1] : (ey >= p.nc[1] ? p.L[1] : 0.f);
             t.img[2] = ez < 0 ? -p.L[2] : (ez >= p.nc[2] ? p.L[2] : 0.f);
@@ -251,7 +253,7 @@ struct WarpBox {
 
 __device__ __forceinline__ void axis_box(float v0, bool has0, float v1, bool has1, bool split, float img, float pad,
                                          float& c, float& h) {
-    // Coordinates of cull tasks lie in [0, L): their bit patterns order like the values (+0 for -0).
+    // Wrapped coordinates of cull tasks lie in [0, L]: their bit patterns order like the values (+0 for -0).
     const unsigned b0 = __float_as_uint(v0 + 0.0f), b1 = __float_as_uint(v1 + 0.0f);
     const unsigned lo = min(has0 ? b0 : 0x7f800000u, has1 ? b1 : 0x7f800000u);
     const unsigned hi = max(has0 ? b0 : 0u, has1 ? b1 : 0u);
@@ -261,10 +263,16 @@ __device__ __forceinline__ void axis_box(float v0, bool has0, float v1, bool has
     h = split ? 0.5f * (mx - mn) + pad : INFINITY;
 }
 
-__device__ __forceinline__ bool maybe_near(const float4& b, const float4& c, const float4& h, float cull2) {
-    const float gx = fmaxf(fabsf(b.x - c.x) - h.x, 0.f);
-    const float gy = fmaxf(fabsf(b.y - c.y) - h.y, 0.f);
-    const float gz = fmaxf(fabsf(b.z - c.z) - h.z, 0.f);
+// Wrapped coordinate of a folded one in [-L, L): x, or x + L for x < 0 (the same FP32 value the cell
+// assignment computes, so the atom lies in its cell's range).  The fold of select_ncdfinput keeps
+// negative coordinates negative; the cull works on the wrapped values.
+__device__ __forceinline__ float wrap_cull(float x, float L) { return x < 0.f ? __fadd_rn(x, L) : x; }
+
+__device__ __forceinline__ bool maybe_near(const float4& b, const float4& c, const float4& h, float cull2,
+                                           const float (&L)[3]) {
+    const float gx = fmaxf(fabsf(wrap_cull(b.x, L[0]) - c.x) - h.x, 0.f);
+    const float gy = fmaxf(fabsf(wrap_cull(b.y, L[1]) - c.y) - h.y, 0.f);
+    const float gz = fmaxf(fabsf(wrap_cull(b.z, L[2]) - c.z) - h.z, 0.f);
     return fmaf(gz, gz, fmaf(gy, gy, gx * gx)) <= cull2;
 }
 
@@ -288,9 +296,9 @@ __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* _
     if (il0w >= ti.na) return 0u;
     if (ti.cull) {
         float cx, cy, cz, hx, hy, hz;
-        axis_box(a0.x, h0, a1.x, h1, p.nc[0] > 1, ti.img[0], p.cull_pad, cx, hx);
-        axis_box(a0.y, h0, a1.y, h1, p.nc[1] > 1, ti.img[1], p.cull_pad, cy, hy);
-        axis_box(a0.z, h0, a1.z, h1, p.nc[2] > 1, ti.img[2], p.cull_pad, cz, hz);
+        axis_box(wrap_cull(a0.x, p.L[0]), h0, wrap_cull(a1.x, p.L[0]), h1, p.nc[0] > 1, ti.img[0], p.cull_pad, cx, hx);
+        axis_box(wrap_cull(a0.y, p.L[1]), h0, wrap_cull(a1.y, p.L[1]), h1, p.nc[1] > 1, ti.img[1], p.cull_pad, cy, hy);
+        axis_box(wrap_cull(a0.z, p.L[2]), h0, wrap_cull(a1.z, p.L[2]), h1, p.nc[2] > 1, ti.img[2], p.cull_pad, cz, hz);
         if (lane == 0) {
             wb->c = make_float4(cx, cy, cz, 0.f);
             wb->h = make_float4(hx, hy, hz, 0.f);
@@ -304,7 +312,7 @@ __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* _
     for (int jj0 = jbeg; jj0 < ti.jcount; jj0 += 32) {
         const int jl = jj0 + (int)lane;
         bool keep = jl < ti.jcount;
-        if (ti.cull && keep) keep = maybe_near(bj[jl], wb->c, wb->h, p.cull2);
+        if (ti.cull && keep) keep = maybe_near(bj[jl], wb->c, wb->h, p.cull2, p.L);
         unsigned m = __ballot_sync(0xffffffffu, keep);
         if (SELF)
             tested += (h0 ? __popc(m & after_mask(lim0, jj0)) : 0) + (h1 ? __popc(m & after_mask(lim1, jj0)) : 0);
@@ -364,6 +372,7 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
     float4* buf = reinterpret_cast<float4*>(smem);                       // [kSlots][kJChunk]
     unsigned* hist = reinterpret_cast<unsigned*>(smem + kSlots * kJChunk * sizeof(float4));
     __shared__ __align__(8) uint64_t bars[kSlots];
+    __shared__ __align__(8) uint64_t never;  // no thread arrives on it: the target of the stall test
     __shared__ TaskInfo tinfo[kSlots];
     __shared__ unsigned released[kSlots];  // warps done with the slot's task
     __shared__ unsigned phases[kSlots];    // phases armed per slot
@@ -393,6 +402,7 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
             released[sl] = 0u;
             phases[sl] = 0u;
         }
+        trj_mbar_init(&never, 1);
         trj_fence_mbar_init();
         for (int sl = 0; sl < kSlots; ++sl) refill_slot(sl, gen, p, cstart, ccount, cflag, work, sorted, tinfo, bars, phases, buf);
     }
@@ -406,7 +416,10 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         const int slot = t % kSlots;
         if (__shfl_sync(0xffffffffu, *(volatile int*)&abort_flag, 0)) break;  // warp-uniform
         // Warp-uniform outcome: the task loop below uses full-warp ballots.
-        if (!__all_sync(0xffffffffu, trj_mbar_wait(&bars[slot], (unsigned)(t / kSlots) & 1u))) {
+        const bool stall = p.stall_test && t == 0;
+        if (!__all_sync(0xffffffffu, trj_mbar_wait_limit(stall ? &never : &bars[slot],
+                                                         stall ? 0u : (unsigned)(t / kSlots) & 1u,
+                                                         p.wait_clocks))) {
             if (lane == 0) {
                 trj_raise(status, TRJ_DEV_TIMEOUT);
                 *(volatile int*)&abort_flag = 1;
@@ -450,7 +463,8 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
     }
     __syncthreads();
     if (tid == 0 && abort_flag) {
-        // Let copies still in flight land before the CTA exits (bounded).
+        // Let copies still in flight land before the CTA exits (bounded by the default limit, not by
+        // the plan's wait limit: a copy always lands).
         for (int sl = 0; sl < kSlots; ++sl)
             if (phases[sl]) trj_mbar_wait(&bars[sl], (phases[sl] - 1) & 1);
     }
@@ -502,10 +516,11 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     float r[3] = {v.x, v.y, v.z};
     int k[3], sub[3];
     const int S = 1 << sbits;
-    bool outside = false;
+    bool outside = false, far = false;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         outside |= !(r[d] >= 0.0f && r[d] < L[d]);
+        far |= !(r[d] >= -L[d] && r[d] < L[d]);
         float w = r[d] - L[d] * floorf(r[d] / L[d]);
         float t = w * ((float)nc[d] / L[d]);
         int c = (int)t;
@@ -523,7 +538,9 @@ __global__ void cell_assign_kernel(const float4* __restrict__ packed, int64_t n,
     akey[i] = key;
     aslot[i] = atomicAdd(&fcount[key], 1);
     atomicAdd(&ccount[c], 1);
-    if (outside) cflag[c] = 1;
+    // bit 0: a coordinate outside [0, L) (pairs of the cell need the minimum image);
+    // bit 1: a coordinate outside [-L, L) or NaN (its wrapped value is not x or x + L: no box cull)
+    if (outside) atomicOr(&cflag[c], far ? 3 : 1);
 }
 
 // Start of every (cell, sub-cell) key: the cell's start plus the exclusive prefix of its sub-cell
@@ -683,13 +700,15 @@ struct trj_rdf_plan {
     trj_ctx* ctx = nullptr;
     int nsp = 0, nit = 0, lsmax = 0;
     int floor_bins = 0;
+    long long wait_clocks = TRJ_WAIT_CLOCKS;  // limit of the pair kernel's waits for staged chunks
+    int stall_test = 0;
     int dim = 3;                // 2: frames in the xy plane (z = 0); z is neither clipped nor split
     float deltar = 0.f, rcrdf_eff = 0.f, side2 = 0.f;
     int64_t n_max = 0;
     int ncell_cap = 0;
     int nc[3] = {1, 1, 1};
     int32_t* ccount = nullptr;  // ncell_cap
-    int32_t* cflag = nullptr;   // ncell_cap: cell holds a coordinate outside [0, L)
+    int32_t* cflag = nullptr;   // ncell_cap: bit 0 a coordinate outside [0, L), bit 1 outside [-L, L)
     unsigned long long* work = nullptr;  // item counter of the pair kernel
     int32_t* cstart = nullptr;  // ncell_cap + 1
     int64_t fine_cap = 0;       // capacity of the per-(cell, sub-cell) arrays
@@ -912,6 +931,8 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     P.inv_deltar = 1.0f / plan->deltar;
     P.lsmax = plan->lsmax;
     P.floor_bins = plan->floor_bins;
+    P.wait_clocks = plan->wait_clocks;
+    P.stall_test = plan->stall_test;
     P.nsp = plan->nsp;
     P.nit = plan->nit;
     cells_for(box, plan->side2, P.nc, plan->dim);
@@ -1061,5 +1082,15 @@ extern "C" int trj_rdf_s2n(trj_rdf_plan* plan, int nrandom, uint64_t* gi_dev, ui
 extern "C" int trj_rdf_plan_set_binning(trj_rdf_plan* plan, int floor_bins) {
     if (!plan) return TRJ_ERR_INVALID;
     plan->floor_bins = floor_bins ? 1 : 0;
+    return TRJ_OK;
+}
+
+extern "C" int trj_rdf_plan_set_wait(trj_rdf_plan* plan, int64_t clocks, int stall_test) {
+    if (!plan) return TRJ_ERR_INVALID;
+    if (clocks != 0 && (clocks < 1000 || clocks > TRJ_WAIT_CLOCKS))
+        return trj_fail(plan->ctx, TRJ_ERR_INVALID, "trj_rdf_plan_set_wait: clocks %lld outside [1000, %lld] (0: default)",
+                        (long long)clocks, (long long)TRJ_WAIT_CLOCKS);
+    plan->wait_clocks = clocks ? clocks : TRJ_WAIT_CLOCKS;
+    plan->stall_test = stall_test ? 1 : 0;
     return TRJ_OK;
 }

@@ -149,7 +149,7 @@ __device__ __forceinline__ void trj_mbar_arrive(uint64_t* bar) {
 // Returns true once phase `parity` of the barrier has completed; false after TRJ_WAIT_CLOCKS
 // (caller raises TRJ_DEV_TIMEOUT and leaves).  try_wait with a suspend-time hint parks the thread
 // in hardware until the phase completes, so a waiting warp issues no polling instructions.
-__device__ __forceinline__ bool trj_mbar_wait(uint64_t* bar, unsigned parity) {
+__device__ __forceinline__ bool trj_mbar_wait_limit(uint64_t* bar, unsigned parity, long long limit) {
     const uint32_t addr = trj_smem_addr(bar);
     const long long t0 = clock64();
     while (true) {
@@ -162,8 +162,12 @@ __device__ __forceinline__ bool trj_mbar_wait(uint64_t* bar, unsigned parity) {
             : "r"(addr), "r"(parity), "r"(TRJ_SUSPEND_NS)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > TRJ_WAIT_CLOCKS) return false;
+        if (clock64() - t0 > limit) return false;
     }
+}
+
+__device__ __forceinline__ bool trj_mbar_wait(uint64_t* bar, unsigned parity) {
+    return trj_mbar_wait_limit(bar, parity, TRJ_WAIT_CLOCKS);
 }
 
 // 1-D bulk copy global -> shared (TMA engine, no multicast), completion on `bar`.

@@ -146,6 +146,12 @@ class RdfPlan:
         check(self.ctx.lib.trj_rdf_plan_set_binning(self.h, 1 if floor_bins else 0), self.ctx.h,
               "trj_rdf_plan_set_binning")
 
+    def set_wait(self, clocks: int = 0, stall_test: bool = False) -> None:
+        """Limit (SM clocks, 0 = default) of the pair kernel's waits for staged chunks; stall_test makes
+        every launch run out of it once (see trj_rdf_plan_set_wait)."""
+        check(self.ctx.lib.trj_rdf_plan_set_wait(self.h, int(clocks), 1 if stall_test else 0), self.ctx.h,
+              "trj_rdf_plan_set_wait")
+
     def new_s2n(self):
         """(gi, g2i): uint64 [lsmax+1] sums of N_k and N_k^2 over sample points and frames."""
         dev = self.ctx.torch_device

@@ -13,7 +13,10 @@ parameters.  The loop:
   requests with several frames replay a CUDA graph of the per-frame launch sequence
   after the first frame (double-buffered pinned input);
 * on the last frame reads the accumulated counts and sums back, normalises them on the
-  host, stamps the latency and frees the slot for the next request.
+  host, stamps the latency and frees the slot for the next request;
+* ``cancel(rid)`` (from any thread) drops a request that is still waiting, or stops a running one
+  after the frames already on its stream: once they have finished its plans, slot and HBM budget
+  are released and it yields no result (its id is listed in ``cancelled``).
 
 The S(Q) method of each (size, species) bucket is picked by a small autotuner that times
 the tensor-core and direct-sum paths once on the bucket's first request.
@@ -177,6 +180,7 @@ class _Job:
         self.graphs = [None, None]
         self.done_event = None
         self.footprint = 0
+        self.cancelled = False
 
 
 class Server:
@@ -195,6 +199,46 @@ class Server:
         self.in_use = 0
         self.peak_in_use = 0
         self.admission_waits = 0
+        self.cancelled: List[int] = []
+        self._cancel: set = set()
+        self._cancel_lock = threading.Lock()
+
+    def cancel(self, rid: int) -> None:
+        """Requests cancellation of request `rid` (thread-safe; takes effect at the loop's next turn)."""
+        with self._cancel_lock:
+            self._cancel.add(int(rid))
+
+    def _apply_cancels(self, pending, queue, jobs) -> None:
+        with self._cancel_lock:
+            want = set(self._cancel)
+        if not want:
+            return
+        done = set()
+        for dq in (pending, queue):
+            keep = [r for r in dq if r.rid not in want]
+            for r in dq:
+                if r.rid in want:
+                    self.cancelled.append(r.rid)
+                    done.add(r.rid)
+            dq.clear()
+            dq.extend(keep)
+        for job in jobs:
+            if job.req.rid in want and not job.cancelled:
+                # no further frames; the release waits for the frames already on the stream
+                job.cancelled = True
+                job.next_frame = len(job.req.frames)
+                job.done_event = torch.cuda.Event()
+                job.done_event.record(job.slot.stream)
+                done.add(job.req.rid)
+        with self._cancel_lock:
+            self._cancel -= done
+
+    def _release(self, job: _Job) -> None:
+        job.graphs = [None, None]
+        job.rdf.close()
+        job.sq.close()
+        self.in_use -= job.footprint
+        job.slot.req = None
 
     # ---- footprint / admission ---------------------------------------------------------
     def footprint(self, req: Request, ks: refsem.KSet, method: str) -> int:
@@ -301,16 +345,13 @@ class Server:
         sq = normalise_sq(out, job.ks, job.ntype, job.bsc, nconf)
         res = Result(rid=req.rid, hist=hist, sq_sums=out, rdf=rdf, sq=sq, method=job.method, arrival=req.arrival,
                      done=time.perf_counter() - t0, nframes=nconf)
-        job.graphs = [None, None]
-        job.rdf.close()
-        job.sq.close()
-        self.in_use -= job.footprint
-        job.slot.req = None
+        self._release(job)
         return res
 
     # ---- the loop ---------------------------------------------------------------------
-    def run(self, requests: Sequence[Request], realtime: bool = True) -> List[Result]:
-        """Serves `requests` (arrival times in seconds from now when realtime, else all at once)."""
+    def run(self, requests: Sequence[Request], realtime: bool = True, on_turn=None) -> List[Result]:
+        """Serves `requests` (arrival times in seconds from now when realtime, else all at once).
+        ``on_turn(server, turn)``, if given, is called at the start of every turn of the loop."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         queue: collections.deque = collections.deque()
         jobs: List[_Job] = []
@@ -319,7 +360,12 @@ class Server:
         if not realtime:
             for r in pending:
                 r.arrival = 0.0
+        turn = 0
         while pending or queue or jobs:
+            if on_turn is not None:
+                on_turn(self, turn)
+            turn += 1
+            self._apply_cancels(pending, queue, jobs)
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
@@ -346,7 +392,11 @@ class Server:
             still = []
             for job in jobs:
                 if job.done_event is not None and job.done_event.query():
-                    results.append(self._finish(job, t0))
+                    if job.cancelled:
+                        self._release(job)
+                        self.cancelled.append(job.req.rid)
+                    else:
+                        results.append(self._finish(job, t0))
                 else:
                     still.append(job)
             jobs = still
