@@ -61,11 +61,11 @@ constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
 constexpr int kMaxStages = 8;
 constexpr int kChunkAtoms = 12288;  // atom slots per chunk: the Z-table rows of one chunk are ~10 MB
 constexpr int kMaxTileCols = 224;
-// TMEM columns (512 allocated): accumulator at 0, running sum at 224, A half-stage buffers at 448
-// and 480 (16 columns of packed bf16 pairs for hi, then 16 for lo).
+// TMEM columns (512 allocated): the accumulator at 0 (bmax columns, the widest tile), the running sum
+// at bmax, then as many A half-stage buffers of 32 columns (16 of packed bf16 pairs for hi, then 16
+// for lo) as fit, up to kMaxABufs: 2 for bmax = 224, 3 for 208, 4 for <= 192.
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kSumCol = 224;
-constexpr uint32_t kACol = 448;
+constexpr int kMaxABufs = 4;
 // CTA-pair form: accumulator at 0, four full-stage A buffers (32 columns hi, 32 lo) from 224; its
 // FP32 running sum lives in shared memory.
 constexpr uint32_t kPairACol = 224;
@@ -98,6 +98,8 @@ struct TcParams {
     int stage_bytes;
     int bmax;  // B rows of a stage buffer
     int table_rows;  // Z-table rows per 32-slot block
+    uint32_t sum_col, a_col;  // TMEM columns of the running sum and of the first A buffer
+    int nabuf;                // A half-stage buffers
     unsigned* status;
 };
 
@@ -147,6 +149,7 @@ struct TcState {
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
+    int nabuf = 2;  // A half-stage buffers in TMEM
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
     // CTA-pair (cta_group::2) form
@@ -346,13 +349,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t full_a[2], empty_a[2], xy_full[2], xy_empty[2], acc_full, acc_empty, mma_done;
+    __shared__ __align__(8) uint64_t full_a[kMaxABufs], empty_a[kMaxABufs], xy_full[2], xy_empty[2], acc_full,
+        acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int NS = p.nstages;
+    const int NA = p.nabuf;
     const int F = p.flush_stages;
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
     // stage layout: B hi [bmax rows x 128 B], B lo, x/y phases of the stage's atoms
@@ -366,9 +371,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             trj_mbar_init(&full_b[s], 1);
             trj_mbar_init(&empty_b[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kMaxABufs; ++b) {
             trj_mbar_init(&full_a[b], kBuildWarps);
             trj_mbar_init(&empty_a[b], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
             trj_mbar_init(&xy_full[b], kXyWarps);
             trj_mbar_init(&xy_empty[b], kBuildWarps);
         }
@@ -449,8 +456,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
             const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
             const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
-            int slot = 0, fg = 0;
-            unsigned phase = 0, aphase = 0;  // B ring phase; A buffers flip every stage
+            int slot = 0, fg = 0, ab = 0;
+            unsigned phase = 0, aphase = 0;  // B ring phase; A ring (NA half-stage buffers) phase
             uint64_t bh = b0desc;            // B descriptor of the current slot
             for (int li = item0; li < item1 && !abort_flag; ++li) {
                 const int it = p.cta_items[li];
@@ -474,13 +481,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const uint64_t bl = bh + b_lo;
                     bool ok = true;
                     for (int hh = 0; hh < 2 && ok; ++hh) {
-                        const int hb = hh;
+                        const int hb = ab;
                         if (!timed_wait(&full_a[hb], aphase, p.status)) {
                             ok = false;
                             break;
                         }
                         tc_fence_after();
-                        const uint32_t ah = tmem + kACol + (uint32_t)(32 * hb), al = ah + 16;
+                        const uint32_t ah = tmem + p.a_col + (uint32_t)(32 * hb), al = ah + 16;
 #pragma unroll
                         for (int k2 = 0; k2 < 2; ++k2) {
                             const int kk = 2 * hh + k2;
@@ -489,6 +496,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
                         }
                         mma_commit(&empty_a[hb]);
+                        if (++ab == NA) {
+                            ab = 0;
+                            aphase ^= 1;
+                        }
                     }
                     if (!ok) {
                         abort_flag = 1;
@@ -500,7 +511,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         ++fg;
                         rs = 0;
                     }
-                    aphase ^= 1;
                     bh += b_step;
                     if (++slot == NS) {
                         slot = 0;
@@ -540,7 +550,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 tc_fence_after();
                 const bool last = f == nflush - 1;
-                const uint32_t ta = tmem + lanes, ts = tmem + lanes + kSumCol;
+                const uint32_t ta = tmem + lanes, ts = tmem + lanes + p.sum_col;
                 for (int c = c0; c < T.ncols; c += 32) {  // ncols is a multiple of 16
                     uint32_t a0[16], s0[16];
                     tmem_ld16_nowait(ta + (uint32_t)c, a0);
@@ -611,7 +621,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int m = 32 * q + lane;
         const int nxl = m & 15, nyl = m >> 4;
         const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        int sg = 0;
+        int sg = 0, ab = 0;
+        unsigned aphase = 0;  // A ring (NA half-stage buffers), in the MMA warp's order
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
@@ -629,8 +640,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const ulonglong2* xs = reinterpret_cast<const ulonglong2*>(xy_ptr(xb));
                 const ulonglong2* ys = xs + kStageSlots * kTcTileNx;
                 for (int hh = 0; hh < 2; ++hh) {
-                    const int hg = 2 * sg + hh, hb = hg & 1;
-                    if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], ((hg >> 1) & 1) ^ 1))) {
+                    const int hb = ab;
+                    if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], aphase ^ 1))) {
                         if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                         abort_flag = 1;
                         stop = true;
@@ -643,13 +654,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         const int j = 16 * hh + 8 * g + jj;
                         product_split(xs[j * kTcTileNx + nxl], ys[j * kTcTileNy + nyl], hw[jj], lw[jj]);
                     }
-                    const uint32_t ta = tmem + lanes + kACol + (uint32_t)(32 * hb + 8 * g);
+                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + 8 * g);
                     tmem_st8(ta, hw);
                     tmem_st8(ta + 16, lw);
                     tmem_wait_st();
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) trj_mbar_arrive(&full_a[hb]);
+                    if (++ab == NA) {
+                        ab = 0;
+                        aphase ^= 1;
+                    }
                 }
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_empty[xb]);
@@ -1292,6 +1307,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile of %d columns > %d", st->bmax, kMaxTileCols);
     st->nz_min = nz_min;
     st->table_rows = 2 * (nz_max - nz_min + 1);
+    st->nabuf = std::min(kMaxABufs, (int)(kTmemCols - 2 * st->bmax) / 32);  // bmax <= 224: at least 2
     const int ntiles = (int)plan->tiles.size();
     std::vector<TcTile> tt(ntiles);
     int64_t acc = 0;
@@ -1449,6 +1465,9 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.stage_bytes = st->stage_bytes;
     P.bmax = st->bmax;
     P.table_rows = st->table_rows;
+    P.sum_col = (uint32_t)st->bmax;
+    P.a_col = (uint32_t)(2 * st->bmax);
+    P.nabuf = st->nabuf;
     P.status = ctx->status_dev;
     // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
