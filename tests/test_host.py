@@ -185,6 +185,20 @@ def test_netcdf_roundtrip(tmp_path):
         assert np.array_equal(a.box, b.box)
 
 
+def test_netcdf4_file_refused_with_conversion_hint(tmp_path):
+    """A NETCDF4 (HDF5) trajectory, the format of tools/lammpstrj_to_netcdf.py:28, needs netCDF4;
+    without it the reader names the conversion to the classic 64-bit-offset format."""
+    p = tmp_path / "t4.nc"
+    p.write_bytes(frames.NetCDFTrajectory.HDF5_SIGNATURE + bytes(64))
+    try:
+        import netCDF4  # noqa: F401
+        pytest.skip("netCDF4 is installed: the file would be read by it")
+    except ImportError:
+        pass
+    with pytest.raises(ValueError, match="nccopy -k 64-bit-offset"):
+        frames.open_trajectory(str(p))
+
+
 def test_linear_kset_counts():
     box = np.array([20.0, 20.0, 20.0], F32)
     ks = refsem.linear_kset(box, 2 * np.pi / 20.0, 2.0, 10)

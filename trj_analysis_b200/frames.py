@@ -199,8 +199,13 @@ class NetCDFTrajectory:
     """AMBER-convention trajectory (``coordinates``, ``cell_lengths``, optional ``type``, ``q`` and
     ``time`` with its ``units`` and ``scale_factor`` attributes, read as netcdf.f90:432-448 does).
 
-    Uses netCDF4 when importable, else scipy's reader for classic CDF-1/2 files.
+    Uses netCDF4 when importable (every netCDF format), else scipy's reader for the classic
+    formats CDF-1 and CDF-2 (64-bit offset).  A NETCDF4 (HDF5-based) file, as the reference's
+    tools/lammpstrj_to_netcdf.py writes, needs netCDF4; without it the file is refused with the
+    conversion command (netCDF-C's ``nccopy -k 64-bit-offset``) in the message.
     """
+
+    HDF5_SIGNATURE = b"\x89HDF\r\n\x1a\n"
 
     def __init__(self, path: str):
         self._ds = None
@@ -209,6 +214,13 @@ class NetCDFTrajectory:
             self._ds = Dataset(path)
             self._v = self._ds.variables
         except ImportError:
+            with open(path, "rb") as f:
+                head = f.read(8)
+            if head == self.HDF5_SIGNATURE:
+                raise ValueError(
+                    f"{path}: a NETCDF4 (HDF5) file, which needs the netCDF4 package (not installed). Convert it "
+                    f"to the 64-bit-offset classic format with 'nccopy -k 64-bit-offset {path} out.nc', or write "
+                    f"it with format=\"NETCDF3_64BIT_OFFSET\" in the converter")
             from scipy.io import netcdf_file
             self._ds = netcdf_file(path, "r", mmap=False)
             self._v = self._ds.variables
