@@ -54,8 +54,8 @@ constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
 constexpr int kMmaWarp = kTmaWarp + 1;             // 21
 constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
-constexpr int kXBytes = kStageSlots * kTcTileNx * 16;  // 32 atoms x 16 X factors as (xr, xr, xi, xi)
-constexpr int kYBytes = kStageSlots * kTcTileNy * 16;  // 32 atoms x 8 Y factors as (yr, yi, -yi, yr)
+constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // X factors [16 nx][32 atoms] as (xr, xi)
+constexpr int kYBytes = kStageSlots * kTcTileNy * 8;  // Y factors [8 ny][32 atoms] as (yr, yi)
 constexpr int kXyBytes = kXBytes + kYBytes;           // one of the two X/Y buffers
 constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
 constexpr int kMaxStages = 8;
@@ -236,34 +236,47 @@ __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.
 
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
-// Packed FP32 pairs (sm_100 f32x2 arithmetic, round to nearest): low word = first value.
-__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
+// e^{i pi f} for the fixed-point phase ph (f = ph / 2^31 in [-1, 1)).
+__device__ __forceinline__ float2 phase_factor(unsigned ph) {
+    float s, c;
+    sincospif(__int2float_rn((int)ph) * 4.656612873077393e-10f, &s, &c);
+    return make_float2(c, s);
 }
 
-__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
-__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
-// A = X * Y from the packed smem forms X = ((xr, xr), (xi, xi)), Y = ((yr, yi), (-yi, yr)):
-// (ar, ai) = (xr, xr) * (yr, yi) + (xi, xi) * (-yi, yr); then the hi/lo BF16 split of (ar, ai).
-__device__ __forceinline__ void product_split(ulonglong2 x, ulonglong2 y, uint32_t& hi, uint32_t& lo) {
-    const uint64_t r = f2_fma(x.x, y.x, f2_mul(x.y, y.y));
-    const uint32_t h = bf2_bits(__floats2bfloat162_rn(__uint_as_float((uint32_t)r), __uint_as_float((uint32_t)(r >> 32))));
-    const uint64_t hf = ((uint64_t)(h & 0xffff0000u) << 32) | (uint64_t)(h << 16);
-    const uint64_t d = f2_sub(r, hf);  // exact: r minus its 8-bit rounding
+// A = X * Y: (ar, ai) = (xr yr - xi yi, xr yi + xi yr), each rounded once after the first product,
+// then the hi/lo BF16 split of (ar, ai) (low half of each word: ar).
+__device__ __forceinline__ void product_split(float xr, float xi, float yr, float yi, uint32_t& hi, uint32_t& lo) {
+    const float ar = __fmaf_rn(xr, yr, -__fmul_rn(xi, yi));
+    const float ai = __fmaf_rn(xr, yi, __fmul_rn(xi, yr));
+    const uint32_t h = bf2_bits(__floats2bfloat162_rn(ar, ai));
+    const float dr = __fsub_rn(ar, __uint_as_float(h << 16));  // exact: ar minus its 8-bit rounding
+    const float di = __fsub_rn(ai, __uint_as_float(h & 0xffff0000u));
     hi = h;
-    lo = bf2_bits(__floats2bfloat162_rn(__uint_as_float((uint32_t)d), __uint_as_float((uint32_t)(d >> 32))));
+    lo = bf2_bits(__floats2bfloat162_rn(dr, di));
+}
+
+// X/Y buffer: X factors [16 nx][32 atoms], then Y factors [8 ny][32 atoms], each (re, im).  Consecutive
+// threads take consecutive atoms of one nx (ny): each thread reads its atom's phases once per factor.
+__device__ __forceinline__ void fill_xy(float2* xs, const uint2* u, int nx0, int ny0, int xt) {
+    float2* ys = xs + kTcTileNx * kStageSlots;
+    for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32)
+        xs[e] = phase_factor((unsigned)(nx0 + (e >> 5)) * u[e & (kStageSlots - 1)].x);
+    for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32)
+        ys[e] = phase_factor((unsigned)(ny0 + (e >> 5)) * u[e & (kStageSlots - 1)].y);
+}
+
+// The hi and lo BF16 pairs of A for row (nxl, nyl) and atoms j0 .. j0 + 7 of the stage (j0 a multiple of
+// 8): every 16-byte load carries two atoms' factors that this lane uses.
+__device__ __forceinline__ void build8(const float2* xs, int nxl, int nyl, int j0, uint32_t (&hw)[8],
+                                       uint32_t (&lw)[8]) {
+    const float4* xr = reinterpret_cast<const float4*>(xs + nxl * kStageSlots + j0);
+    const float4* yr = reinterpret_cast<const float4*>(xs + (kTcTileNx + nyl) * kStageSlots + j0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 x = xr[k], y = yr[k];
+        product_split(x.x, x.y, y.x, y.y, hw[2 * k], lw[2 * k]);
+        product_split(x.z, x.w, y.z, y.w, hw[2 * k + 1], lw[2 * k + 1]);
+    }
 }
 
 // hi/lo BF16 split of a pair (one value in each half of the 32-bit word, low half first).
@@ -273,13 +286,6 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t&
     __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
     hi = bf2_bits(h);
     lo = bf2_bits(l);
-}
-
-// e^{i pi f} for the fixed-point phase ph (f = ph / 2^31 in [-1, 1)).
-__device__ __forceinline__ float2 phase_factor(unsigned ph) {
-    float s, c;
-    sincospif(__int2float_rn((int)ph) * 4.656612873077393e-10f, &s, &c);
-    return make_float2(c, s);
 }
 
 __device__ __forceinline__ bool timed_wait(uint64_t* bar, unsigned parity, unsigned* status) {
@@ -362,8 +368,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
     // stage layout: B hi [bmax rows x 128 B], B lo, x/y phases of the stage's atoms
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
-    // X/Y buffer b: [32 atoms][16 nx] X factors, then [32 atoms][8 ny] Y factors
-    auto xy_ptr = [&](int b) { return reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
+    // X/Y buffer b: [16 nx][32 atoms] X factors, then [8 ny][32 atoms] Y factors (fill_xy)
+    auto xy_ptr = [&](int b) { return reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
 
     if (tid == 0) {
         abort_flag = 0;
@@ -596,16 +602,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128);
-                float4* xs = xy_ptr(xb);
-                float4* ys = xs + kStageSlots * kTcTileNx;
-                for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32) {
-                    const float2 f = phase_factor((unsigned)(T.nx0 + (e & 15)) * u[e >> 4].x);
-                    xs[e] = make_float4(f.x, f.x, f.y, f.y);
-                }
-                for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32) {
-                    const float2 f = phase_factor((unsigned)(T.ny0 + (e & 7)) * u[e >> 3].y);
-                    ys[e] = make_float4(f.x, f.y, -f.y, f.x);
-                }
+                fill_xy(xy_ptr(xb), u, T.nx0, T.ny0, xt);
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
                 if (++slot == NS) {
@@ -637,8 +634,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     stop = true;
                     break;
                 }
-                const ulonglong2* xs = reinterpret_cast<const ulonglong2*>(xy_ptr(xb));
-                const ulonglong2* ys = xs + kStageSlots * kTcTileNx;
+                const float2* xs = xy_ptr(xb);
                 for (int hh = 0; hh < 2; ++hh) {
                     const int hb = ab;
                     if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], aphase ^ 1))) {
@@ -649,11 +645,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     }
                     tc_fence_after();
                     uint32_t hw[8], lw[8];
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj) {
-                        const int j = 16 * hh + 8 * g + jj;
-                        product_split(xs[j * kTcTileNx + nxl], ys[j * kTcTileNy + nyl], hw[jj], lw[jj]);
-                    }
+                    build8(xs, nxl, nyl, 16 * hh + 8 * g, hw, lw);
                     const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + 8 * g);
                     tmem_st8(ta, hw);
                     tmem_st8(ta + 16, lw);
@@ -785,7 +777,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int F = p.flush_stages;
     const int item0 = p.cl_off[cl], item1 = p.cl_off[cl + 1];
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
-    auto xy_ptr = [&](int b) { return reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
+    auto xy_ptr = [&](int b) { return reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
     // FP32 running sum of this CTA's 128 accumulator rows: [16-column chunk][4 x 4 columns][row] float4
     float4* sums = reinterpret_cast<float4*>(smem + (size_t)NS * p.stage_bytes + 2 * kXyBytes);
 
@@ -1027,16 +1019,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bhalf * 128);
-                float4* xs = xy_ptr(xb);
-                float4* ys = xs + kStageSlots * kTcTileNx;
-                for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32) {
-                    const float2 f = phase_factor((unsigned)(nx0 + (e & 15)) * u[e >> 4].x);
-                    xs[e] = make_float4(f.x, f.x, f.y, f.y);
-                }
-                for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32) {
-                    const float2 f = phase_factor((unsigned)(ny0 + (e & 7)) * u[e >> 3].y);
-                    ys[e] = make_float4(f.x, f.y, -f.y, f.x);
-                }
+                fill_xy(xy_ptr(xb), u, nx0, ny0, xt);
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
                 if (++slot == NS) {
@@ -1070,17 +1053,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                const ulonglong2* xs = reinterpret_cast<const ulonglong2*>(xy_ptr(xb));
-                const ulonglong2* ys = xs + kStageSlots * kTcTileNx;
+                const float2* xs = xy_ptr(xb);
                 const uint32_t ta = tmem + lanes + kPairACol + (uint32_t)(64 * ab + 16 * g);
 #pragma unroll
                 for (int h8 = 0; h8 < 2; ++h8) {
                     uint32_t hw[8], lw[8];
-#pragma unroll
-                    for (int jj = 0; jj < 8; ++jj) {
-                        const int j = 16 * g + 8 * h8 + jj;
-                        product_split(xs[j * kTcTileNx + nxl], ys[j * kTcTileNy + nyl], hw[jj], lw[jj]);
-                    }
+                    build8(xs, nxl, nyl, 16 * g + 8 * h8, hw, lw);
                     tmem_st8(ta + 8 * h8, hw);
                     tmem_st8(ta + 32 + 8 * h8, lw);
                 }
