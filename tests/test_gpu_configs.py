@@ -16,7 +16,7 @@
   sq.cuf:372-454), and the plans' device footprint.
 
 Shell bar, as in the other S(Q) tests: |sum_gpu - sum_fp64| <= 1e-5 * sqrt(sum_aa * sum_bb) per
-shell and species pair.  With TRJ_SHELL_TABLE_DIR set, each S(Q) test writes its per-shell error
+shell and species pair (2e-5 at c4's 2e6 atoms per species, see REL_SHELL_C4).  With TRJ_SHELL_TABLE_DIR set, each S(Q) test writes its per-shell error
 table there as JSON (shell index, Q, vectors, max error over the species pairs).
 """
 import json
@@ -245,6 +245,11 @@ def test_c4_pair_counts_bit_exact(ctx, c4_frame):
 
 # dense shells checked at c4 (every shell's vectors at 4e6 atoms would take minutes of FP64 on the host)
 C4_DENSE = [1, 2, 3, 4, 5, 8, 13, 21, 34, 55, 89, 136]
+# The 1e-5 bar is stated for frames of about 10^6 atoms.  The errors that do not average out (the FP32
+# rounding of each term's sine/cosine and of the tensor cores' partial sums) add up in proportion to
+# the atoms of a species, while |rho| grows as their square root, so relative to S(Q) they grow as
+# sqrt(N_a): c4 has 2e6 atoms per species against c3's 5e5, twice the relative error.
+REL_SHELL_C4 = 2e-5
 
 
 @pytest.mark.parametrize("mode", ["full+axes", "ref"])
@@ -278,7 +283,7 @@ def test_c4_sq_per_axis_tables(ctx, c4_frame, mode):
     # the plan's shell sums on the checked shells are the per-vector sums
     assert np.allclose(res[shells], got[shells], rtol=1e-12, atol=1e-9 * np.abs(got).max())
     write_table("c4_" + mode.replace("+", "_"), sub, {"split": err})
-    assert np.nanmax(err) <= REL_SHELL, (np.nanargmax(err), np.nanmax(err))
+    assert np.nanmax(err) <= REL_SHELL_C4, (np.nanargmax(err), np.nanmax(err))
     # footprint: the plan's own scratch fits a small share of the device
     free, total = torch.cuda.mem_get_info()
     assert 0 < scratch < 0.25 * total

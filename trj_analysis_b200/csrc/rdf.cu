@@ -55,6 +55,7 @@ struct RdfParams {
     int fast_ok;                // every axis split into >= 5 cells
     float cull2;                // (cutoff * (1 + 2^-10))^2: neighbours farther from a warp's box are skipped
     float cull_pad;             // added to the box half-widths: covers the FP32 rounding of the cull test
+    int sbits;                  // sub-cells per cell axis: 2^sbits (Morton order inside a cell)
     long long wait_clocks;      // limit of a warp's wait for a staged neighbour chunk
     int stall_test;             // 1: each warp's first wait is on a barrier nothing arrives on (timeout test)
     int off[kMaxOffsets][3];
@@ -72,6 +73,8 @@ struct TaskInfo {
     int cull;          // both cells hold only coordinates in [-L, L): the box cull applies (wrapped values)
     float img[3];      // periodic image of the neighbour cell: 0 or -+L per axis
     int valid;         // 0 = no more tasks
+    int oct;           // 1: warp w's homes are octant w of the home cell (ostart[w] .. ostart[w + 1])
+    short ostart[9];   // octant starts within the home cell (oct = 1)
 };
 
 __device__ __forceinline__ float min_image_exact(float d, float L) {
@@ -107,9 +110,27 @@ struct TaskGen {
 
 __device__ __forceinline__ int wrapc(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
 
+// Octant starts of cell c (atoms sa .. sa + na of the sorted array) from the sub-cell starts; returns 1
+// when no octant holds more than 64 atoms.  Not inlined: it runs on the refill path only, and its
+// loads would otherwise add to the register pressure of the pair loop.
+__device__ __noinline__ int octant_starts(const int32_t* __restrict__ fstart, int c, int sa, int na, int sbits,
+                                          short* ostart) {
+    const int64_t kb = (int64_t)c << (3 * sbits);
+    const int step = 1 << (3 * (sbits - 1));
+    int mx = 0, prev = 0;
+    ostart[0] = 0;
+    for (int o = 1; o <= 8; ++o) {
+        const int v = o < 8 ? fstart[kb + o * step] - sa : na;
+        ostart[o] = (short)v;
+        mx = max(mx, v - prev);
+        prev = v;
+    }
+    return mx <= 64;
+}
+
 __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restrict__ cstart,
                           const int32_t* __restrict__ ccount, const int32_t* __restrict__ cflag,
-                          unsigned long long* work, TaskInfo& t) {
+                          const int32_t* __restrict__ fstart, unsigned long long* work, TaskInfo& t) {
     for (;;) {
         if (!g.started) {
             g.started = 1;
@@ -165,6 +186,10 @@ __device__ bool next_task(TaskGen& g, const RdfParams& p, const int32_t* __restr
             t.img[1] = ey < 0 ? -p.L[1] : (ey >= p.nc[1] ? p.L[1] : 0.f);
             t.img[2] = ez < 0 ? -p.L[2] : (ez >= p.nc[2] ? p.L[2] : 0.f);
             t.valid = 1;
+            // Octant homes: a cell of one home round whose eight Morton octants (sub-cell keys
+            // o * 8^(sbits-1) ..) each hold at most 64 atoms gives warp w octant w, a box of half the
+            // cell edge, instead of 64 consecutive atoms that may span two octants.
+            t.oct = (p.sbits >= 1 && na <= kHomeChunk) ? octant_starts(fstart, c, t.sa, na, p.sbits, t.ostart) : 0;
             g.jc += 1;
             return true;
         }
@@ -288,12 +313,10 @@ __device__ __forceinline__ unsigned after_mask(int lim, int jj0) {
 // SELF: home and neighbour cell are the same cell (pairs need j > i within it).
 template <bool FAST, bool SELF, bool FLOOR, bool QMODE>
 __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* __restrict__ bj, const float4& a0,
-                                             const float4& a1, bool h0, bool h1, int il0, int s0, int s1,
+                                             const float4& a1, bool h0, bool h1, int il0, int il0w, int s0, int s1,
                                              unsigned lane, const RdfParams& p, const int* rowtab, unsigned* myhist,
                                              PairCounters& pc, double* myq, float qa0, float qa1, const float* qj,
                                              WarpBox* wb) {
-    const int il0w = il0 - (int)lane;  // the warp's first home atom
-    if (il0w >= ti.na) return 0u;
     if (ti.cull) {
         float cx, cy, cz, hx, hy, hz;
         axis_box(wrap_cull(a0.x, p.L[0]), h0, wrap_cull(a1.x, p.L[0]), h1, p.nc[0] > 1, ti.img[0], p.cull_pad, cx, hx);
@@ -336,11 +359,12 @@ __device__ __forceinline__ unsigned run_task(const TaskInfo& ti, const float4* _
 // arrival with valid = 0 when the work is exhausted (readers of that phase leave the task loop).
 __device__ __forceinline__ void refill_slot(int slot, TaskGen& gen, const RdfParams& p,
                                             const int32_t* __restrict__ cstart, const int32_t* __restrict__ ccount,
-                                            const int32_t* __restrict__ cflag, unsigned long long* work,
+                                            const int32_t* __restrict__ cflag, const int32_t* __restrict__ fstart,
+                                            unsigned long long* work,
                                             const float4* __restrict__ sorted, TaskInfo* tinfo, uint64_t* bars,
                                             unsigned* phases, float4* buf) {
     TaskInfo nx;
-    const bool ok = next_task(gen, p, cstart, ccount, cflag, work, nx);
+    const bool ok = next_task(gen, p, cstart, ccount, cflag, fstart, work, nx);
     tinfo[slot] = nx;
     phases[slot] += 1u;
     if (ok) {
@@ -362,6 +386,7 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
                                                              const int32_t* __restrict__ cstart,
                                                              const int32_t* __restrict__ ccount,
                                                              const int32_t* __restrict__ cflag,
+                                                             const int32_t* __restrict__ fstart,
                                                              unsigned long long* __restrict__ work,
                                                              unsigned long long* __restrict__ hist_g,
                                                              unsigned long long* __restrict__ edge_g,
@@ -404,7 +429,7 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         }
         trj_mbar_init(&never, 1);
         trj_fence_mbar_init();
-        for (int sl = 0; sl < kSlots; ++sl) refill_slot(sl, gen, p, cstart, ccount, cflag, work, sorted, tinfo, bars, phases, buf);
+        for (int sl = 0; sl < kSlots; ++sl) refill_slot(sl, gen, p, cstart, ccount, cflag, fstart, work, sorted, tinfo, bars, phases, buf);
     }
     __syncthreads();
     PairCounters pc;
@@ -428,26 +453,31 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
         }
         const TaskInfo ti = tinfo[slot];
         if (!ti.valid) break;
-        const int il0 = ti.hc * kHomeChunk + 64 * warp + (int)lane, il1 = il0 + 32;
+        // The warp's home atoms [hbeg, hend) within the cell: its octant, or 64 consecutive atoms of the round.
+        const int hbeg = ti.oct ? (int)tinfo[slot].ostart[warp] : ti.hc * kHomeChunk + 64 * warp;
+        const int hend = ti.oct ? (int)tinfo[slot].ostart[warp + 1] : min(ti.na, hbeg + 64);
+        const int il0 = hbeg + (int)lane, il1 = il0 + 32;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 a0 = il0 < ti.na ? sorted[ti.sa + il0] : z4;
-        const float4 a1 = il1 < ti.na ? sorted[ti.sa + il1] : z4;
+        const float4 a0 = il0 < hend ? sorted[ti.sa + il0] : z4;
+        const float4 a1 = il1 < hend ? sorted[ti.sa + il1] : z4;
         const int s0 = __float_as_int(a0.w), s1 = __float_as_int(a1.w);
         // A species outside 0..nsp-1 can only come from a frame already flagged as bad data.
-        const bool h0 = il0 < ti.na && (unsigned)s0 < (unsigned)p.nsp;
-        const bool h1 = il1 < ti.na && (unsigned)s1 < (unsigned)p.nsp;
-        const float qa0 = (QMODE && il0 < ti.na) ? sorted_q[ti.sa + il0] : 0.f;
-        const float qa1 = (QMODE && il1 < ti.na) ? sorted_q[ti.sa + il1] : 0.f;
+        const bool h0 = il0 < hend && (unsigned)s0 < (unsigned)p.nsp;
+        const bool h1 = il1 < hend && (unsigned)s1 < (unsigned)p.nsp;
+        const float qa0 = (QMODE && il0 < hend) ? sorted_q[ti.sa + il0] : 0.f;
+        const float qa1 = (QMODE && il1 < hend) ? sorted_q[ti.sa + il1] : 0.f;
         const float* qj = QMODE ? sorted_q + ti.sb : nullptr;
         const float4* bj = buf + slot * kJChunk;
         WarpBox* wb = &wboxes[warp];
 #define TRJ_RUN(F, S)                                                                                       \
-    run_task<F, S, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, s0, s1, lane, p, rowtab, myhist, pc, myq, qa0, qa1, qj, \
-                                 wb)
-        if (ti.fast)
-            n_tested += ti.self ? TRJ_RUN(true, true) : TRJ_RUN(true, false);
-        else
-            n_tested += ti.self ? TRJ_RUN(false, true) : TRJ_RUN(false, false);
+    run_task<F, S, FLOOR, QMODE>(ti, bj, a0, a1, h0, h1, il0, hbeg, s0, s1, lane, p, rowtab, myhist, pc, myq, qa0, \
+                                 qa1, qj, wb)
+        if (hbeg < hend) {  // warp-uniform: the warp has home atoms in this task
+            if (ti.fast)
+                n_tested += ti.self ? TRJ_RUN(true, true) : TRJ_RUN(true, false);
+            else
+                n_tested += ti.self ? TRJ_RUN(false, true) : TRJ_RUN(false, false);
+        }
 #undef TRJ_RUN
         // Release the slot; the last warp refills it.
         __syncwarp();
@@ -456,7 +486,7 @@ __global__ void __launch_bounds__(kThreads, 4) rdf_pairs_kernel(RdfParams p, con
             if (atomicAdd(&released[slot], 1u) == kThreads / 32 - 1) {
                 released[slot] = 0u;
                 __threadfence_block();
-                refill_slot(slot, gen, p, cstart, ccount, cflag, work, sorted, tinfo, bars, phases, buf);
+                refill_slot(slot, gen, p, cstart, ccount, cflag, fstart, work, sorted, tinfo, bars, phases, buf);
             }
         }
         __syncwarp();
@@ -996,8 +1026,8 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     if (nrep < 1) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "rdf accumulate: histogram too large");
     P.nrep = nrep;
     size_t smem = stage + (size_t)nrep * hist_bytes;
-    void (*kern)(RdfParams, const float4*, const int32_t*, const int32_t*, const int32_t*, unsigned long long*,
-                 unsigned long long*, unsigned long long*, unsigned*, const float*, double*) =
+    void (*kern)(RdfParams, const float4*, const int32_t*, const int32_t*, const int32_t*, const int32_t*,
+                 unsigned long long*, unsigned long long*, unsigned long long*, unsigned*, const float*, double*) =
         plan->floor_bins ? (charged ? rdf_pairs_kernel<true, true> : rdf_pairs_kernel<true, false>)
                          : (charged ? rdf_pairs_kernel<false, true> : rdf_pairs_kernel<false, false>);
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1008,6 +1038,7 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     int sbits = per_cell >= 128.0 ? 2 : (per_cell >= 16.0 ? 1 : 0);
     while (sbits > 0 && ((int64_t)P.ncell << (3 * sbits)) > plan->fine_cap) --sbits;
     const int nkey = P.ncell << (3 * sbits);
+    P.sbits = sbits;
 
     // Cell binning: count, scan over cells, sub-cell offsets, scatter.
     TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->fcount, 0, sizeof(int32_t) * nkey, s));
@@ -1026,7 +1057,8 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     if (charged) TRJ_CUDA_TRY(ctx, cudaMemsetAsync(plan->gqq_frame, 0, sizeof(double) * plan->lsmax, s));
     int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * ctas_per_sm, P.nitems);
     plan->timer.begin(ctx, s);
-    kern<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->work,
+    kern<<<(unsigned)grid, kThreads, smem, s>>>(P, plan->sorted, plan->cstart, plan->ccount, plan->cflag, plan->fstart,
+                                                plan->work,
                                                 (unsigned long long*)hist_dev, (unsigned long long*)edge_dev,
                                                 ctx->status_dev, charged ? plan->sorted_q : nullptr,
                                                 charged ? plan->gqq_frame : nullptr);

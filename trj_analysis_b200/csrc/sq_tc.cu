@@ -54,8 +54,11 @@ constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
 constexpr int kMmaWarp = kTmaWarp + 1;             // 21
 constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
-constexpr int kXBytes = kStageSlots * kTcTileNx * 8;  // X factors [16 nx][32 atoms] as (xr, xi)
-constexpr int kYBytes = kStageSlots * kTcTileNy * 8;  // Y factors [8 ny][32 atoms] as (yr, yi)
+// X/Y factor rows: 32 atoms as (re, im) plus 2 pad entries, so that rows start 272 bytes (68 banks)
+// apart and the 16-byte loads of eight lanes on eight different rows fall in different banks.
+constexpr int kXyRow = kStageSlots + 2;
+constexpr int kXBytes = kXyRow * kTcTileNx * 8;  // X factors [16 nx][kXyRow] as (xr, xi)
+constexpr int kYBytes = kXyRow * kTcTileNy * 8;  // Y factors [8 ny][kXyRow] as (yr, yi)
 constexpr int kXyBytes = kXBytes + kYBytes;           // one of the two X/Y buffers
 constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
 constexpr int kMaxStages = 8;
@@ -255,22 +258,23 @@ __device__ __forceinline__ void product_split(float xr, float xi, float yr, floa
     lo = bf2_bits(__floats2bfloat162_rn(dr, di));
 }
 
-// X/Y buffer: X factors [16 nx][32 atoms], then Y factors [8 ny][32 atoms], each (re, im).  Consecutive
-// threads take consecutive atoms of one nx (ny): each thread reads its atom's phases once per factor.
+// X/Y buffer: X factors [16 nx][kXyRow], then Y factors [8 ny][kXyRow], each (re, im) per atom.
+// Consecutive threads take consecutive atoms of one nx (ny): each thread reads its atom's phases once per
+// factor, and a warp's stores cover one row.
 __device__ __forceinline__ void fill_xy(float2* xs, const uint2* u, int nx0, int ny0, int xt) {
-    float2* ys = xs + kTcTileNx * kStageSlots;
+    float2* ys = xs + kTcTileNx * kXyRow;
     for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32)
-        xs[e] = phase_factor((unsigned)(nx0 + (e >> 5)) * u[e & (kStageSlots - 1)].x);
+        xs[(e >> 5) * kXyRow + (e & 31)] = phase_factor((unsigned)(nx0 + (e >> 5)) * u[e & (kStageSlots - 1)].x);
     for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32)
-        ys[e] = phase_factor((unsigned)(ny0 + (e >> 5)) * u[e & (kStageSlots - 1)].y);
+        ys[(e >> 5) * kXyRow + (e & 31)] = phase_factor((unsigned)(ny0 + (e >> 5)) * u[e & (kStageSlots - 1)].y);
 }
 
 // The hi and lo BF16 pairs of A for row (nxl, nyl) and atoms j0 .. j0 + 7 of the stage (j0 a multiple of
 // 8): every 16-byte load carries two atoms' factors that this lane uses.
 __device__ __forceinline__ void build8(const float2* xs, int nxl, int nyl, int j0, uint32_t (&hw)[8],
                                        uint32_t (&lw)[8]) {
-    const float4* xr = reinterpret_cast<const float4*>(xs + nxl * kStageSlots + j0);
-    const float4* yr = reinterpret_cast<const float4*>(xs + (kTcTileNx + nyl) * kStageSlots + j0);
+    const float4* xr = reinterpret_cast<const float4*>(xs + nxl * kXyRow + j0);
+    const float4* yr = reinterpret_cast<const float4*>(xs + (kTcTileNx + nyl) * kXyRow + j0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float4 x = xr[k], y = yr[k];
