@@ -152,6 +152,7 @@ struct TcState {
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
+    int nstages_f = 2, smem_bytes_f = 0;  // fused form: one X/Y buffer
     int nabuf = 2;  // A half-stage buffers in TMEM
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
@@ -261,11 +262,11 @@ __device__ __forceinline__ void product_split(float xr, float xi, float yr, floa
 // X/Y buffer: X factors [16 nx][kXyRow], then Y factors [8 ny][kXyRow], each (re, im) per atom.
 // Consecutive threads take consecutive atoms of one nx (ny): each thread reads its atom's phases once per
 // factor, and a warp's stores cover one row.
-__device__ __forceinline__ void fill_xy(float2* xs, const uint2* u, int nx0, int ny0, int xt) {
+__device__ __forceinline__ void fill_xy(float2* xs, const uint2* u, int nx0, int ny0, int xt, int nthreads) {
     float2* ys = xs + kTcTileNx * kXyRow;
-    for (int e = xt; e < kStageSlots * kTcTileNx; e += kXyWarps * 32)
+    for (int e = xt; e < kStageSlots * kTcTileNx; e += nthreads)
         xs[(e >> 5) * kXyRow + (e & 31)] = phase_factor((unsigned)(nx0 + (e >> 5)) * u[e & (kStageSlots - 1)].x);
-    for (int e = xt; e < kStageSlots * kTcTileNy; e += kXyWarps * 32)
+    for (int e = xt; e < kStageSlots * kTcTileNy; e += nthreads)
         ys[(e >> 5) * kXyRow + (e & 31)] = phase_factor((unsigned)(ny0 + (e >> 5)) * u[e & (kStageSlots - 1)].y);
 }
 
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128);
-                fill_xy(xy_ptr(xb), u, T.nx0, T.ny0, xt);
+                fill_xy(xy_ptr(xb), u, T.nx0, T.ny0, xt, kXyWarps * 32);
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
                 if (++slot == NS) {
@@ -670,6 +671,285 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_before();
     __syncthreads();
     if (warp == kMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// ---- fused form: the A builders also evaluate the X/Y factors and issue the MMAs ----------------
+// Warps 0-7 (256 threads) do, per stage: wait for the stage's B rows and phases, evaluate its X/Y
+// factors into one shared buffer, meet at a named barrier, then per half-stage form the products into
+// the next free A buffer in TMEM, meet again, and one thread (warp 0, lane 0) issues that half-stage's
+// six MMAs and commits.  The builders' own hardware barrier replaces the mbarrier handoffs between
+// factor warps, builders and a separate MMA warp; the A ring (empty_a) and the B ring (full_b,
+// empty_b) stay mbarriers, but with several buffers in flight their waits are normally already
+// complete.  Warps 8-15 drain the accumulator as in the split-role form, warp 16 issues the loads.
+constexpr int kFBuildWarps = 8;
+constexpr int kFEpiWarp0 = kFBuildWarps;          // 8
+constexpr int kFTmaWarp = kFEpiWarp0 + kEpiWarps;  // 16
+constexpr int kFThreads = (kFTmaWarp + 1) * 32;    // 544
+constexpr int kFBuildBar = 1;                      // named barrier of the builders
+
+// Barrier of the builders that also returns, to every one of them, whether any passed `stop`: the
+// abort flag can be raised at any time by other roles, so the builders decide on the value they reduce
+// here, never on separate reads, and all of them take the same branch (and the same barriers).
+__device__ __forceinline__ bool builders_sync_any(bool stop) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)stop), "n"(kFBuildBar), "n"(kFBuildWarps * 32)
+        : "memory");
+    return r != 0;
+}
+
+__global__ void __launch_bounds__(kFThreads, 1)
+    sq_tcf_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
+                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
+    __shared__ __align__(8) uint64_t empty_a[kMaxABufs], acc_full, acc_empty, mma_done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag_s;
+    volatile int& abort_flag = abort_flag_s;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int NS = p.nstages;
+    const int NA = p.nabuf;
+    const int F = p.flush_stages;
+    const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
+    auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
+    float2* xy = reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes);  // one X/Y buffer (fill_xy)
+
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < NS; ++s) {
+            trj_mbar_init(&full_b[s], 1);
+            trj_mbar_init(&empty_b[s], 1);
+        }
+        for (int b = 0; b < kMaxABufs; ++b) trj_mbar_init(&empty_a[b], 1);
+        trj_mbar_init(&acc_full, 1);
+        trj_mbar_init(&acc_empty, kEpiWarps);
+        trj_mbar_init(&mma_done, 1);
+        trj_fence_mbar_init();
+    }
+    if (warp == kFTmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         trj_smem_addr(&tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == kFTmaWarp) {
+        if (lane == 0) {
+            int slot = 0, issued = 0;
+            unsigned phase = 0;
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cta_items[li];
+                const TcTile T = p.tiles[it % p.ntiles];
+                const TcChunk C = p.chunks[it / p.ntiles];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kUxyBytes);
+                const int n64 = T.ncols / 64;  // B rows as 64-row boxes, then 16-row boxes
+                for (int s = 0; s < nst; ++s) {
+                    if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t* bh = stage_ptr(slot);
+                    uint8_t* bl = bh + p.bmax * 128;
+                    uint8_t* ux = bl + p.bmax * 128;
+                    trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
+                    const int slot0 = C.slot0 + s * kStageSlots;
+                    const int row0 = (slot0 / kStageSlots) * p.table_rows + T.brow;
+                    int r = 0;
+                    for (int b = 0; b < n64; ++b, r += 64) {
+                        tma_load_2d(bh + r * 128, &map_hi64, 0, row0 + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo64, 0, row0 + r, &full_b[slot]);
+                    }
+                    for (; r < T.ncols; r += 16) {
+                        tma_load_2d(bh + r * 128, &map_hi, 0, row0 + r, &full_b[slot]);
+                        tma_load_2d(bl + r * 128, &map_lo, 0, row0 + r, &full_b[slot]);
+                    }
+                    trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
+                    ++issued;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            // the copies issued last land before the CTA may exit: walk the ring back over them
+            for (int q = 0; q < NS && q < issued; ++q) {
+                if (--slot < 0) {
+                    slot = NS - 1;
+                    phase ^= 1;
+                }
+                trj_mbar_wait(&full_b[slot], phase);
+            }
+        }
+    } else if (warp >= kFEpiWarp0) {
+        // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
+        //      last run writes (sum + run) to this CTA's FP64 block once ----
+        const int q4 = warp & 3;
+        const int c0 = 16 * ((warp - kFEpiWarp0) >> 2);
+        const int row = 32 * q4 + lane;
+        const uint32_t lanes = (uint32_t)(32 * q4) << 16;
+        int fg = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cta_items[li];
+            const TcTile T = p.tiles[it % p.ntiles];
+            const int chunk = it / p.ntiles;
+            const TcChunk C = p.chunks[chunk];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const int nflush = (nst + F - 1) / F;
+            double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
+            for (int f = 0; f < nflush; ++f, ++fg) {
+                const bool ok = trj_mbar_wait(&acc_full, fg & 1);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const bool last = f == nflush - 1;
+                const uint32_t ta = tmem + lanes, ts = tmem + lanes + p.sum_col;
+                for (int c = c0; c < T.ncols; c += 32) {
+                    uint32_t a0[16], s0[16];
+                    tmem_ld16_nowait(ta + (uint32_t)c, a0);
+                    if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const float v = __uint_as_float(a0[k]);
+                        s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
+                    }
+                    if (last) {
+#pragma unroll
+                        for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
+                    } else {
+                        tmem_st16(ts + (uint32_t)c, s0);
+                    }
+                }
+                if (!last) tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&acc_empty);
+            }
+        }
+    } else {
+        // ---- builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
+        //      half-stage buffer, the K-columns of atoms [8*(w/4), 8*(w/4) + 8); warp 0 lane 0 issues ----
+        const int q = warp & 3, g = warp >> 2;
+        const int m = 32 * q + lane;
+        const int nxl = m & 15, nyl = m >> 4;
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
+        const bool issuer = tid == 0;
+        // issuer state: B descriptor of stage slot 0 (slot k sits k * stage_bytes further); a K-step of
+        // 16 bf16 adds 2 to the start-address field; the lo rows of B sit bmax rows after the hi rows
+        const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
+        const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
+        const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
+        uint64_t bh = b0desc;
+        int slot = 0, ab = 0, fg = 0, rs = 0;
+        unsigned phase = 0, aphase = 0;
+        bool stop = false;
+        for (int li = item0; li < item1 && !stop; ++li) {
+            const int it = p.cta_items[li];
+            const TcTile T = p.tiles[it % p.ntiles];
+            const TcChunk C = p.chunks[it / p.ntiles];
+            const int nst = (C.slot1 - C.slot0) / kStageSlots;
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
+                                   ((uint32_t)(128 >> 4) << 24);
+            for (int s = 0; s < nst; ++s) {
+                // the stage's B rows and phases; then its X/Y factors (the previous stage's products
+                // are done: every builder passed the barrier after them)
+                if (!trj_mbar_wait(&full_b[slot], phase)) {
+                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                }
+                fill_xy(xy, reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128), T.nx0, T.ny0, tid,
+                        kFBuildWarps * 32);
+                if (builders_sync_any(abort_flag != 0)) {
+                    stop = true;
+                    break;
+                }
+                const bool first_stage_of_run = rs == 0;
+                for (int hh = 0; hh < 2; ++hh) {
+                    if (!trj_mbar_wait(&empty_a[ab], aphase ^ 1)) {
+                        trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                        abort_flag = 1;
+                    }
+                    tc_fence_after();
+                    uint32_t hw[8], lw[8];
+                    build8(xy, nxl, nyl, 16 * hh + 8 * g, hw, lw);
+                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * ab + 8 * g);
+                    tmem_st8(ta, hw);
+                    tmem_st8(ta + 16, lw);
+                    tmem_wait_st();
+                    tc_fence_before();
+                    if (builders_sync_any(abort_flag != 0)) {
+                        stop = true;
+                        break;
+                    }
+                    if (issuer) {
+                        tc_fence_after();
+                        // the epilogue must have read the previous run out of the accumulator
+                        if (first_stage_of_run && hh == 0 && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status))
+                            abort_flag = 1;
+                        const uint32_t ah = tmem + p.a_col + (uint32_t)(32 * ab), al = ah + 16;
+                        const uint64_t bl = bh + b_lo;
+#pragma unroll
+                        for (int k2 = 0; k2 < 2; ++k2) {
+                            const int kk = 2 * hh + k2;
+                            mma_ts(tmem, ah + 8 * k2, bh + 2 * kk, idesc, (first_stage_of_run && kk == 0) ? 0u : 1u);
+                            mma_ts(tmem, ah + 8 * k2, bl + 2 * kk, idesc, 1u);
+                            mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
+                        }
+                        mma_commit(&empty_a[ab]);
+                    }
+                    if (++ab == NA) {
+                        ab = 0;
+                        aphase ^= 1;
+                    }
+                }
+                if (stop) break;
+                if (issuer) {
+                    mma_commit(&empty_b[slot]);
+                    if (rs + 1 == F || s == nst - 1) mma_commit(&acc_full);
+                }
+                if (++rs == F || s == nst - 1) {
+                    ++fg;
+                    rs = 0;
+                }
+                bh += b_step;
+                if (++slot == NS) {
+                    slot = 0;
+                    phase ^= 1;
+                    bh = b0desc;
+                }
+            }
+        }
+        if (issuer) {
+            // every MMA of this CTA has completed before TMEM is released
+            mma_commit(&mma_done);
+            trj_mbar_wait(&mma_done, 0);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == kFTmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -1023,7 +1303,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     break;
                 }
                 const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bhalf * 128);
-                fill_xy(xy_ptr(xb), u, nx0, ny0, xt);
+                fill_xy(xy_ptr(xb), u, nx0, ny0, xt, kXyWarps * 32);
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
                 if (++slot == NS) {
@@ -1327,6 +1607,8 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
     st->smem_bytes = st->nstages * st->stage_bytes + 2 * kXyBytes + 1024;
+    st->nstages_f = std::min(kMaxStages, ((int)ctx->smem_optin - 2048 - kXyBytes) / st->stage_bytes);
+    st->smem_bytes_f = st->nstages_f * st->stage_bytes + kXyBytes + 1024;
     const int64_t nitems = (int64_t)ntiles * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
     // Schedule: the items in chunk-major order are cut into windows of `grid` items; within a window
@@ -1414,6 +1696,8 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
+    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tcf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           st->smem_bytes_f));
     return prepare_pairs(plan, st, tt);
 }
 
@@ -1490,9 +1774,12 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         TRJ_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, sq_tc2_kernel, st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, Q));
         plan->timer.end(ctx, s);
     } else {
+        TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tcf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               st->smem_bytes_f));
+        P.nstages = st->nstages_f;
         plan->timer.begin(ctx, s);
-        sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
-                                                                  st->map_lo64, P);
+        sq_tcf_kernel<<<st->grid, kFThreads, st->smem_bytes_f, s>>>(st->map_hi, st->map_lo, st->map_hi64,
+                                                                    st->map_lo64, P);
         plan->timer.end(ctx, s);
     }
     const dim3 rg((unsigned)((st->bmax * 128 + 255) / 256), (unsigned)plan->tiles.size(), (unsigned)plan->nsp);
