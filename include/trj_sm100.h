@@ -94,6 +94,13 @@ TRJ_API int trj_ctx_set_allocator(trj_ctx* ctx, trj_alloc_fn alloc, trj_free_fn 
 TRJ_API int trj_ctx_set_timing(trj_ctx* ctx, int enable);
 /* Number of kernels this library has launched on the context so far. */
 TRJ_API int64_t trj_ctx_launches(const trj_ctx* ctx);
+/* Widest tensor-core S(Q) tile (output columns: 2 per nz value) of the S(Q)
+ * plans this context creates from now on: 0 (default, 224) or 32..224 in steps
+ * of 16.  Narrower tiles give more, smaller work items (small frames), wider ones
+ * fewer tensor-core instructions per vector; the serving loop's autotuner picks
+ * it per request size.  No counterpart in the reference (its sqfnD launch shape
+ * is fixed, sq.cuf:175-186). */
+TRJ_API int trj_ctx_set_sq_tile_cols(trj_ctx* ctx, int cols);
 
 /* ---- frame layout ---------------------------------------------------- */
 /* Replaces the per-frame layout of select_ncdfinput (src/core/netcdf.f90:582-692)

@@ -85,3 +85,13 @@ def test_cancel_running_and_queued_requests(workload):
             _, alone = _run([req], slots=1, method="split")
             assert np.array_equal(alone[req.rid].hist, res[req.rid].hist)
             assert np.array_equal(alone[req.rid].sq_sums, res[req.rid].sq_sums)
+
+
+def test_autotuner_picks_method_and_tile_width(workload):
+    from trj_analysis_b200.serve import Autotuner, Server
+    tuner = Autotuner()
+    srv = Server(slots=2, n_max=1 << 14, autotuner=tuner)
+    res = srv.run(workload[:3], realtime=False)
+    assert len(res) == 3 and tuner.table
+    for e in tuner.table.values():
+        assert (e["method"], e["cols"]) in Autotuner.CANDIDATES and e["ms"]

@@ -150,3 +150,22 @@ def test_sq_split_deterministic(ctx):
     _, a = run_gpu(ctx, fr, 1, ks, "split")
     _, b = run_gpu(ctx, fr, 1, ks, "split")
     assert np.array_equal(a, b)
+
+
+def test_sq_tile_width_knob(ctx):
+    """Narrower tensor-core tiles (more, smaller work items) give the same shell sums: every output
+    element sums the same atoms in the same order whatever the tile's width."""
+    from trj_analysis_b200._lib import TrjError
+    spec, mode, qmax, qmin = SPECS["3sp_ref"]
+    fr = spec.frame(0)
+    ks = refsem.make_kset(mode, fr.box, qmax, qmin)
+    _, a = run_gpu(ctx, fr, 3, ks, "split")
+    ctx.set_sq_tile_cols(96)
+    try:
+        _, b = run_gpu(ctx, fr, 3, ks, "split")
+    finally:
+        ctx.set_sq_tile_cols(0)
+    check_shells(b, a, 3)
+    assert np.allclose(a, b, rtol=1e-12, atol=0)
+    with pytest.raises(TrjError):
+        ctx.set_sq_tile_cols(100)

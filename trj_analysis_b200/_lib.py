@@ -46,6 +46,7 @@ SIGNATURES = {
     "trj_ctx_set_timing": (c_int, [vp, c_int]),
     "trj_ctx_set_allocator": (c_int, [vp, vp, vp, vp]),
     "trj_ctx_launches": (c_int64, [vp]),
+    "trj_ctx_set_sq_tile_cols": (c_int, [vp, c_int]),
     "trj_rdf_kernel_ms": (c_int, [vp, P(c_float)]),
     "trj_sq_kernel_ms": (c_int, [vp, P(c_float)]),
     "trj_frame_pack": (c_int, [vp, vp, vp, c_int64, c_int, P(c_float), vp, vp, vp]),

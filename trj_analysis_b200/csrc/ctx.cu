@@ -100,6 +100,14 @@ extern "C" int trj_ctx_set_allocator(trj_ctx* ctx, trj_alloc_fn alloc, trj_free_
 
 extern "C" int64_t trj_ctx_launches(const trj_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" int trj_ctx_set_sq_tile_cols(trj_ctx* ctx, int cols) {
+    if (!ctx) return TRJ_ERR_INVALID;
+    if (cols != 0 && (cols < 32 || cols > 224 || cols % 16 != 0))
+        return trj_fail(ctx, TRJ_ERR_INVALID, "trj_ctx_set_sq_tile_cols: %d (0, or 32..224 in steps of 16)", cols);
+    ctx->sq_tile_cols = cols;
+    return TRJ_OK;
+}
+
 extern "C" int trj_ctx_set_timing(trj_ctx* ctx, int enable) {
     if (!ctx) return TRJ_ERR_INVALID;
     ctx->timing = enable != 0;

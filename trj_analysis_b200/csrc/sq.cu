@@ -305,6 +305,7 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
     // grouped by (nx/16, ny/8) blocks; a block's nz span (both signs) becomes the tile's columns,
     // split into column groups of <= 224 (112 nz values).  A negative stride marks a conjugate.
     std::vector<int64_t> dense_src(nvec, -1), dense_stride(nvec, 0);
+    const int max_cols = ctx->sq_tile_cols > 0 ? ctx->sq_tile_cols : kTcMaxCols;  // a multiple of 16
     if (!dense_idx.empty()) {
         struct Rep { int x, y, z; bool conj; };
         std::vector<Rep> rep(nvec);
@@ -331,7 +332,7 @@ extern "C" int trj_sq_plan_create(trj_ctx* ctx, int nsp, int64_t nvec, const int
             while (a < j) {
                 int z0 = rep[keyed[a].second].z;
                 size_t b = a;
-                while (b < j && rep[keyed[b].second].z - z0 < kTcMaxCols / 2) ++b;
+                while (b < j && rep[keyed[b].second].z - z0 < max_cols / 2) ++b;
                 int zspan = rep[keyed[b - 1].second].z - z0 + 1;
                 int ncols = ((2 * zspan + 15) / 16) * 16;
                 SqTile t;

@@ -36,6 +36,7 @@ struct trj_ctx {
     trj_alloc_fn alloc = nullptr;       // caller-provided device allocator (NULL: cudaMalloc)
     trj_free_fn free_fn = nullptr;
     void* alloc_user = nullptr;
+    int sq_tile_cols = 0;               // widest tensor-core S(Q) tile of plans created next (0: 224)
     std::string last_error;
 };
 

@@ -48,6 +48,10 @@ class Context:
         """Synchronises ``stream`` and raises on device-side status (bad data, timeouts)."""
         check(self.lib.trj_ctx_check(self.h, _stream(stream)), self.h, "device status")
 
+    def set_sq_tile_cols(self, cols: int) -> None:
+        """Widest tensor-core S(Q) tile of plans created from now on (0: default 224)."""
+        check(self.lib.trj_ctx_set_sq_tile_cols(self.h, int(cols)), self.h, "trj_ctx_set_sq_tile_cols")
+
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.trj_ctx_destroy(self.h)

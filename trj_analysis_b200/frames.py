@@ -91,9 +91,19 @@ class FCCSpec:
         rng.shuffle(types)
         return keep, types
 
+    def _base(self):
+        """Kept lattice sites and types, computed once per spec (every frame shares them)."""
+        key = (self.cells, self.density, self.fractions, self.remove, self.seed)
+        cache = self.__dict__.get("_base_cache")
+        if cache is None or cache[0] != key:
+            keep, types = self._identity()
+            cache = (key, self._lattice()[keep], types)
+            self.__dict__["_base_cache"] = cache
+        return cache[1], cache[2]
+
     def frame(self, index: int) -> Frame:
-        keep, types = self._identity()
-        pos = self._lattice()[keep]
+        base, types = self._base()
+        pos = base.copy()
         rng = np.random.default_rng([self.seed, 1 + index])
         pos = pos + rng.normal(0.0, self.sigma * self.a, size=pos.shape)
         box = self.box.astype(np.float64)

@@ -18,8 +18,8 @@ parameters.  The loop:
   after the frames already on its stream: once they have finished its plans, slot and HBM budget
   are released and it yields no result (its id is listed in ``cancelled``).
 
-The S(Q) method of each (size, species) bucket is picked by a small autotuner that times
-the tensor-core and direct-sum paths once on the bucket's first request.
+The S(Q) method and the tensor-core tile width of each (size, species) bucket are picked by an
+autotuner that times the candidates once on the bucket's first request.
 Results do not depend on what else runs: pair counts are integers and the S(Q) sums use a
 fixed reduction order, so a request gives bit-identical output alone and in a mix.
 """
@@ -116,11 +116,16 @@ class Result:
 
 
 class Autotuner:
-    """Chooses the S(Q) method per (log2 N, species) bucket by timing both once."""
+    """Chooses, per (k-set mode, log2 N, species) bucket, the S(Q) method and the widest tensor-core tile
+    (output columns per tile: narrow tiles make more, smaller work items for small frames; wide ones issue
+    fewer tensor-core instructions per vector) by timing every candidate once on the bucket's first
+    request.  The table is kept (and saved to `path`, when given) with the measured times."""
+
+    CANDIDATES = (("split", 224), ("split", 160), ("split", 96), ("plain", 0))
 
     def __init__(self, path: Optional[str] = None):
         self.path = path
-        self.table: Dict[str, str] = {}
+        self.table: Dict[str, dict] = {}
         if path and os.path.exists(path):
             self.table = json.load(open(path))
 
@@ -128,28 +133,43 @@ class Autotuner:
     def key(n: int, nsp: int, kset: str) -> str:
         return f"{kset}:{int(math.log2(max(n, 1)))}:{nsp}"
 
-    def lookup(self, n: int, nsp: int, kset: str) -> Optional[str]:
-        return self.table.get(self.key(n, nsp, kset))
+    def lookup(self, n: int, nsp: int, kset: str):
+        """(method, tile columns) of the bucket, or None before it is tuned."""
+        e = self.table.get(self.key(n, nsp, kset))
+        return None if e is None else (e["method"], int(e["cols"]))
 
-    def tune(self, sq: engine.SqPlan, packed: torch.Tensor, n: int, box, stream) -> str:
-        if sq.n_tiles == 0:
-            return "plain"
-        scratch = sq.new_out()
+    def tune(self, ctx: engine.Context, ks: refsem.KSet, counts, packed: torch.Tensor, n: int, box, stream):
+        """Times every candidate on the laid-out frame `packed` (2 accumulations after a warm one);
+        returns (method, tile columns, {candidate: ms})."""
+        nsp = len(counts)
         times = {}
-        for m in ("split", "plain"):
+        for method, cols in self.CANDIDATES:
+            ctx.set_sq_tile_cols(cols)
+            try:
+                with torch.cuda.stream(stream):
+                    plan = engine.SqPlan(ctx, nsp, ks, counts)
+            finally:
+                ctx.set_sq_tile_cols(0)
+            if method == "split" and plan.n_tiles == 0:
+                plan.close()
+                continue
             with torch.cuda.stream(stream):
-                sq.accumulate(packed, n, box, scratch, engine.METHODS[m], stream=stream)  # warm
+                out = plan.new_out()
+                plan.accumulate(packed, n, box, out, engine.METHODS[method], stream=stream)  # warm
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
                 for _ in range(2):
-                    sq.accumulate(packed, n, box, scratch, engine.METHODS[m], stream=stream)
+                    plan.accumulate(packed, n, box, out, engine.METHODS[method], stream=stream)
                 b.record(stream)
             b.synchronize()
-            times[m] = a.elapsed_time(b)
-        return min(times, key=times.get)
+            times[f"{method}:{cols}"] = a.elapsed_time(b) / 2.0
+            plan.close()
+        best = min(times, key=times.get)
+        method, cols = best.split(":")
+        return method, int(cols), times
 
-    def record(self, n: int, nsp: int, kset: str, method: str) -> None:
-        self.table[self.key(n, nsp, kset)] = method
+    def record(self, n: int, nsp: int, kset: str, method: str, cols: int, times=None) -> None:
+        self.table[self.key(n, nsp, kset)] = {"method": method, "cols": int(cols), "ms": times or {}}
         if self.path:
             with open(self.path, "w") as f:
                 json.dump(self.table, f, indent=1)
@@ -257,7 +277,9 @@ class Server:
         bsc = list(req.bsc) if req.bsc is not None else [1.0] * req.nsp
         ks = refsem.make_kset(req.kset, fr0.box, req.qmax, req.qmin)
         counts = np.bincount(sp[sp >= 0], minlength=req.nsp)
-        method = req.method or self.method or self.tuner.lookup(req.n, req.nsp, req.kset) or "split"
+        tuned = self.tuner.lookup(req.n, req.nsp, req.kset)
+        method = req.method or self.method or (tuned[0] if tuned else "split")
+        cols = tuned[1] if (tuned and req.method is None and self.method is None) else 0
         fp = self.footprint(req, ks, method)
         if self.in_use + fp > self.hbm_budget and self.in_use > 0:
             self.admission_waits += 1
@@ -269,11 +291,16 @@ class Server:
         job.ks = ks
         with torch.cuda.stream(slot.stream):
             job.rdf = engine.RdfPlan(self.ctx, req.nsp, req.deltar, req.rcrdf, fr0.box, max(req.n, 2))
-            job.sq = engine.SqPlan(self.ctx, req.nsp, ks, counts)
+            self.ctx.set_sq_tile_cols(cols)
+            try:
+                job.sq = engine.SqPlan(self.ctx, req.nsp, ks, counts)
+            finally:
+                self.ctx.set_sq_tile_cols(0)
             job.hist = job.rdf.new_hist()
             job.out = job.sq.new_out()
         job.method = method
-        job.tune = req.method is None and self.method is None and self.tuner.lookup(req.n, req.nsp, req.kset) is None
+        job.cols = cols
+        job.tune = req.method is None and self.method is None and tuned is None
         job.footprint = fp
         self.in_use += fp
         self.peak_in_use = max(self.peak_in_use, self.in_use)
@@ -307,8 +334,16 @@ class Server:
                 s.d_sp[:n].copy_(s.h_sp[buf][:n], non_blocking=True)
                 engine.pack_frame(self.ctx, s.d_xyz[:n], s.d_sp[:n], req.nsp, fr.box, s.packed, s.counts,
                                   stream=s.stream)
-                job.method = self.tuner.tune(job.sq, s.packed, n, fr.box, s.stream)
-                self.tuner.record(req.n, req.nsp, req.kset, job.method)
+                job.method, cols, times = self.tuner.tune(self.ctx, job.ks, job.ntype, s.packed, n, fr.box, s.stream)
+                self.tuner.record(req.n, req.nsp, req.kset, job.method, cols, times)
+                if cols != job.cols:  # the job's plan takes the tuned tile width
+                    job.sq.close()
+                    self.ctx.set_sq_tile_cols(cols)
+                    try:
+                        job.sq = engine.SqPlan(self.ctx, req.nsp, job.ks, job.ntype)
+                    finally:
+                        self.ctx.set_sq_tile_cols(0)
+                    job.cols = cols
             graphed = self.use_graphs and len(req.frames) >= 4
             if graphed and k >= 1 and job.graphs[buf] is None:
                 # capture this frame's launch sequence (no device synchronisation: other requests keep
