@@ -345,6 +345,8 @@ def run_ours(args, rank, world, local_rank):
                                f"rcrdf={wl['rcrdf']}, S(Q) qmax={wl['qmax']} qmin={wl['qmin']} kset={wl['kset']}",
                    "method": method, "n_kvec": int(sq.kset.nvec), "n_kvec_tensor": int(n_dense),
                    "rdf_cells": list(rdf.cells), "parallelism": f"replicas x{world}",
+                   "plan_scratch_bytes": {"rdf": int(rdf.scratch_bytes), "sq": int(sq.scratch_bytes)},
+                   "device_bytes_in_use": int(torch.cuda.memory_allocated(dev)),
                    "l2": "256 MB buffer written between steps (inside the timed region)",
                    "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
         "clocks": clocks, "gpu_launches": int(launches), "roofline": roof, "roofline_pairs": roof_pairs, "e2e": e2e,
