@@ -29,11 +29,11 @@
 // factor at FP32 accuracy.
 //
 // Work item = (tile, chunk of one species' atoms).  Persistent CTAs walk their items chunk-major.
-// Roles per CTA (704 threads), handing stages to each other through mbarriers only: warps 8-11
-// evaluate the X/Y factors of a stage into one of two shared-memory buffers; warps 0-7 form the
-// products, split them and store them into the A buffers in TMEM (the two warps of one TMEM lane
-// quarter split a half-stage's 16 atoms); warps 12-19 drain the accumulator (two warps per lane
-// quarter, alternating 16-column chunks); warp 20 issues the TMA loads; warp 21 allocates TMEM and
+// Roles per CTA (960 threads), handing stages to each other through mbarriers only: warps 16-19
+// evaluate the X/Y factors of a stage into one of two shared-memory buffers; warps 0-15 form the
+// products, split them and store them into the A buffers in TMEM (the four warps of one TMEM lane
+// quarter split a half-stage's 16 atoms); warps 20-27 drain the accumulator (two warps per lane
+// quarter, alternating 16-column chunks); warp 28 issues the TMA loads; warp 29 allocates TMEM and
 // one of its lanes issues the MMAs.  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -45,15 +45,20 @@
 
 namespace {
 
-constexpr int kBuildWarps = 8;                     // warps 0-7: A products into TMEM
-constexpr int kXyWarps = 4;                        // warps 8-11: X/Y factors into shared memory
-constexpr int kEpiWarps = 8;                       // warps 12-19: accumulator drains
+// Builders: four warps per TMEM lane quarter (four per SM sub-partition, so that the latency of one
+// warp's shared-memory loads and TMEM stores is covered by the others).
+constexpr int kBuildWarps = 16;                    // warps 0-15: A products into TMEM
+constexpr int kXyWarps = 4;                        // warps 16-19: X/Y factors into shared memory
+constexpr int kEpiWarps = 8;                       // warps 20-27: accumulator drains
 constexpr int kXyWarp0 = kBuildWarps;
 constexpr int kEpiWarp0 = kXyWarp0 + kXyWarps;
-constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
-constexpr int kMmaWarp = kTmaWarp + 1;             // 21
-constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
+constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 28
+constexpr int kMmaWarp = kTmaWarp + 1;             // 29
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 960
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
+constexpr int kBuildGroups = kBuildWarps / 4;      // builder warps per lane quarter
+constexpr int kHalfAtoms = kStageSlots / 2 / kBuildGroups;  // atoms of a half-stage per builder warp
+static_assert(kBuildWarps % 4 == 0 && kHalfAtoms % 4 == 0, "builder layout");
 // X/Y factor rows: 32 atoms as (re, im) plus 2 pad entries, so that rows start 272 bytes (68 banks)
 // apart and the 16-byte loads of eight lanes on eight different rows fall in different banks.
 constexpr int kXyRow = kStageSlots + 2;
@@ -152,7 +157,6 @@ struct TcState {
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
-    int nstages_f = 2, smem_bytes_f = 0;  // fused form: one X/Y buffer
     int nabuf = 2;  // A half-stage buffers in TMEM
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
@@ -236,6 +240,18 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8])
                  : "memory");
 }
 
+__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&r)[4]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(r[0]), "r"(r[1]),
+                 "r"(r[2]), "r"(r[3])
+                 : "memory");
+}
+
+template <int NJ>
+__device__ __forceinline__ void tmem_st_cols(uint32_t taddr, const uint32_t (&r)[NJ]) {
+    if constexpr (NJ == 8) tmem_st8(taddr, r);
+    else tmem_st4(taddr, r);
+}
+
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
@@ -270,14 +286,15 @@ __device__ __forceinline__ void fill_xy(float2* xs, const uint2* u, int nx0, int
         ys[(e >> 5) * kXyRow + (e & 31)] = phase_factor((unsigned)(ny0 + (e >> 5)) * u[e & (kStageSlots - 1)].y);
 }
 
-// The hi and lo BF16 pairs of A for row (nxl, nyl) and atoms j0 .. j0 + 7 of the stage (j0 a multiple of
-// 8): every 16-byte load carries two atoms' factors that this lane uses.
-__device__ __forceinline__ void build8(const float2* xs, int nxl, int nyl, int j0, uint32_t (&hw)[8],
-                                       uint32_t (&lw)[8]) {
+// The hi and lo BF16 pairs of A for row (nxl, nyl) and atoms j0 .. j0 + NJ - 1 of the stage (j0 a
+// multiple of 4): every 16-byte load carries two atoms' factors that this lane uses.
+template <int NJ>
+__device__ __forceinline__ void build_row(const float2* xs, int nxl, int nyl, int j0, uint32_t (&hw)[NJ],
+                                          uint32_t (&lw)[NJ]) {
     const float4* xr = reinterpret_cast<const float4*>(xs + nxl * kXyRow + j0);
     const float4* yr = reinterpret_cast<const float4*>(xs + (kTcTileNx + nyl) * kXyRow + j0);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < NJ / 2; ++k) {
         const float4 x = xr[k], y = yr[k];
         product_split(x.x, x.y, y.x, y.y, hw[2 * k], lw[2 * k]);
         product_split(x.z, x.w, y.z, y.w, hw[2 * k + 1], lw[2 * k + 1]);
@@ -617,8 +634,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
         }
     } else {
-        // ---- A builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
-        //      half-stage buffer, the K-columns of atoms [8*(w/4), 8*(w/4) + 8) ----
+        // ---- A builders (warps 0-15): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
+        //      half-stage buffer, the K-columns of atoms [kHalfAtoms*(w/4), kHalfAtoms*(w/4 + 1)) ----
         const int q = warp & 3, g = warp >> 2;
         const int m = 32 * q + lane;
         const int nxl = m & 15, nyl = m >> 4;
@@ -649,11 +666,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    uint32_t hw[8], lw[8];
-                    build8(xs, nxl, nyl, 16 * hh + 8 * g, hw, lw);
-                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + 8 * g);
-                    tmem_st8(ta, hw);
-                    tmem_st8(ta + 16, lw);
+                    uint32_t hw[kHalfAtoms], lw[kHalfAtoms];
+                    build_row<kHalfAtoms>(xs, nxl, nyl, 16 * hh + kHalfAtoms * g, hw, lw);
+                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + kHalfAtoms * g);
+                    tmem_st_cols<kHalfAtoms>(ta, hw);
+                    tmem_st_cols<kHalfAtoms>(ta + 16, lw);
                     tmem_wait_st();
                     tc_fence_before();
                     __syncwarp();
@@ -671,285 +688,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_before();
     __syncthreads();
     if (warp == kMmaWarp) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
-    }
-}
-
-// ---- fused form: the A builders also evaluate the X/Y factors and issue the MMAs ----------------
-// Warps 0-7 (256 threads) do, per stage: wait for the stage's B rows and phases, evaluate its X/Y
-// factors into one shared buffer, meet at a named barrier, then per half-stage form the products into
-// the next free A buffer in TMEM, meet again, and one thread (warp 0, lane 0) issues that half-stage's
-// six MMAs and commits.  The builders' own hardware barrier replaces the mbarrier handoffs between
-// factor warps, builders and a separate MMA warp; the A ring (empty_a) and the B ring (full_b,
-// empty_b) stay mbarriers, but with several buffers in flight their waits are normally already
-// complete.  Warps 8-15 drain the accumulator as in the split-role form, warp 16 issues the loads.
-constexpr int kFBuildWarps = 8;
-constexpr int kFEpiWarp0 = kFBuildWarps;          // 8
-constexpr int kFTmaWarp = kFEpiWarp0 + kEpiWarps;  // 16
-constexpr int kFThreads = (kFTmaWarp + 1) * 32;    // 544
-constexpr int kFBuildBar = 1;                      // named barrier of the builders
-
-// Barrier of the builders that also returns, to every one of them, whether any passed `stop`: the
-// abort flag can be raised at any time by other roles, so the builders decide on the value they reduce
-// here, never on separate reads, and all of them take the same branch (and the same barriers).
-__device__ __forceinline__ bool builders_sync_any(bool stop) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, %2, %3, q;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)stop), "n"(kFBuildBar), "n"(kFBuildWarps * 32)
-        : "memory");
-    return r != 0;
-}
-
-__global__ void __launch_bounds__(kFThreads, 1)
-    sq_tcf_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
-                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t empty_a[kMaxABufs], acc_full, acc_empty, mma_done;
-    __shared__ uint32_t tmem_slot;
-    __shared__ int abort_flag_s;
-    volatile int& abort_flag = abort_flag_s;
-
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NS = p.nstages;
-    const int NA = p.nabuf;
-    const int F = p.flush_stages;
-    const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
-    auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
-    float2* xy = reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes);  // one X/Y buffer (fill_xy)
-
-    if (tid == 0) {
-        abort_flag = 0;
-        for (int s = 0; s < NS; ++s) {
-            trj_mbar_init(&full_b[s], 1);
-            trj_mbar_init(&empty_b[s], 1);
-        }
-        for (int b = 0; b < kMaxABufs; ++b) trj_mbar_init(&empty_a[b], 1);
-        trj_mbar_init(&acc_full, 1);
-        trj_mbar_init(&acc_empty, kEpiWarps);
-        trj_mbar_init(&mma_done, 1);
-        trj_fence_mbar_init();
-    }
-    if (warp == kFTmaWarp) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         trj_smem_addr(&tmem_slot)),
-                     "r"(kTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = tmem_slot;
-
-    if (warp == kFTmaWarp) {
-        if (lane == 0) {
-            int slot = 0, issued = 0;
-            unsigned phase = 0;
-            for (int li = item0; li < item1 && !abort_flag; ++li) {
-                const int it = p.cta_items[li];
-                const TcTile T = p.tiles[it % p.ntiles];
-                const TcChunk C = p.chunks[it / p.ntiles];
-                const int nst = (C.slot1 - C.slot0) / kStageSlots;
-                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kUxyBytes);
-                const int n64 = T.ncols / 64;  // B rows as 64-row boxes, then 16-row boxes
-                for (int s = 0; s < nst; ++s) {
-                    if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
-                        abort_flag = 1;
-                        break;
-                    }
-                    uint8_t* bh = stage_ptr(slot);
-                    uint8_t* bl = bh + p.bmax * 128;
-                    uint8_t* ux = bl + p.bmax * 128;
-                    trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
-                    const int slot0 = C.slot0 + s * kStageSlots;
-                    const int row0 = (slot0 / kStageSlots) * p.table_rows + T.brow;
-                    int r = 0;
-                    for (int b = 0; b < n64; ++b, r += 64) {
-                        tma_load_2d(bh + r * 128, &map_hi64, 0, row0 + r, &full_b[slot]);
-                        tma_load_2d(bl + r * 128, &map_lo64, 0, row0 + r, &full_b[slot]);
-                    }
-                    for (; r < T.ncols; r += 16) {
-                        tma_load_2d(bh + r * 128, &map_hi, 0, row0 + r, &full_b[slot]);
-                        tma_load_2d(bl + r * 128, &map_lo, 0, row0 + r, &full_b[slot]);
-                    }
-                    trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
-                    ++issued;
-                    if (++slot == NS) {
-                        slot = 0;
-                        phase ^= 1;
-                    }
-                }
-            }
-            // the copies issued last land before the CTA may exit: walk the ring back over them
-            for (int q = 0; q < NS && q < issued; ++q) {
-                if (--slot < 0) {
-                    slot = NS - 1;
-                    phase ^= 1;
-                }
-                trj_mbar_wait(&full_b[slot], phase);
-            }
-        }
-    } else if (warp >= kFEpiWarp0) {
-        // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
-        //      last run writes (sum + run) to this CTA's FP64 block once ----
-        const int q4 = warp & 3;
-        const int c0 = 16 * ((warp - kFEpiWarp0) >> 2);
-        const int row = 32 * q4 + lane;
-        const uint32_t lanes = (uint32_t)(32 * q4) << 16;
-        int fg = 0;
-        bool stop = false;
-        for (int li = item0; li < item1 && !stop; ++li) {
-            const int it = p.cta_items[li];
-            const TcTile T = p.tiles[it % p.ntiles];
-            const int chunk = it / p.ntiles;
-            const TcChunk C = p.chunks[chunk];
-            const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            const int nflush = (nst + F - 1) / F;
-            double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
-            for (int f = 0; f < nflush; ++f, ++fg) {
-                const bool ok = trj_mbar_wait(&acc_full, fg & 1);
-                if (!__all_sync(0xffffffffu, ok)) {
-                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                    abort_flag = 1;
-                    stop = true;
-                    break;
-                }
-                tc_fence_after();
-                const bool last = f == nflush - 1;
-                const uint32_t ta = tmem + lanes, ts = tmem + lanes + p.sum_col;
-                for (int c = c0; c < T.ncols; c += 32) {
-                    uint32_t a0[16], s0[16];
-                    tmem_ld16_nowait(ta + (uint32_t)c, a0);
-                    if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
-                    tmem_wait_ld();
-#pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const float v = __uint_as_float(a0[k]);
-                        s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
-                    }
-                    if (last) {
-#pragma unroll
-                        for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
-                    } else {
-                        tmem_st16(ts + (uint32_t)c, s0);
-                    }
-                }
-                if (!last) tmem_wait_st();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&acc_empty);
-            }
-        }
-    } else {
-        // ---- builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
-        //      half-stage buffer, the K-columns of atoms [8*(w/4), 8*(w/4) + 8); warp 0 lane 0 issues ----
-        const int q = warp & 3, g = warp >> 2;
-        const int m = 32 * q + lane;
-        const int nxl = m & 15, nyl = m >> 4;
-        const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        const bool issuer = tid == 0;
-        // issuer state: B descriptor of stage slot 0 (slot k sits k * stage_bytes further); a K-step of
-        // 16 bf16 adds 2 to the start-address field; the lo rows of B sit bmax rows after the hi rows
-        const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
-        const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
-        const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
-        uint64_t bh = b0desc;
-        int slot = 0, ab = 0, fg = 0, rs = 0;
-        unsigned phase = 0, aphase = 0;
-        bool stop = false;
-        for (int li = item0; li < item1 && !stop; ++li) {
-            const int it = p.cta_items[li];
-            const TcTile T = p.tiles[it % p.ntiles];
-            const TcChunk C = p.chunks[it / p.ntiles];
-            const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
-                                   ((uint32_t)(128 >> 4) << 24);
-            for (int s = 0; s < nst; ++s) {
-                // the stage's B rows and phases; then its X/Y factors (the previous stage's products
-                // are done: every builder passed the barrier after them)
-                if (!trj_mbar_wait(&full_b[slot], phase)) {
-                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                    abort_flag = 1;
-                }
-                fill_xy(xy, reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128), T.nx0, T.ny0, tid,
-                        kFBuildWarps * 32);
-                if (builders_sync_any(abort_flag != 0)) {
-                    stop = true;
-                    break;
-                }
-                const bool first_stage_of_run = rs == 0;
-                for (int hh = 0; hh < 2; ++hh) {
-                    if (!trj_mbar_wait(&empty_a[ab], aphase ^ 1)) {
-                        trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                        abort_flag = 1;
-                    }
-                    tc_fence_after();
-                    uint32_t hw[8], lw[8];
-                    build8(xy, nxl, nyl, 16 * hh + 8 * g, hw, lw);
-                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * ab + 8 * g);
-                    tmem_st8(ta, hw);
-                    tmem_st8(ta + 16, lw);
-                    tmem_wait_st();
-                    tc_fence_before();
-                    if (builders_sync_any(abort_flag != 0)) {
-                        stop = true;
-                        break;
-                    }
-                    if (issuer) {
-                        tc_fence_after();
-                        // the epilogue must have read the previous run out of the accumulator
-                        if (first_stage_of_run && hh == 0 && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status))
-                            abort_flag = 1;
-                        const uint32_t ah = tmem + p.a_col + (uint32_t)(32 * ab), al = ah + 16;
-                        const uint64_t bl = bh + b_lo;
-#pragma unroll
-                        for (int k2 = 0; k2 < 2; ++k2) {
-                            const int kk = 2 * hh + k2;
-                            mma_ts(tmem, ah + 8 * k2, bh + 2 * kk, idesc, (first_stage_of_run && kk == 0) ? 0u : 1u);
-                            mma_ts(tmem, ah + 8 * k2, bl + 2 * kk, idesc, 1u);
-                            mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
-                        }
-                        mma_commit(&empty_a[ab]);
-                    }
-                    if (++ab == NA) {
-                        ab = 0;
-                        aphase ^= 1;
-                    }
-                }
-                if (stop) break;
-                if (issuer) {
-                    mma_commit(&empty_b[slot]);
-                    if (rs + 1 == F || s == nst - 1) mma_commit(&acc_full);
-                }
-                if (++rs == F || s == nst - 1) {
-                    ++fg;
-                    rs = 0;
-                }
-                bh += b_step;
-                if (++slot == NS) {
-                    slot = 0;
-                    phase ^= 1;
-                    bh = b0desc;
-                }
-            }
-        }
-        if (issuer) {
-            // every MMA of this CTA has completed before TMEM is released
-            mma_commit(&mma_done);
-            trj_mbar_wait(&mma_done, 0);
-        }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == kFTmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -1314,7 +1052,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else {
         // ---- A builders: warp w writes TMEM lanes 32*(w%4).. and the K-columns of atoms
-        //      [16*(w/4), 16*(w/4) + 16) of the stage's A buffer, arriving on the leader's full_a ----
+        //      [2*kHalfAtoms*(w/4), 2*kHalfAtoms*(w/4 + 1)) of the stage's A buffer, arriving on the
+        //      leader's full_a ----
         const int q = warp & 3, g = warp >> 2;
         const int m = 32 * q + lane;
         const int nxl = m & 15, nyl = m >> 4;
@@ -1338,11 +1077,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 }
                 tc_fence_after();
                 const float2* xs = xy_ptr(xb);
-                const uint32_t ta = tmem + lanes + kPairACol + (uint32_t)(64 * ab + 16 * g);
+                const uint32_t ta = tmem + lanes + kPairACol + (uint32_t)(64 * ab + 2 * kHalfAtoms * g);
 #pragma unroll
-                for (int h8 = 0; h8 < 2; ++h8) {
+                for (int h8 = 0; h8 < 2 * kHalfAtoms / 8; ++h8) {
                     uint32_t hw[8], lw[8];
-                    build8(xs, nxl, nyl, 16 * g + 8 * h8, hw, lw);
+                    build_row<8>(xs, nxl, nyl, 2 * kHalfAtoms * g + 8 * h8, hw, lw);
                     tmem_st8(ta + 8 * h8, hw);
                     tmem_st8(ta + 32 + 8 * h8, lw);
                 }
@@ -1607,8 +1346,6 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
     st->smem_bytes = st->nstages * st->stage_bytes + 2 * kXyBytes + 1024;
-    st->nstages_f = std::min(kMaxStages, ((int)ctx->smem_optin - 2048 - kXyBytes) / st->stage_bytes);
-    st->smem_bytes_f = st->nstages_f * st->stage_bytes + kXyBytes + 1024;
     const int64_t nitems = (int64_t)ntiles * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
     // Schedule: the items in chunk-major order are cut into windows of `grid` items; within a window
@@ -1696,8 +1433,6 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     if (rc != TRJ_OK) return rc;
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
-    TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tcf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           st->smem_bytes_f));
     return prepare_pairs(plan, st, tt);
 }
 
@@ -1774,12 +1509,9 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         TRJ_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, sq_tc2_kernel, st->map_hi, st->map_lo, st->map_hi64, st->map_lo64, Q));
         plan->timer.end(ctx, s);
     } else {
-        TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tcf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               st->smem_bytes_f));
-        P.nstages = st->nstages_f;
         plan->timer.begin(ctx, s);
-        sq_tcf_kernel<<<st->grid, kFThreads, st->smem_bytes_f, s>>>(st->map_hi, st->map_lo, st->map_hi64,
-                                                                    st->map_lo64, P);
+        sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
+                                                                  st->map_lo64, P);
         plan->timer.end(ctx, s);
     }
     const dim3 rg((unsigned)((st->bmax * 128 + 255) / 256), (unsigned)plan->tiles.size(), (unsigned)plan->nsp);
