@@ -29,12 +29,15 @@
 // factor at FP32 accuracy.
 //
 // Work item = (tile, chunk of one species' atoms).  Persistent CTAs walk their items chunk-major.
-// Roles per CTA (960 threads), handing stages to each other through mbarriers only: warps 16-19
-// evaluate the X/Y factors of a stage into one of two shared-memory buffers; warps 0-15 form the
-// products, split them and store them into the A buffers in TMEM (the four warps of one TMEM lane
-// quarter split a half-stage's 16 atoms); warps 20-27 drain the accumulator (two warps per lane
-// quarter, alternating 16-column chunks); warp 28 issues the TMA loads; warp 29 allocates TMEM and
-// one of its lanes issues the MMAs.  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
+// Roles per CTA (704 threads), handing stages to each other through mbarriers only: warps 8-11
+// evaluate the X/Y factors of a stage into one of two shared-memory buffers; warps 0-7 form the
+// products, split them and store them into the A buffers in TMEM (the two warps of one TMEM lane
+// quarter split a half-stage's 16 atoms); warps 12-19 drain the accumulator (two warps per lane
+// quarter, alternating 16-column chunks); warp 20 issues the TMA loads; warp 21 allocates TMEM and
+// one of its lanes issues the MMAs.  Each role runs at its own pace: a warp arrives on a barrier and
+// moves on (two forms that tied the roles closer were slower at c3: the builders evaluating the
+// factors themselves and issuing the MMAs, 16.2 ms, and the builders issuing the MMAs after a named
+// barrier per half-stage, 13.5 ms, against 10.9 ms).  Every mbarrier wait is bounded and raises TRJ_DEV_TIMEOUT instead of hanging.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -45,18 +48,17 @@
 
 namespace {
 
-// Builders: two warps per TMEM lane quarter.  (Four per quarter, 16 warps, measured slower at c3:
-// 11.46 against 10.90 ms.)
+// Builders: two warps per TMEM lane quarter, each taking 8 atoms of a half-stage.  Measured at c3
+// against other layouts of the same roles: four warps per quarter (4 atoms each) 11.46 ms, against
+// 10.88 ms for two.
 constexpr int kBuildWarps = 8;                     // warps 0-7: A products into TMEM
 constexpr int kXyWarps = 4;                        // warps 8-11: X/Y factors into shared memory
 constexpr int kEpiWarps = 8;                       // warps 12-19: accumulator drains
 constexpr int kXyWarp0 = kBuildWarps;
 constexpr int kEpiWarp0 = kXyWarp0 + kXyWarps;
 constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
-constexpr int kMmaWarp = kTmaWarp + 1;             // 21: the MMA warp of the CTA-pair form
-constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704: CTA-pair form
-constexpr int kTc1Threads = (kTmaWarp + 1) * 32;   // 672: one-CTA form (the builders issue the MMAs)
-constexpr int kBuildBar = 1;                       // named barrier of the builders
+constexpr int kMmaWarp = kTmaWarp + 1;             // 21
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
 constexpr int kBuildGroups = kBuildWarps / 4;      // builder warps per lane quarter
 constexpr int kHalfAtoms = kStageSlots / 2 / kBuildGroups;  // atoms of a half-stage per builder warp
@@ -256,22 +258,6 @@ __device__ __forceinline__ void tmem_st_cols(uint32_t taddr, const uint32_t (&r)
 
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// Barrier of the builder warps that returns, to every one of them, whether any passed `stop`: other
-// roles can raise the abort flag at any time, so the builders branch on the value reduced here, never
-// on separate reads of the flag, and all of them take the same path through the same barriers.
-__device__ __forceinline__ bool builders_sync_any(bool stop) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, %2, %3, q;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)stop), "n"(kBuildBar), "n"(kBuildWarps * 32)
-        : "memory");
-    return r != 0;
-}
-
 __device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
 
 // e^{i pi f} for the fixed-point phase ph (f = ph / 2^31 in [-1, 1)).
@@ -389,13 +375,14 @@ __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t*
 
 // ---- the contraction kernel ------------------------------------------------
 
-__global__ void __launch_bounds__(kTc1Threads, 1)
+__global__ void __launch_bounds__(kTcThreads, 1)
     sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t empty_a[kMaxABufs], xy_full[2], xy_empty[2], acc_full, acc_empty, mma_done;
+    __shared__ __align__(8) uint64_t full_a[kMaxABufs], empty_a[kMaxABufs], xy_full[2], xy_empty[2], acc_full,
+        acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -416,7 +403,10 @@ __global__ void __launch_bounds__(kTc1Threads, 1)
             trj_mbar_init(&full_b[s], 1);
             trj_mbar_init(&empty_b[s], 1);
         }
-        for (int b = 0; b < kMaxABufs; ++b) trj_mbar_init(&empty_a[b], 1);
+        for (int b = 0; b < kMaxABufs; ++b) {
+            trj_mbar_init(&full_a[b], kBuildWarps);
+            trj_mbar_init(&empty_a[b], 1);
+        }
         for (int b = 0; b < 2; ++b) {
             trj_mbar_init(&xy_full[b], kXyWarps);
             trj_mbar_init(&xy_empty[b], kBuildWarps);
@@ -426,7 +416,7 @@ __global__ void __launch_bounds__(kTc1Threads, 1)
         trj_mbar_init(&mma_done, 1);
         trj_fence_mbar_init();
     }
-    if (warp == kTmaWarp) {
+    if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          trj_smem_addr(&tmem_slot)),
                      "r"(kTmemCols)
@@ -488,6 +478,82 @@ __global__ void __launch_bounds__(kTc1Threads, 1)
                 }
                 trj_mbar_wait(&full_b[slot], phase);
             }
+        }
+    } else if (warp == kMmaWarp) {
+        if (lane == 0) {
+            // B descriptor of stage slot 0; slot k sits k * stage_bytes further (the start-address
+            // field holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds
+            // without carry).  A K-step of 16 bf16 (32 bytes) adds 2; the lo operand of B sits bmax
+            // rows after the hi one.  A K-step of A in TMEM is 8 columns.
+            const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
+            const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
+            const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
+            int slot = 0, fg = 0, ab = 0;
+            unsigned phase = 0, aphase = 0;  // B ring phase; A ring (NA half-stage buffers) phase
+            uint64_t bh = b0desc;            // B descriptor of the current slot
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cta_items[li];
+                const TcTile T = p.tiles[it % p.ntiles];
+                const TcChunk C = p.chunks[it / p.ntiles];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
+                                       ((uint32_t)(128 >> 4) << 24);
+                int rs = 0;  // stage within the current run
+                for (int s = 0; s < nst; ++s) {
+                    const bool first = rs == 0;
+                    // the epilogue must have read the previous run out of the accumulator
+                    if (first && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    if (!timed_wait(&full_b[slot], phase, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    const uint64_t bl = bh + b_lo;
+                    bool ok = true;
+                    for (int hh = 0; hh < 2 && ok; ++hh) {
+                        const int hb = ab;
+                        if (!timed_wait(&full_a[hb], aphase, p.status)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t ah = tmem + p.a_col + (uint32_t)(32 * hb), al = ah + 16;
+#pragma unroll
+                        for (int k2 = 0; k2 < 2; ++k2) {
+                            const int kk = 2 * hh + k2;
+                            mma_ts(tmem, ah + 8 * k2, bh + 2 * kk, idesc, (first && kk == 0) ? 0u : 1u);
+                            mma_ts(tmem, ah + 8 * k2, bl + 2 * kk, idesc, 1u);
+                            mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
+                        }
+                        mma_commit(&empty_a[hb]);
+                        if (++ab == NA) {
+                            ab = 0;
+                            aphase ^= 1;
+                        }
+                    }
+                    if (!ok) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    mma_commit(&empty_b[slot]);
+                    if (++rs == F || s == nst - 1) {
+                        mma_commit(&acc_full);
+                        ++fg;
+                        rs = 0;
+                    }
+                    bh += b_step;
+                    if (++slot == NS) {
+                        slot = 0;
+                        phase ^= 1;
+                        bh = b0desc;
+                    }
+                }
+            }
+            // every MMA of this CTA has completed before TMEM is released
+            mma_commit(&mma_done);
+            trj_mbar_wait(&mma_done, 0);
         }
     } else if (warp >= kEpiWarp0) {
         // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
@@ -573,111 +639,59 @@ __global__ void __launch_bounds__(kTc1Threads, 1)
         }
     } else {
         // ---- A builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
-        //      half-stage buffer, the K-columns of atoms [kHalfAtoms*(w/4), kHalfAtoms*(w/4 + 1)).  After
-        //      each half-stage the builders meet at a named barrier and one thread (warp 0, lane 0)
-        //      issues its six MMAs: no handoff to a separate MMA warp ----
+        //      half-stage buffer, the K-columns of atoms [kHalfAtoms*(w/4), kHalfAtoms*(w/4 + 1)) ----
         const int q = warp & 3, g = warp >> 2;
         const int m = 32 * q + lane;
         const int nxl = m & 15, nyl = m >> 4;
         const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        const bool issuer = tid == 0;
-        // issuer state: B descriptor of stage slot 0 (slot k sits k * stage_bytes further: the start-address
-        // field holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds without
-        // carry); a K-step of 16 bf16 (32 bytes) adds 2; the lo rows of B sit bmax rows after the hi rows;
-        // a K-step of A in TMEM is 8 columns
-        const uint64_t b0desc = sw128_desc(trj_smem_addr(stage_ptr(0)));
-        const uint64_t b_lo = (uint64_t)((p.bmax * 128) >> 4);
-        const uint64_t b_step = (uint64_t)(p.stage_bytes >> 4);
-        uint64_t bh = b0desc;
-        int sg = 0, ab = 0, slot = 0, fg = 0, rs = 0;
-        unsigned aphase = 0;  // A ring (NA half-stage buffers)
+        int sg = 0, ab = 0;
+        unsigned aphase = 0;  // A ring (NA half-stage buffers), in the MMA warp's order
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
-            const TcTile T = p.tiles[it % p.ntiles];
             const TcChunk C = p.chunks[it / p.ntiles];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T.ncols >> 3) << 17) |
-                                   ((uint32_t)(128 >> 4) << 24);
-            for (int s = 0; s < nst; ++s, ++sg) {
+            for (int s = 0; s < nst && !stop; ++s, ++sg) {
                 const int xb = sg & 1;
-                // this stage's X/Y factors (their warps waited for the stage's B rows and phases first,
-                // so the B operand has landed too)
-                if (!trj_mbar_wait(&xy_full[xb], (sg >> 1) & 1)) {
-                    trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                const bool ok = trj_mbar_wait(&xy_full[xb], (sg >> 1) & 1);
+                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
+                    stop = true;
+                    break;
                 }
                 const float2* xs = xy_ptr(xb);
-                const bool first = rs == 0;
                 for (int hh = 0; hh < 2; ++hh) {
-                    if (!trj_mbar_wait(&empty_a[ab], aphase ^ 1)) {
-                        trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    const int hb = ab;
+                    if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], aphase ^ 1))) {
+                        if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                         abort_flag = 1;
+                        stop = true;
+                        break;
                     }
                     tc_fence_after();
                     uint32_t hw[kHalfAtoms], lw[kHalfAtoms];
                     build_row<kHalfAtoms>(xs, nxl, nyl, 16 * hh + kHalfAtoms * g, hw, lw);
-                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * ab + kHalfAtoms * g);
+                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + kHalfAtoms * g);
                     tmem_st_cols<kHalfAtoms>(ta, hw);
                     tmem_st_cols<kHalfAtoms>(ta + 16, lw);
                     tmem_wait_st();
                     tc_fence_before();
-                    if (builders_sync_any(abort_flag != 0)) {
-                        stop = true;
-                        break;
-                    }
-                    if (issuer) {
-                        tc_fence_after();
-                        // the epilogue must have read the previous run out of the accumulator
-                        if (first && hh == 0 && fg >= 1 && !timed_wait(&acc_empty, (fg - 1) & 1, p.status))
-                            abort_flag = 1;
-                        const uint32_t ah = tmem + p.a_col + (uint32_t)(32 * ab), al = ah + 16;
-                        const uint64_t bl = bh + b_lo;
-#pragma unroll
-                        for (int k2 = 0; k2 < 2; ++k2) {
-                            const int kk = 2 * hh + k2;
-                            mma_ts(tmem, ah + 8 * k2, bh + 2 * kk, idesc, (first && kk == 0) ? 0u : 1u);
-                            mma_ts(tmem, ah + 8 * k2, bl + 2 * kk, idesc, 1u);
-                            mma_ts(tmem, al + 8 * k2, bh + 2 * kk, idesc, 1u);
-                        }
-                        mma_commit(&empty_a[ab]);
-                    }
+                    __syncwarp();
+                    if (lane == 0) trj_mbar_arrive(&full_a[hb]);
                     if (++ab == NA) {
                         ab = 0;
                         aphase ^= 1;
                     }
                 }
-                if (stop) break;
-                // the X/Y buffer is free again; the stage's B slot once its MMAs have completed
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&xy_empty[xb]);
-                const bool run_end = rs + 1 == F || s == nst - 1;
-                if (issuer) {
-                    mma_commit(&empty_b[slot]);
-                    if (run_end) mma_commit(&acc_full);
-                }
-                if (run_end) {
-                    ++fg;
-                    rs = 0;
-                } else {
-                    ++rs;
-                }
-                bh += b_step;
-                if (++slot == NS) {
-                    slot = 0;
-                    bh = b0desc;
-                }
             }
-        }
-        if (issuer) {
-            // every MMA of this CTA has completed before TMEM is released
-            mma_commit(&mma_done);
-            trj_mbar_wait(&mma_done, 0);
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == kTmaWarp) {
+    if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -1500,7 +1514,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         plan->timer.end(ctx, s);
     } else {
         plan->timer.begin(ctx, s);
-        sq_tc_kernel<<<st->grid, kTc1Threads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
+        sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
                                                                   st->map_lo64, P);
         plan->timer.end(ctx, s);
     }
