@@ -58,7 +58,12 @@ constexpr int kXyWarp0 = kBuildWarps;
 constexpr int kEpiWarp0 = kXyWarp0 + kXyWarps;
 constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
 constexpr int kMmaWarp = kTmaWarp + 1;             // 21
-constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704
+constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704 (CTA-pair form)
+// One-CTA form: the X/Y factors come from per-frame tables with the B rows, so it has no factor warps.
+constexpr int k1EpiWarp0 = kBuildWarps;            // warps 8-15: accumulator drains
+constexpr int k1TmaWarp = k1EpiWarp0 + kEpiWarps;  // 16
+constexpr int k1MmaWarp = k1TmaWarp + 1;           // 17
+constexpr int k1Threads = (k1MmaWarp + 1) * 32;    // 576
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
 constexpr int kBuildGroups = kBuildWarps / 4;      // builder warps per lane quarter
 constexpr int kHalfAtoms = kStageSlots / 2 / kBuildGroups;  // atoms of a half-stage per builder warp
@@ -70,6 +75,10 @@ constexpr int kXBytes = kXyRow * kTcTileNx * 8;  // X factors [16 nx][kXyRow] as
 constexpr int kYBytes = kXyRow * kTcTileNy * 8;  // Y factors [8 ny][kXyRow] as (yr, yi)
 constexpr int kXyBytes = kXBytes + kYBytes;           // one of the two X/Y buffers
 constexpr int kUxyBytes = kStageSlots * 8;            // 32 atoms x (ux, uy)
+// Factor blocks of one stage in the one-CTA form: [16 atom pairs][16 nx (8 ny)] x (re, im) of the pair's
+// two atoms, the order in which the builders read them.
+constexpr int kXBlockBytes = kStageSlots / 2 * kTcTileNx * 16;  // 4096
+constexpr int kYBlockBytes = kStageSlots / 2 * kTcTileNy * 16;  // 2048
 constexpr int kMaxStages = 8;
 constexpr int kChunkAtoms = 12288;  // atom slots per chunk: the Z-table rows of one chunk are ~10 MB
 constexpr int kMaxTileCols = 224;
@@ -112,6 +121,9 @@ struct TcParams {
     int table_rows;  // Z-table rows per 32-slot block
     uint32_t sum_col, a_col;  // TMEM columns of the running sum and of the first A buffer
     int nabuf;                // A half-stage buffers
+    const float4* xtab;       // X factor blocks [stage][nx block][pair][16]
+    const float4* ytab;       // Y factor blocks [stage][ny block][pair][8]
+    int nxb, nyb, nx0min, ny0min;
     unsigned* status;
 };
 
@@ -157,6 +169,9 @@ struct TcState {
     __nv_bfloat16* tab_hi = nullptr;
     __nv_bfloat16* tab_lo = nullptr;
     uint2* uxy = nullptr;
+    float4* xtab = nullptr;  // X/Y factor blocks of the one-CTA form
+    float4* ytab = nullptr;
+    int nxb = 0, nyb = 0, nx0min = 0, ny0min = 0;
     double* part = nullptr;
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
@@ -373,16 +388,55 @@ __global__ void tc_ztable_kernel(const uint4* __restrict__ phase, const int64_t*
     }
 }
 
+// X and Y factors of every 32-slot stage, per block of 16 nx (8 ny) values of the tiles, in the order
+// the builders read them: [stage][block][atom pair][value of the block] x (re, im) of the pair's two
+// atoms.  Consecutive threads take consecutive values of one pair: the stores of a warp are contiguous.
+__global__ void tc_xytable_kernel(const uint2* __restrict__ uxy, int64_t nstage, int nxb, int nx0min, int nyb,
+                                  int ny0min, float4* __restrict__ xtab, float4* __restrict__ ytab) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nxe = nstage * nxb * (kStageSlots / 2) * kTcTileNx;
+    const int64_t nye = nstage * nyb * (kStageSlots / 2) * kTcTileNy;
+    if (e < nxe) {
+        const int v = (int)(e & (kTcTileNx - 1)), pair = (int)((e / kTcTileNx) & (kStageSlots / 2 - 1));
+        const int64_t sb = e / (kTcTileNx * kStageSlots / 2);
+        const int b = (int)(sb % nxb);
+        const int64_t slot = (sb / nxb) * kStageSlots + 2 * pair;
+        const unsigned n = (unsigned)(nx0min + kTcTileNx * b + v);
+        const float2 f0 = phase_factor(n * uxy[slot].x), f1 = phase_factor(n * uxy[slot + 1].x);
+        xtab[e] = make_float4(f0.x, f0.y, f1.x, f1.y);
+    } else if (e < nxe + nye) {
+        const int64_t f = e - nxe;
+        const int v = (int)(f & (kTcTileNy - 1)), pair = (int)((f / kTcTileNy) & (kStageSlots / 2 - 1));
+        const int64_t sb = f / (kTcTileNy * kStageSlots / 2);
+        const int b = (int)(sb % nyb);
+        const int64_t slot = (sb / nyb) * kStageSlots + 2 * pair;
+        const unsigned n = (unsigned)(ny0min + kTcTileNy * b + v);
+        const float2 f0 = phase_factor(n * uxy[slot].y), f1 = phase_factor(n * uxy[slot + 1].y);
+        ytab[f] = make_float4(f0.x, f0.y, f1.x, f1.y);
+    }
+}
+
+// The hi and lo BF16 pairs of A for row (nxl, nyl) and the 8 atoms of pairs p0 .. p0 + 3 from a stage's
+// factor blocks (lanes of one quarter-warp read consecutive 16-byte entries: no bank conflicts).
+__device__ __forceinline__ void build_row_tab(const float4* xb, const float4* yb, int nxl, int nyl, int p0,
+                                              uint32_t (&hw)[8], uint32_t (&lw)[8]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 x = xb[(p0 + k) * kTcTileNx + nxl], y = yb[(p0 + k) * kTcTileNy + nyl];
+        product_split(x.x, x.y, y.x, y.y, hw[2 * k], lw[2 * k]);
+        product_split(x.z, x.w, y.z, y.w, hw[2 * k + 1], lw[2 * k + 1]);
+    }
+}
+
 // ---- the contraction kernel ------------------------------------------------
 
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(k1Threads, 1)
     sq_tc_kernel(const __grid_constant__ CUtensorMap map_hi, const __grid_constant__ CUtensorMap map_lo,
                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t full_a[kMaxABufs], empty_a[kMaxABufs], xy_full[2], xy_empty[2], acc_full,
-        acc_empty, mma_done;
+    __shared__ __align__(8) uint64_t full_a[kMaxABufs], empty_a[kMaxABufs], acc_full, acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -392,10 +446,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int NA = p.nabuf;
     const int F = p.flush_stages;
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
-    // stage layout: B hi [bmax rows x 128 B], B lo, x/y phases of the stage's atoms
+    // stage layout: B hi [bmax rows x 128 B], B lo, the X factor block, the Y factor block
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
-    // X/Y buffer b: [16 nx][32 atoms] X factors, then [8 ny][32 atoms] Y factors (fill_xy)
-    auto xy_ptr = [&](int b) { return reinterpret_cast<float2*>(smem + (size_t)NS * p.stage_bytes + b * kXyBytes); };
 
     if (tid == 0) {
         abort_flag = 0;
@@ -407,16 +459,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             trj_mbar_init(&full_a[b], kBuildWarps);
             trj_mbar_init(&empty_a[b], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            trj_mbar_init(&xy_full[b], kXyWarps);
-            trj_mbar_init(&xy_empty[b], kBuildWarps);
-        }
         trj_mbar_init(&acc_full, 1);
         trj_mbar_init(&acc_empty, kEpiWarps);
         trj_mbar_init(&mma_done, 1);
         trj_fence_mbar_init();
     }
-    if (warp == kMmaWarp) {
+    if (warp == k1MmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          trj_smem_addr(&tmem_slot)),
                      "r"(kTmemCols)
@@ -428,7 +476,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (warp == kTmaWarp) {
+    if (warp == k1TmaWarp) {
         if (lane == 0) {
             // ring position of the next stage (slot, phase) kept incrementally: no divisions per stage
             int slot = 0, issued = 0;
@@ -438,7 +486,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const TcTile T = p.tiles[it % p.ntiles];
                 const TcChunk C = p.chunks[it / p.ntiles];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
-                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kUxyBytes);
+                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kXBlockBytes + kYBlockBytes);
+                const int bx = (T.nx0 - p.nx0min) / kTcTileNx, by = (T.ny0 - p.ny0min) / kTcTileNy;
                 const int n64 = T.ncols / 64;  // B rows as 64-row boxes, then 16-row boxes
                 for (int s = 0; s < nst; ++s) {
                     if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     }
                     uint8_t* bh = stage_ptr(slot);
                     uint8_t* bl = bh + p.bmax * 128;
-                    uint8_t* ux = bl + p.bmax * 128;
+                    uint8_t* xf = bl + p.bmax * 128;
                     trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
                     // rows of this stage's 32-slot block: contiguous 128-byte rows from row0
@@ -461,7 +510,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         tma_load_2d(bh + r * 128, &map_hi, 0, row0 + r, &full_b[slot]);
                         tma_load_2d(bl + r * 128, &map_lo, 0, row0 + r, &full_b[slot]);
                     }
-                    trj_bulk_g2s(ux, p.uxy + slot0, kUxyBytes, &full_b[slot]);
+                    const int64_t stg = slot0 / kStageSlots;
+                    trj_bulk_g2s(xf, p.xtab + (stg * p.nxb + bx) * (kXBlockBytes / 16), kXBlockBytes, &full_b[slot]);
+                    trj_bulk_g2s(xf + kXBlockBytes, p.ytab + (stg * p.nyb + by) * (kYBlockBytes / 16), kYBlockBytes,
+                                 &full_b[slot]);
                     ++issued;
                     if (++slot == NS) {
                         slot = 0;
@@ -479,7 +531,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 trj_mbar_wait(&full_b[slot], phase);
             }
         }
-    } else if (warp == kMmaWarp) {
+    } else if (warp == k1MmaWarp) {
         if (lane == 0) {
             // B descriptor of stage slot 0; slot k sits k * stage_bytes further (the start-address
             // field holds addr >> 4 in 14 bits, which covers all of shared memory, so the offset adds
@@ -555,11 +607,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mma_commit(&mma_done);
             trj_mbar_wait(&mma_done, 0);
         }
-    } else if (warp >= kEpiWarp0) {
+    } else if (warp >= k1EpiWarp0) {
         // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
         //      last run writes (sum + run) to this CTA's FP64 block once ----
         const int q4 = warp & 3;
-        const int c0 = 16 * ((warp - kEpiWarp0) >> 2);  // first 16-column chunk of this warp
+        const int c0 = 16 * ((warp - k1EpiWarp0) >> 2);  // first 16-column chunk of this warp
         const int row = 32 * q4 + lane;
         const uint32_t lanes = (uint32_t)(32 * q4) << 16;
         int fg = 0;
@@ -606,37 +658,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (lane == 0) trj_mbar_arrive(&acc_empty);
             }
         }
-    } else if (warp >= kXyWarp0) {
-        // ---- X/Y factors of each stage from the x/y phases that arrived with its B rows ----
-        const int xt = tid - kXyWarp0 * 32;
-        int sg = 0, slot = 0;
-        unsigned phase = 0;
-        bool stop = false;
-        for (int li = item0; li < item1 && !stop; ++li) {
-            const int it = p.cta_items[li];
-            const TcTile T = p.tiles[it % p.ntiles];
-            const TcChunk C = p.chunks[it / p.ntiles];
-            const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            for (int s = 0; s < nst; ++s, ++sg) {
-                const int xb = sg & 1;
-                bool ok = trj_mbar_wait(&full_b[slot], phase);
-                ok = ok && trj_mbar_wait(&xy_empty[xb], ((sg >> 1) & 1) ^ 1);
-                if (__any_sync(0xffffffffu, !ok || abort_flag)) {
-                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                    abort_flag = 1;
-                    stop = true;
-                    break;
-                }
-                const uint2* u = reinterpret_cast<const uint2*>(stage_ptr(slot) + 2 * p.bmax * 128);
-                fill_xy(xy_ptr(xb), u, T.nx0, T.ny0, xt, kXyWarps * 32);
-                __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&xy_full[xb]);
-                if (++slot == NS) {
-                    slot = 0;
-                    phase ^= 1;
-                }
-            }
-        }
     } else {
         // ---- A builders (warps 0-7): warp w writes TMEM lanes 32*(w%4).. (A rows m) and, in each
         //      half-stage buffer, the K-columns of atoms [kHalfAtoms*(w/4), kHalfAtoms*(w/4 + 1)) ----
@@ -644,23 +665,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int m = 32 * q + lane;
         const int nxl = m & 15, nyl = m >> 4;
         const uint32_t lanes = (uint32_t)(32 * q) << 16;
-        int sg = 0, ab = 0;
-        unsigned aphase = 0;  // A ring (NA half-stage buffers), in the MMA warp's order
+        int ab = 0, slot = 0;
+        unsigned aphase = 0, phase = 0;  // A ring (NA half-stage buffers) in the MMA warp's order; B ring
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
             const TcChunk C = p.chunks[it / p.ntiles];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
-            for (int s = 0; s < nst && !stop; ++s, ++sg) {
-                const int xb = sg & 1;
-                const bool ok = trj_mbar_wait(&xy_full[xb], (sg >> 1) & 1);
+            for (int s = 0; s < nst && !stop; ++s) {
+                // the stage's B rows and factor blocks (released by the MMA warp's commit, which follows
+                // this stage's full_a arrivals and so every read below)
+                const bool ok = trj_mbar_wait(&full_b[slot], phase);
                 if (__any_sync(0xffffffffu, !ok || abort_flag)) {
                     if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
                     stop = true;
                     break;
                 }
-                const float2* xs = xy_ptr(xb);
+                const float4* xf = reinterpret_cast<const float4*>(stage_ptr(slot) + 2 * p.bmax * 128);
+                const float4* yf = xf + kXBlockBytes / 16;
                 for (int hh = 0; hh < 2; ++hh) {
                     const int hb = ab;
                     if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], aphase ^ 1))) {
@@ -671,7 +694,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     }
                     tc_fence_after();
                     uint32_t hw[kHalfAtoms], lw[kHalfAtoms];
-                    build_row<kHalfAtoms>(xs, nxl, nyl, 16 * hh + kHalfAtoms * g, hw, lw);
+                    build_row_tab(xf, yf, nxl, nyl, (16 * hh + kHalfAtoms * g) / 2, hw, lw);
                     const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + kHalfAtoms * g);
                     tmem_st_cols<kHalfAtoms>(ta, hw);
                     tmem_st_cols<kHalfAtoms>(ta + 16, lw);
@@ -684,14 +707,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         aphase ^= 1;
                     }
                 }
-                __syncwarp();
-                if (lane == 0) trj_mbar_arrive(&xy_empty[xb]);
+                if (++slot == NS) {
+                    slot = 0;
+                    phase ^= 1;
+                }
             }
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == kMmaWarp) {
+    if (warp == k1MmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
@@ -1168,7 +1193,7 @@ void trj_sq_tc_release(trj_sq_plan* plan) {
     if (!st) return;
     void* ptrs[] = {st->sched_dev, st->tiles_dev, st->chunks_dev, st->pad_off_dev, st->chunk_begin_dev,
                     st->tab_hi,    st->tab_lo,    st->uxy,        st->part,           st->pairs_dev,
-                    st->sched2_dev};
+                    st->sched2_dev, st->xtab,     st->ytab};
     for (void* q : ptrs) trj_dev_free(plan->ctx, q);
     delete st;
     plan->tc_state = nullptr;
@@ -1345,11 +1370,24 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     st->chunk_of_species_begin[nsp] = (int)st->chunks.size();
     if (st->chunks.empty()) return TRJ_OK;
     // shared memory: a ring of B stages (hi, lo, x/y phases), then the two X/Y factor buffers
-    st->stage_bytes = (2 * st->bmax * 128 + kUxyBytes + 1023) / 1024 * 1024;
-    const int avail = (int)ctx->smem_optin - 2048 - 2 * kXyBytes;
+    // shared memory: a ring of stages, each B hi, B lo and the stage's X and Y factor blocks
+    st->stage_bytes = (2 * st->bmax * 128 + kXBlockBytes + kYBlockBytes + 1023) / 1024 * 1024;
+    const int avail = (int)ctx->smem_optin - 2048;
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
-    st->smem_bytes = st->nstages * st->stage_bytes + 2 * kXyBytes + 1024;
+    st->smem_bytes = st->nstages * st->stage_bytes + 1024;
+    // X/Y factor blocks: every 16-nx (8-ny) block a tile starts at
+    int nxmax = tt[0].nx0, nymax = tt[0].ny0;
+    st->nx0min = tt[0].nx0;
+    st->ny0min = tt[0].ny0;
+    for (const TcTile& t : tt) {
+        st->nx0min = std::min(st->nx0min, t.nx0);
+        st->ny0min = std::min(st->ny0min, t.ny0);
+        nxmax = std::max(nxmax, t.nx0);
+        nymax = std::max(nymax, t.ny0);
+    }
+    st->nxb = (nxmax - st->nx0min) / kTcTileNx + 1;
+    st->nyb = (nymax - st->ny0min) / kTcTileNy + 1;
     const int64_t nitems = (int64_t)ntiles * (int64_t)st->chunks.size();
     st->grid = (int)std::min<int64_t>(nitems, ctx->sm_count);
     // Schedule: the items in chunk-major order are cut into windows of `grid` items; within a window
@@ -1387,18 +1425,24 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     const int64_t kdim = 2 * st->total_slots;
     size_t tab_bytes = (size_t)st->table_rows * (size_t)kdim * sizeof(__nv_bfloat16);
     size_t uxy_bytes = sizeof(uint2) * (size_t)st->total_slots;
+    const int64_t nstage_tot = st->total_slots / kStageSlots;
+    const size_t xtab_bytes = (size_t)nstage_tot * st->nxb * kXBlockBytes;
+    const size_t ytab_bytes = (size_t)nstage_tot * st->nyb * kYBlockBytes;
     size_t part_bytes = sizeof(double) * (size_t)st->acc_stride * st->chunks.size();
     std::vector<int32_t> cb(st->chunk_of_species_begin.begin(), st->chunk_of_species_begin.end());
     if (trj_dev_alloc(ctx, (void**)&st->tab_hi, tab_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->tab_lo, tab_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->uxy, uxy_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->xtab, xtab_bytes) != cudaSuccess ||
+        trj_dev_alloc(ctx, (void**)&st->ytab, ytab_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->part, part_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->tiles_dev, sizeof(TcTile) * tt.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunks_dev, sizeof(TcChunk) * st->chunks.size()) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->pad_off_dev, sizeof(int64_t) * (2 * nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->chunk_begin_dev, sizeof(int32_t) * (nsp + 1)) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->sched_dev, sizeof(int32_t) * sched.size()) != cudaSuccess)
-        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables", 2 * tab_bytes + uxy_bytes + part_bytes);
+        return trj_fail(ctx, TRJ_ERR_NOMEM, "tensor path: %zu bytes of tables",
+                        2 * tab_bytes + uxy_bytes + xtab_bytes + ytab_bytes + part_bytes);
     cudaMemcpy(st->tiles_dev, tt.data(), sizeof(TcTile) * tt.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunks_dev, st->chunks.data(), sizeof(TcChunk) * st->chunks.size(), cudaMemcpyHostToDevice);
     // pad offsets, then the per-species slot -> atom multipliers
@@ -1420,7 +1464,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     cudaMemcpy(st->pad_off_dev, pad_mul.data(), sizeof(int64_t) * (2 * nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->chunk_begin_dev, cb.data(), sizeof(int32_t) * (nsp + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(st->sched_dev, sched.data(), sizeof(int32_t) * sched.size(), cudaMemcpyHostToDevice);
-    plan->scratch_bytes += (int64_t)(2 * tab_bytes + uxy_bytes + part_bytes);
+    plan->scratch_bytes += (int64_t)(2 * tab_bytes + uxy_bytes + xtab_bytes + ytab_bytes + part_bytes);
     // Blocked table: [total_slots / 32][table_rows][64 bf16] as a 2-D map of 128-byte rows.
     const int64_t brows = (st->total_slots / kStageSlots) * (int64_t)st->table_rows;
     int rc = encode_map(ctx, &st->map_hi, st->tab_hi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, 64, brows, 64, 16,
@@ -1455,6 +1499,14 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
                                         st->total_slots, st->nz_min, nz_count, (int64_t)st->table_rows, st->tab_hi,
                                         st->tab_lo, st->uxy,
                                         plan->qsp >= 0 ? plan->n_atoms : INT64_MAX);
+    const bool pair_form = st->pairs_ok && st->use_pairs;
+    if (!pair_form) {  // the one-CTA form reads its X/Y factors from per-frame blocks
+        const int64_t nstage_tot = st->total_slots / kStageSlots;
+        const int64_t nent = nstage_tot * (st->nxb * (kStageSlots / 2) * kTcTileNx + st->nyb * (kStageSlots / 2) * kTcTileNy);
+        tc_xytable_kernel<<<(unsigned)((nent + 255) / 256), 256, 0, s>>>(st->uxy, nstage_tot, st->nxb, st->nx0min,
+                                                                         st->nyb, st->ny0min, st->xtab, st->ytab);
+        ctx->launches += 1;
+    }
     TcParams P;
     P.tiles = st->tiles_dev;
     P.chunks = st->chunks_dev;
@@ -1473,11 +1525,17 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.sum_col = (uint32_t)st->bmax;
     P.a_col = (uint32_t)(2 * st->bmax);
     P.nabuf = st->nabuf;
+    P.xtab = st->xtab;
+    P.ytab = st->ytab;
+    P.nxb = st->nxb;
+    P.nyb = st->nyb;
+    P.nx0min = st->nx0min;
+    P.ny0min = st->ny0min;
     P.status = ctx->status_dev;
     // The attribute is per kernel, shared by all plans: set this plan's size right before its launch.
     TRJ_CUDA_TRY(ctx, cudaFuncSetAttribute(sq_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            st->smem_bytes));
-    if (st->pairs_ok && st->use_pairs) {
+    if (pair_form) {
         Tc2Params Q;
         Q.tiles = st->tiles_dev;
         Q.pairs = st->pairs_dev;
@@ -1514,7 +1572,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
         plan->timer.end(ctx, s);
     } else {
         plan->timer.begin(ctx, s);
-        sq_tc_kernel<<<st->grid, kTcThreads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
+        sq_tc_kernel<<<st->grid, k1Threads, st->smem_bytes, s>>>(st->map_hi, st->map_lo, st->map_hi64,
                                                                   st->map_lo64, P);
         plan->timer.end(ctx, s);
     }
