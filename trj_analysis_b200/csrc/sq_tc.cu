@@ -684,29 +684,51 @@ __global__ void __launch_bounds__(k1Threads, 1)
                 }
                 const float4* xf = reinterpret_cast<const float4*>(stage_ptr(slot) + 2 * p.bmax * 128);
                 const float4* yf = xf + kXBlockBytes / 16;
-                for (int hh = 0; hh < 2; ++hh) {
-                    const int hb = ab;
-                    if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb], aphase ^ 1))) {
-                        if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
-                        abort_flag = 1;
-                        stop = true;
-                        break;
-                    }
-                    tc_fence_after();
-                    uint32_t hw[kHalfAtoms], lw[kHalfAtoms];
-                    build_row_tab(xf, yf, nxl, nyl, (16 * hh + kHalfAtoms * g) / 2, hw, lw);
-                    const uint32_t ta = tmem + lanes + p.a_col + (uint32_t)(32 * hb + kHalfAtoms * g);
-                    tmem_st_cols<kHalfAtoms>(ta, hw);
-                    tmem_st_cols<kHalfAtoms>(ta + 16, lw);
-                    tmem_wait_st();
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) trj_mbar_arrive(&full_a[hb]);
-                    if (++ab == NA) {
-                        ab = 0;
-                        aphase ^= 1;
-                    }
+                // Half-stage 0 is built and stored, half-stage 1 built while those stores drain; then
+                // each half is released to the MMA warp once its own stores are complete.
+                const int hb0 = ab;
+                if (!__all_sync(0xffffffffu, trj_mbar_wait(&empty_a[hb0], aphase ^ 1))) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
                 }
+                if (++ab == NA) {
+                    ab = 0;
+                    aphase ^= 1;
+                }
+                tc_fence_after();
+                uint32_t hw[kHalfAtoms], lw[kHalfAtoms];
+                build_row_tab(xf, yf, nxl, nyl, (kHalfAtoms * g) / 2, hw, lw);
+                const uint32_t ta0 = tmem + lanes + p.a_col + (uint32_t)(32 * hb0 + kHalfAtoms * g);
+                tmem_st_cols<kHalfAtoms>(ta0, hw);
+                tmem_st_cols<kHalfAtoms>(ta0 + 16, lw);
+                const int hb1 = ab;
+                const bool ok1 = trj_mbar_wait(&empty_a[hb1], aphase ^ 1);
+                if (++ab == NA) {
+                    ab = 0;
+                    aphase ^= 1;
+                }
+                uint32_t hw1[kHalfAtoms], lw1[kHalfAtoms];
+                build_row_tab(xf, yf, nxl, nyl, (16 + kHalfAtoms * g) / 2, hw1, lw1);
+                tmem_wait_st();  // half-stage 0's stores
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&full_a[hb0]);
+                if (!__all_sync(0xffffffffu, ok1)) {
+                    if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
+                    abort_flag = 1;
+                    stop = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ta1 = tmem + lanes + p.a_col + (uint32_t)(32 * hb1 + kHalfAtoms * g);
+                tmem_st_cols<kHalfAtoms>(ta1, hw1);
+                tmem_st_cols<kHalfAtoms>(ta1 + 16, lw1);
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&full_a[hb1]);
                 if (++slot == NS) {
                     slot = 0;
                     phase ^= 1;
