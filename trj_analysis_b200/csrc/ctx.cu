@@ -7,6 +7,7 @@
 
 #include <mutex>
 
+#include "batch.cuh"
 #include "trj_common.cuh"
 
 int trj_fail(trj_ctx* ctx, int code, const char* fmt, ...) {
@@ -219,13 +220,6 @@ __global__ void pack_scan_kernel(int32_t* __restrict__ block_counts, int64_t nbl
     }
 }
 
-// FP32 fold of the reference: r - L*int(r/L), each operation rounded once.
-__device__ __forceinline__ float fold_ref(float r, float L) {
-    float q = __fdiv_rn(r, L);
-    float t = truncf(q);
-    return __fsub_rn(r, __fmul_rn(L, t));
-}
-
 __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t* __restrict__ sp,
                                     int64_t n, int nsp, float Lx, float Ly, float Lz,
                                     const int64_t* __restrict__ block_base,
@@ -256,9 +250,9 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
             for (int w = 0; w < warp; ++w) off += warp_cnt[w][s];
             off += rank;
             float4 v;
-            v.x = fold_ref(xyz[3 * i], Lx);
-            v.y = fold_ref(xyz[3 * i + 1], Ly);
-            v.z = fold_ref(xyz[3 * i + 2], Lz);
+            v.x = trj_fold_ref(xyz[3 * i], Lx);
+            v.y = trj_fold_ref(xyz[3 * i + 1], Ly);
+            v.z = trj_fold_ref(xyz[3 * i + 2], Lz);
             v.w = __int_as_float(s);
             packed[off] = v;
             if (q) qpacked[off] = q[i];  // charges follow their atoms (netcdf.f90:656-658)
@@ -272,6 +266,142 @@ __global__ void pack_scatter_kernel(const float* __restrict__ xyz, const int32_t
             }
             base[threadIdx.x] += tot;
         }
+        __syncthreads();
+    }
+}
+
+
+// ---- fused multi-request launch: frame layout -------------------------------------------------
+//
+// Two passes over units of kBatchChunk atoms of every packed frame, with the arithmetic of
+// pack_count_kernel / pack_scatter_kernel: the count pass reads the staged positions and species
+// (mapped host memory, all loads of a unit issued before any is used), copies them to device memory
+// and counts species per unit; the scatter pass places each atom at its species offset (the plan's
+// offsets plus the counts of the item's earlier units, stable within a unit by warp ranks), folds it
+// and writes its fixed-point phase entry as well.
+__global__ void __launch_bounds__(kBatchThreads) batch_count_kernel(const BatchHeader* __restrict__ hdr,
+                                                                    const BatchItem* __restrict__ items,
+                                                                    const float* __restrict__ xyz,
+                                                                    const int32_t* __restrict__ sp,
+                                                                    float4* __restrict__ raw,
+                                                                    int32_t* __restrict__ chunk_counts,
+                                                                    unsigned* status) {
+    constexpr int kRounds = kBatchChunk / kBatchThreads;
+    __shared__ int cnt[kBatchMaxSpecies];
+    const int nitems = hdr->nitems;
+    const int64_t total = hdr->total_chunk;
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+        const BatchItem& it = items[batch_item_of<&BatchItem::chunk_begin>(items, nitems, u)];
+        const int64_t c = u - it.chunk_begin, off = it.atom_off;
+        const int n = it.n, nsp = it.nsp;
+        if (threadIdx.x < kBatchMaxSpecies) cnt[threadIdx.x] = 0;
+        __syncthreads();
+        float x[kRounds], y[kRounds], z[kRounds];
+        int t[kRounds];
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+            const int64_t i = c * kBatchChunk + r * kBatchThreads + threadIdx.x;
+            if (i < n) {
+                x[r] = xyz[3 * (off + i)];
+                y[r] = xyz[3 * (off + i) + 1];
+                z[r] = xyz[3 * (off + i) + 2];
+                t[r] = sp[off + i];
+            }
+        }
+        bool bad = false;
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+            const int64_t i = c * kBatchChunk + r * kBatchThreads + threadIdx.x;
+            if (i < n) {
+                const bool ok = t[r] >= 0 && t[r] < nsp;
+                if (!ok || !isfinite(x[r]) || !isfinite(y[r]) || !isfinite(z[r])) bad = true;
+                if (ok) atomicAdd(&cnt[t[r]], 1);
+                raw[off + i] = make_float4(x[r], y[r], z[r], __int_as_float(ok ? t[r] : -1));
+            }
+        }
+        if (bad) trj_raise(status, TRJ_DEV_BAD_DATA);
+        __syncthreads();
+        if (threadIdx.x < kBatchMaxSpecies) chunk_counts[u * kBatchMaxSpecies + threadIdx.x] = cnt[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_scatter_kernel(const BatchHeader* __restrict__ hdr,
+                                                                      const BatchItem* __restrict__ items,
+                                                                      const float4* __restrict__ raw,
+                                                                      const int32_t* __restrict__ chunk_counts,
+                                                                      float4* __restrict__ packed,
+                                                                      uint4* __restrict__ phase, unsigned* status) {
+    constexpr int kRounds = kBatchChunk / kBatchThreads;
+    __shared__ int64_t base[kBatchMaxSpecies];
+    __shared__ int warp_cnt[kBatchThreads / 32][kBatchMaxSpecies];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int nitems = hdr->nitems;
+    const int64_t total = hdr->total_chunk;
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+        const BatchItem& it = items[batch_item_of<&BatchItem::chunk_begin>(items, nitems, u)];
+        const int64_t c = u - it.chunk_begin, off = it.atom_off;
+        const int n = it.n, nsp = it.nsp;
+        const bool sorted = it.sp_off[nsp] >= 0;  // -1: g(r) only, atoms keep their order
+        if (threadIdx.x < nsp) {
+            int64_t b = it.sp_off[threadIdx.x];
+            for (int64_t c2 = 0; c2 < c; ++c2) b += chunk_counts[(it.chunk_begin + c2) * kBatchMaxSpecies + threadIdx.x];
+            base[threadIdx.x] = b;
+        }
+        for (int k = threadIdx.x; k < (kBatchThreads / 32) * kBatchMaxSpecies; k += kBatchThreads)
+            (&warp_cnt[0][0])[k] = 0;
+        __syncthreads();
+        const double Lx = (double)it.L[0], Ly = (double)it.L[1], Lz = (double)it.L[2];
+        for (int r = 0; r < kRounds; ++r) {
+            const int64_t i = c * kBatchChunk + r * kBatchThreads + threadIdx.x;
+            int s = -1;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i < n) {
+                v = raw[off + i];
+                s = __float_as_int(v.w);  // -1 for a species flagged by the count pass: dropped
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, s);
+            const int rank = __popc(peers & lt_mask);
+            if (s >= 0 && rank == 0) warp_cnt[warp][s] = __popc(peers);
+            __syncthreads();
+            if (s >= 0) {
+                int64_t pos = i;
+                bool fits = true;
+                if (sorted) {
+                    pos = base[s] + rank;
+                    for (int w = 0; w < warp; ++w) pos += warp_cnt[w][s];
+                    fits = pos < it.sp_off[s + 1];  // more atoms of species s than the plan counts
+                }
+                if (fits) {
+                    float4 f;
+                    f.x = trj_fold_ref(v.x, it.L[0]);
+                    f.y = trj_fold_ref(v.y, it.L[1]);
+                    f.z = trj_fold_ref(v.z, it.L[2]);
+                    f.w = __int_as_float(s);
+                    packed[off + pos] = f;
+                    phase[off + pos] = make_uint4(trj_phase_fraction(f.x, Lx), trj_phase_fraction(f.y, Ly),
+                                                  trj_phase_fraction(f.z, Lz), (unsigned)s);
+                } else {
+                    trj_raise(status, TRJ_DEV_COUNT_MISMATCH);
+                }
+            } else if (!sorted && i < n) {
+                packed[off + i] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));  // no species: never paired
+            }
+            __syncthreads();
+            if (threadIdx.x < nsp) {
+                int tot = 0;
+                for (int w = 0; w < kBatchThreads / 32; ++w) {
+                    tot += warp_cnt[w][threadIdx.x];
+                    warp_cnt[w][threadIdx.x] = 0;
+                }
+                base[threadIdx.x] += tot;
+            }
+            __syncthreads();
+        }
+        // the item's last unit: every species must have filled its range exactly
+        if (sorted && c == it.nchunk - 1 && threadIdx.x < nsp && base[threadIdx.x] != it.sp_off[threadIdx.x + 1])
+            trj_raise(status, TRJ_DEV_COUNT_MISMATCH);
         __syncthreads();
     }
 }
@@ -443,4 +573,11 @@ extern "C" int trj_frame_pack_static(trj_ctx* ctx, const float* xyz_dev, const i
     ctx->launches += 3;
     TRJ_CUDA_TRY(ctx, cudaGetLastError());
     return TRJ_OK;
+}
+
+void trj_batch_launch_layout(const BatchHeader* hdr, const BatchItem* items, const float* xyz_staged,
+                             const int32_t* sp_staged, float4* raw, int32_t* chunk_counts, float4* packed,
+                             uint4* phase, unsigned* status, int grid, cudaStream_t s) {
+    batch_count_kernel<<<grid, kBatchThreads, 0, s>>>(hdr, items, xyz_staged, sp_staged, raw, chunk_counts, status);
+    batch_scatter_kernel<<<grid, kBatchThreads, 0, s>>>(hdr, items, raw, chunk_counts, packed, phase, status);
 }

@@ -38,16 +38,27 @@ __global__ void phase_coords_kernel(const float4* __restrict__ packed, int64_t n
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 v = packed[i];
-    double s[3] = {(double)v.x / Lx, (double)v.y / Ly, (double)v.z / Lz};
-    unsigned u[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double f = s[d] - floor(s[d]);             // [0, 1]
-        u[d] = (unsigned)(long long)rint(f * 4294967296.0);  // 2^32 wraps to 0
-    }
+    unsigned u[3] = {trj_phase_fraction(v.x, Lx), trj_phase_fraction(v.y, Ly), trj_phase_fraction(v.z, Lz)};
     if (zmul) u[2] = u[1] * zmul;
     out[i] = make_uint4(u[0], u[1], u[2], (unsigned)__float_as_int(v.w));
     if (q) out[n + i] = make_uint4(u[0], u[1], u[2], __float_as_uint(q[i]));
+}
+
+// cos and sin of the angle 2 pi ph / 2^32 (ph a 32-bit fixed-point fraction of a turn): the nearest of
+// 256 table angles (the table holds cos, sin of 2 pi k / 256, each rounded once from FP64), rotated by the
+// remainder |theta| <= pi/256 through its Taylor polynomials (theta - theta^3/6; 1 - theta^2/2 +
+// theta^4/24, truncation below 3e-12).  Every step rounds to nearest once, so the error has no
+// systematic part, which matters because it is added once per atom.
+__device__ __forceinline__ void sincos_turn(unsigned ph, const float2* __restrict__ tab, float& sn, float& cs) {
+    const unsigned hi = (ph + 0x800000u) >> 24;         // nearest table angle (mod 256)
+    const int lo = (int)(ph - (hi << 24));               // remainder in [-2^23, 2^23): exact as a float
+    const float th = (float)lo * 1.4629180792671596e-09f;  // 2 pi / 2^32
+    const float t2 = th * th;
+    const float sl = th * fmaf(t2, -0.16666667f, 1.0f);
+    const float cl = fmaf(t2, fmaf(t2, 0.041666668f, -0.5f), 1.0f);
+    const float2 t = tab[hi & 255u];
+    cs = fmaf(t.x, cl, -(t.y * sl));
+    sn = fmaf(t.y, cl, t.x * sl);
 }
 
 // Direct sum: thread owns VPT vectors; block y-index selects a slice of every species.
@@ -58,8 +69,14 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
     const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
     int nsplit, double2* __restrict__ part) {
     __shared__ uint4 atoms[kPlainChunk];
+    __shared__ float2 turn_tab[256];
     const int tid = threadIdx.x;
     const int64_t vbase = (int64_t)blockIdx.x * kPlainThreads * VPT;
+    for (int k = tid; k < 256; k += kPlainThreads) {
+        double sd, cd;
+        sincospi((double)k / 128.0, &sd, &cd);
+        turn_tab[k] = make_float2((float)cd, (float)sd);
+    }  // ordered before the first use by the barrier at the top of the chunk loop
     unsigned nx[VPT], ny[VPT], nz[VPT];
     int vidx[VPT];
 #pragma unroll
@@ -71,7 +88,6 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
         ny[q] = (unsigned)v.y;
         nz[q] = (unsigned)v.z;
     }
-    const float kTurn = 4.656612873077393e-10f;  // 2^-31: the phase as a fraction of pi in [-1, 1)
     for (int a = 0; a < nsp; ++a) {
         int64_t a0 = sp_off[a], a1 = sp_off[a + 1];
         int64_t len = a1 - a0;
@@ -96,11 +112,10 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
 #pragma unroll
                     for (int q = 0; q < VPT; ++q) {
                         unsigned ph = nx[q] * u.x + ny[q] * u.y + nz[q] * u.z;
-                        // sincospif (error within an ulp, no systematic offset): a biased fast
-                        // sine/cosine adds its mean error once per atom, which at 10^6 atoms is a
-                        // few 1e-5 of |rho|^2 on a shell of three vectors
+                        // an unbiased sine/cosine: a biased fast one adds its mean error once per
+                        // atom, which at 10^6 atoms is a few 1e-5 of |rho|^2 on a shell of three vectors
                         float sn, cs;
-                        sincospif(__int2float_rn((int)ph) * kTurn, &sn, &cs);
+                        sincos_turn(ph, turn_tab, sn, cs);
                         fr[q] = fmaf(w, cs, fr[q]);
                         fi[q] = fmaf(w, sn, fi[q]);
                     }

@@ -110,6 +110,21 @@ __host__ __device__ __forceinline__ int trj_pair_row(int a, int b, int nsp) {
     return a * (nsp - 1) - a * (a - 1) / 2 + b;
 }
 
+// FP32 fold of the reference: r - L*int(r/L), each operation rounded once (netcdf.f90:681).
+__device__ __forceinline__ float trj_fold_ref(float r, float L) {
+    float q = __fdiv_rn(r, L);
+    float t = truncf(q);
+    return __fsub_rn(r, __fmul_rn(L, t));
+}
+
+// Fixed-point phase coordinate of a folded coordinate: frac(x / L) as a 32-bit fraction of a turn,
+// rint(frac * 2^32) mod 2^32, in FP64 (so n * u mod 2^32 is the phase of lattice vector n exactly).
+__device__ __forceinline__ unsigned trj_phase_fraction(float x, double L) {
+    const double s = (double)x / L;
+    const double f = s - floor(s);                             // [0, 1]
+    return (unsigned)(long long)rint(f * 4294967296.0);        // 2^32 wraps to 0
+}
+
 // Bound on any mbarrier wait in this library, in SM clocks (2^32 clocks: about 2 s at 2 GHz).
 #define TRJ_WAIT_CLOCKS (1ll << 32)
 // Longest single hardware suspension of a waiting thread (ns); it resumes as soon as the phase
