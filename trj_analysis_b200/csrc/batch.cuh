@@ -16,7 +16,7 @@ constexpr int kBatchThreads = 256;
 constexpr int kBatchMaxSpecies = 16;
 constexpr int kBatchCounters = 4;        // dynamic work counters: pairs, direct sum, reduction, spare
 
-struct BatchItem {
+struct __align__(16) BatchItem {
     // frame: atoms [atom_off, atom_off + n) of the staging and device arrays
     int64_t atom_off;
     int32_t n, nsp;
@@ -47,7 +47,7 @@ struct BatchItem {
     int64_t chunk_begin, pair_begin, sq_begin, red_begin;
 };
 
-struct BatchHeader {
+struct __align__(16) BatchHeader {
     unsigned long long counter[kBatchCounters];  // zero in every turn's copy of the table
     int32_t nitems, pad0;
     int64_t total_chunk, total_pair, total_sq, total_red, total_atoms;
