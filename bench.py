@@ -371,9 +371,16 @@ def run_serving(n_req, seed=5):
         res = srv.run(rq, realtime=realtime)
         return summarize(res, time.perf_counter() - t0)
 
+    warm = reqs[: max(8, n_req // 10)]
     srv = Server(slots=8)
-    timed(srv, [copy.copy(r) for r in reqs[: max(8, n_req // 10)]], False)  # tunes the buckets, warms caches
+    timed(srv, [copy.copy(r) for r in warm], False)  # tunes the buckets, warms caches
+    c0 = (srv.fused_requests, srv.fused_frames, srv.fuse_turns)
     offline = timed(srv, [copy.copy(r) for r in reqs], False)
+    fused_stats = {"fused_requests": srv.fused_requests - c0[0], "fused_frames": srv.fused_frames - c0[1],
+                   "fused_turns": srv.fuse_turns - c0[2], "fuse_max_atoms": srv.fuse_max_atoms,
+                   "batch_device_bytes": srv.batch.device_bytes if srv.batch is not None else 0,
+                   "note": "offline run: requests packed into fused launches, their frames, and the fused "
+                           "launches (each one table copy + five kernels, replayed from a CUDA graph)"}
 
     def poisson(load, seed_):
         rng = np.random.default_rng(seed_)
@@ -390,12 +397,18 @@ def run_serving(n_req, seed=5):
     # arrivals faster than the offline rate: the queue never empties, so the frames/s is what the loop
     # sustains at saturation, with queueing in the latencies
     saturated = timed(srv, poisson(1.25, seed + 2), True)
-    base_srv = Server(slots=1, use_graphs=False, method="plain")
+    # the same loop without fused launches (every request in a slot), for comparison
+    unfused_srv = Server(slots=8, fuse_max_atoms=0)
+    timed(unfused_srv, [copy.copy(r) for r in warm], False)
+    unfused = timed(unfused_srv, [copy.copy(r) for r in reqs], False)
+    base_srv = Server(slots=1, use_graphs=False, method="plain", fuse_max_atoms=0)
     baseline = timed(base_srv, [copy.copy(r) for r in reqs], False)
     return {"workload": f"{n_req} requests, N log-uniform [1e3, 2e5], 1-3 species, cubic or 1:1:2, 1-8 frames, "
                         "deltar 0.02, rcrdf min(L/2, 8), S(Q) reference k-set qmax 12 qmin 3; Poisson arrivals at "
                         "80% (online) and 125% (saturated) of the offline request rate",
-            "offline": offline, "online": online, "saturated": saturated, "per_request_plain_path": baseline,
+            "offline": offline, "online": online, "saturated": saturated, "offline_unfused": unfused,
+            "per_request_plain_path": baseline, "fused": fused_stats,
+            "offline_vs_unfused": offline["frames_per_s"] / unfused["frames_per_s"],
             "online_vs_offline_throughput": online["frames_per_s"] / offline["frames_per_s"],
             "saturated_vs_offline_throughput": saturated["frames_per_s"] / offline["frames_per_s"],
             "offline_vs_plain_path": offline["frames_per_s"] / baseline["frames_per_s"],

@@ -54,6 +54,7 @@ typedef struct trj_ctx trj_ctx;
 typedef struct trj_rdf_plan trj_rdf_plan;
 typedef struct trj_sq_plan trj_sq_plan;
 typedef struct trj_dyn_plan trj_dyn_plan;
+typedef struct trj_batch trj_batch;
 
 /* Edge-pair statistics of one or more accumulate calls (device uint64[4]). */
 enum {
@@ -334,6 +335,53 @@ TRJ_API int trj_dyn_flush(trj_dyn_plan* plan, const uint8_t* done_host, double* 
 /* Duration (ms) of the last self-term kernel launch; needs timing enabled. */
 TRJ_API int trj_dyn_kernel_ms(trj_dyn_plan* plan, float* ms);
 TRJ_API int trj_dyn_plan_destroy(trj_dyn_plan* plan);
+
+/* ---- Fused launches over several small requests ------------------------- */
+/* The reference runs one frame of one system per step of its main loop
+ * (src/main/trj_analysis.f90:208-217: transfer_cpu_gpu, then RDFcomp's rdf_sh
+ * launch rdf.cuf:240 and SQcalc's sqfnD launch sq.cuf:89).  A batch runs one
+ * frame of each of up to max_items requests per turn through one fixed launch
+ * sequence: a copy of the turn's descriptor table, frame layout (fold, species
+ * order, fixed-point phases; select_ncdfinput), an all-pairs histogram with
+ * rdf_sh's arithmetic (rdf.cuf:449-475) and the FP32 direct sum with FP64 shell
+ * sums (the plain method of trj_sq_accumulate), every kernel over the work of
+ * all the turn's frames.  The sequence does not depend on what the table holds,
+ * so a CUDA graph captured once per staging buffer replays every later turn.
+ * Two staging buffers (0, 1) let the host fill one turn while the device runs
+ * the other; the caller orders each buffer's reuse after its previous launch
+ * (an event), since the table and the staged atoms are read when the launch
+ * executes.  Counts are those of trj_rdf_accumulate and S(Q) sums those of
+ * trj_sq_accumulate(TRJ_SQ_PLAIN_FP32) for the same plans, bit for bit.
+ * max_atoms: staged atoms per turn; hist_words: the largest nit*lsmax of a
+ * pair plan the batch takes (shared memory: 8 bytes per word + 4 KB). */
+TRJ_API int trj_batch_create(trj_ctx* ctx, int max_items, int64_t max_atoms, int hist_words, trj_batch** out);
+/* Host staging of buffer buf: xyz[3 * max_atoms] float and species[max_atoms]
+ * int32 (0-based species ids), pinned and mapped into the device's address
+ * space: the layout kernel reads them directly. */
+TRJ_API int trj_batch_staging(trj_batch* batch, int buf, float** xyz_host, int32_t** species_host);
+/* Starts a new turn in buffer buf (no items). */
+TRJ_API int trj_batch_begin(trj_batch* batch, int buf);
+/* Adds one frame of one request: atoms [atom_off, atom_off + n) of the
+ * staging, items in increasing atom order.  rdf: the request's pair plan (its
+ * cutoff, clipped per frame as trj_rdf_accumulate does, bins and species; its
+ * cell arrays are not used, so it may be created with n_max 0) or NULL; sq: its
+ * S(Q) plan (uncharged; species counts summing to n; its partial-sum scratch is
+ * used) or NULL.  Accumulates into hist_dev ([nit][lsmax] uint64), edge_dev
+ * (TRJ_EDGE_* counters, may be NULL) and sq_out_dev ([nbins][nit] double) as
+ * the single-request calls do.  TRJ_ERR_UNSUPPORTED: a plan that runs only
+ * unfused (charged, two-dimensional, nit*lsmax > hist_words, > 16 species). */
+TRJ_API int trj_batch_add(trj_batch* batch, int buf, trj_rdf_plan* rdf, trj_sq_plan* sq, int64_t atom_off,
+                          int64_t n, const float box[3], uint64_t* hist_dev, uint64_t* edge_dev,
+                          double* sq_out_dev);
+/* Enqueues the turn of buffer buf on stream: one table copy and five kernels. */
+TRJ_API int trj_batch_launch(trj_batch* batch, int buf, void* stream);
+/* Items and work units (layout, pair tiles, direct-sum blocks, shell bins) of
+ * buffer buf's turn; device memory the batch holds. */
+TRJ_API int trj_batch_info(const trj_batch* batch, int buf, int* nitems, int64_t units[4], int64_t* device_bytes);
+/* Duration (ms) of the last launched turn's kernels; needs timing enabled. */
+TRJ_API int trj_batch_kernel_ms(trj_batch* batch, float* ms);
+/* Waits for the device, then frees the staging and device memory. */
+TRJ_API int trj_batch_destroy(trj_batch* batch);
 
 #ifdef __cplusplus
 }

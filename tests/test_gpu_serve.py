@@ -90,8 +90,44 @@ def test_cancel_running_and_queued_requests(workload):
 def test_autotuner_picks_method_and_tile_width(workload):
     from trj_analysis_b200.serve import Autotuner, Server
     tuner = Autotuner()
-    srv = Server(slots=2, n_max=1 << 14, autotuner=tuner)
+    srv = Server(slots=2, n_max=1 << 14, autotuner=tuner, fuse_max_atoms=0)
     res = srv.run(workload[:3], realtime=False)
     assert len(res) == 3 and tuner.table
     for e in tuner.table.values():
         assert (e["method"], e["cols"]) in Autotuner.CANDIDATES and e["ms"]
+
+
+def test_fused_requests_match_the_per_request_plain_path(workload):
+    """Small requests packed into fused launches give the bits of the per-request plain method, in a mix
+    with requests that take slots (split method: those above the fused size)."""
+    fused_srv, fused = _run(workload, fuse_max_atoms=3000)
+    assert 0 < fused_srv.fused_requests < len(workload) and fused_srv.fuse_turns > 0
+    _, slots = _run(workload, fuse_max_atoms=0, method="plain")
+    for req in workload:
+        a, b = fused[req.rid], slots[req.rid]
+        assert np.array_equal(a.hist, b.hist)
+        if req.n <= 3000:
+            assert a.method == "plain"
+            assert np.array_equal(a.sq_sums, b.sq_sums)
+
+
+def test_fused_alone_equals_in_mix_and_cancel(workload):
+    """A packed request gives the same bits alone and among others; one cancelled while packed leaves the
+    others unchanged and releases its budget."""
+    from trj_analysis_b200.serve import Server
+    reqs = sorted(workload, key=lambda r: -len(r.frames))[:6]
+    victim = reqs[0].rid
+    assert len(reqs[0].frames) >= 3
+
+    def hook(srv, turn):
+        if turn == 1:
+            srv.cancel(victim)
+
+    srv = Server(slots=2, n_max=1 << 14)
+    res = {r.rid: r for r in srv.run(reqs, realtime=False, on_turn=hook)}
+    assert srv.cancelled == [victim] and victim not in res
+    assert srv.in_use == 0 and srv.fused_requests == len(reqs)
+    for req in reqs[1:4]:
+        _, alone = _run([req], slots=1)
+        assert np.array_equal(alone[req.rid].hist, res[req.rid].hist)
+        assert np.array_equal(alone[req.rid].sq_sums, res[req.rid].sq_sums)

@@ -80,6 +80,14 @@ SIGNATURES = {
     "trj_dyn_flush": (c_int, [vp, vp, vp, vp, vp, vp]),
     "trj_dyn_kernel_ms": (c_int, [vp, P(c_float)]),
     "trj_dyn_plan_destroy": (c_int, [vp]),
+    "trj_batch_create": (c_int, [vp, c_int, c_int64, c_int, P(vp)]),
+    "trj_batch_staging": (c_int, [vp, c_int, P(vp), P(vp)]),
+    "trj_batch_begin": (c_int, [vp, c_int]),
+    "trj_batch_add": (c_int, [vp, c_int, vp, vp, c_int64, c_int64, P(c_float), vp, vp, vp]),
+    "trj_batch_launch": (c_int, [vp, c_int, vp]),
+    "trj_batch_info": (c_int, [vp, c_int, P(c_int), P(c_int64), P(c_int64)]),
+    "trj_batch_kernel_ms": (c_int, [vp, P(c_float)]),
+    "trj_batch_destroy": (c_int, [vp]),
 }
 
 _lib = None

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtrj_sm100.so")
-SOURCES = ["ctx.cu", "rdf.cu", "sq.cu", "sq_tc.cu", "dyn.cu"]
+SOURCES = ["ctx.cu", "rdf.cu", "sq.cu", "sq_tc.cu", "dyn.cu", "batch.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "--expt-relaxed-constexpr",

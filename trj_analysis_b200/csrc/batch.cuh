@@ -73,9 +73,17 @@ __device__ __forceinline__ int batch_item_of(const BatchItem* __restrict__ items
 void trj_batch_launch_layout(const BatchHeader* hdr, const BatchItem* items, const float* xyz_staged,
                              const int32_t* sp_staged, float4* raw, int32_t* chunk_counts, float4* packed,
                              uint4* phase, unsigned* status, int grid, cudaStream_t s);        // ctx.cu
-void trj_batch_launch_pairs(const BatchHeader* hdr, const BatchItem* items, const float4* packed,
-                            int hist_words, int grid, cudaStream_t s);                        // rdf.cu
+void trj_batch_launch_pairs(BatchHeader* hdr, const BatchItem* items, const float4* packed, int hist_words,
+                            int grid, cudaStream_t s);                                        // rdf.cu
 size_t trj_batch_pairs_smem(int hist_words);                                                  // rdf.cu
 int trj_batch_pairs_prepare(int hist_words);                                                  // rdf.cu
-void trj_batch_launch_sq(const BatchHeader* hdr, const BatchItem* items, const uint4* phase, int grid_sq,
-                         int grid_red, cudaStream_t s);                                       // sq.cu
+int trj_batch_pairs_occupancy(int hist_words, int* per_sm);                                   // rdf.cu
+void trj_batch_launch_sq(BatchHeader* hdr, const BatchItem* items, const uint4* phase, int grid_sq, int grid_red,
+                         cudaStream_t s);                                                     // sq.cu
+int trj_batch_sq_occupancy(int* per_sm_sq, int* per_sm_red);                                   // sq.cu
+struct trj_rdf_plan;
+struct trj_sq_plan;
+// Fill the pair part of an item from a plan after the per-frame clip (rdf.cu), and the S(Q) part
+// (sq.cu); non-zero: the plan cannot run in a fused launch (the message is on the context).
+int trj_batch_fill_rdf(trj_rdf_plan* plan, const float box[3], int hist_words, BatchItem* it, int* nsp);
+int trj_batch_fill_sq(trj_sq_plan* plan, int64_t n, BatchItem* it);

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "batch.cuh"
 #include "trj_common.cuh"
 
 namespace {
@@ -724,6 +725,134 @@ __global__ void s2n_kernel(const float4* __restrict__ sorted, const int32_t* __r
     }
 }
 
+
+// ---- fused multi-request launch: all-pairs histogram of every packed frame ---------------------
+//
+// Unit = (item, tile pair bi <= bj) of kBatchTile x kBatchTile atoms of one frame: home atom
+// i = bi * 256 + thread against the staged tile bj (j > i on the diagonal tile), each pair through the
+// general path of the cell kernel (reference minimum image, exact binning near edges), so the counts
+// are those of the reference's all-pairs sweep (rdf.cuf:449-475).  Units come from a global counter;
+// a CTA keeps the counts of one item in two shared replicas (even and odd warps) and merges them into
+// that item's uint64 histogram when its next unit belongs to another item, and at exit.
+template <bool FLOOR>
+__device__ __forceinline__ unsigned batch_tile_pairs(const float4* __restrict__ tile, int jcount, const float4& a,
+                                                     bool has_a, int il, bool diag, int si, const RdfParams& P,
+                                                     const int* rowtab, unsigned* myhist, PairCounters& pc) {
+    unsigned tested = 0;
+    for (int jj = 0; jj < jcount; ++jj) {
+        const bool valid = has_a && (!diag || jj > il);
+        tested += valid ? 1u : 0u;
+        pair<false, FLOOR, false>(a, tile[jj], valid, si, P, rowtab, myhist, pc, nullptr, 0.f, nullptr);
+    }
+    return tested;
+}
+
+__device__ __forceinline__ void batch_pairs_flush(const BatchItem& it, unsigned* hist, int hist_words,
+                                                  PairCounters& pc, unsigned long long& tested) {
+    const int hsz = it.nit * it.lsmax;
+    for (int k = threadIdx.x; k < hsz; k += kBatchThreads) {
+        const unsigned long long v = (unsigned long long)hist[k] + hist[hist_words + k];
+        if (v) atomicAdd(&it.hist[k], v);
+        pc.counted += v;
+        hist[k] = 0u;
+        hist[hist_words + k] = 0u;
+    }
+    if (it.edge) {
+        unsigned long long n_ulp = pc.ulp, n_fma = pc.fma, n_counted = pc.counted, n_tested = tested;
+        for (int off = 16; off > 0; off >>= 1) {
+            n_ulp += __shfl_down_sync(0xffffffffu, n_ulp, off);
+            n_fma += __shfl_down_sync(0xffffffffu, n_fma, off);
+            n_counted += __shfl_down_sync(0xffffffffu, n_counted, off);
+            n_tested += __shfl_down_sync(0xffffffffu, n_tested, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            if (n_ulp) atomicAdd(&it.edge[TRJ_EDGE_ULP], n_ulp);
+            if (n_fma) atomicAdd(&it.edge[TRJ_EDGE_FMA], n_fma);
+            if (n_counted) atomicAdd(&it.edge[TRJ_EDGE_COUNTED], n_counted);
+            if (n_tested) atomicAdd(&it.edge[TRJ_EDGE_TESTED], n_tested);
+        }
+    }
+    pc = PairCounters();
+    tested = 0;
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 3) batch_pairs_kernel(BatchHeader* __restrict__ hdr,
+                                                                    const BatchItem* __restrict__ items,
+                                                                    const float4* __restrict__ packed,
+                                                                    int hist_words) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* tile = reinterpret_cast<float4*>(smem);                              // [kBatchTile]
+    unsigned* hist = reinterpret_cast<unsigned*>(smem + kBatchTile * sizeof(float4));  // [2][hist_words]
+    __shared__ int rowtab[kBatchMaxSpecies * kBatchMaxSpecies];
+    __shared__ long long unit_s;
+    const int tid = threadIdx.x;
+    unsigned* myhist = hist + ((tid >> 5) & 1) * hist_words;
+    for (int k = tid; k < 2 * hist_words; k += kBatchThreads) hist[k] = 0u;
+    const int nitems = hdr->nitems;
+    const int64_t total = hdr->total_pair;
+    int cur = -1;
+    RdfParams P;
+    int n = 0, ntile = 0;
+    int64_t off = 0;
+    PairCounters pc;
+    unsigned long long tested = 0;
+    while (true) {
+        if (tid == 0) unit_s = (long long)atomicAdd(&hdr->counter[0], 1ull);
+        __syncthreads();
+        const int64_t u = unit_s;
+        const int r = u < total ? batch_item_of<&BatchItem::pair_begin>(items, nitems, u) : -1;
+        if (r != cur) {  // block-uniform
+            if (cur >= 0) batch_pairs_flush(items[cur], hist, hist_words, pc, tested);
+            cur = r;
+            if (r >= 0) {
+                const BatchItem& it = items[r];
+                for (int d = 0; d < 3; ++d) {
+                    P.L[d] = it.L[d];
+                    P.t0[d] = it.t0[d];
+                    P.t1[d] = it.t1[d];
+                    P.t2[d] = it.t2[d];
+                }
+                P.side2 = it.side2;
+                P.side2_lo = it.side2_lo;
+                P.side2_hi = it.side2_hi;
+                P.deltar = it.deltar;
+                P.inv_deltar = it.inv_deltar;
+                P.lsmax = it.lsmax;
+                P.nsp = it.nsp;
+                P.nit = it.nit;
+                P.floor_bins = it.floor_bins;
+                n = it.n;
+                ntile = it.ntile;
+                off = it.atom_off;
+                for (int k = tid; k < P.nsp * P.nsp; k += kBatchThreads)
+                    rowtab[k] = trj_pair_row(k / P.nsp, k % P.nsp, P.nsp);
+            }
+            __syncthreads();
+        }
+        if (r < 0) break;
+        // tile pair (bi, bj), bi <= bj, of triangle index t (row bi holds ntile - bi pairs)
+        const int64_t t = u - items[r].pair_begin;
+        const double b2 = 2.0 * ntile + 1.0;
+        int bi = (int)((b2 - sqrt(b2 * b2 - 8.0 * (double)t)) * 0.5);
+        auto row_start = [&](int b) { return (int64_t)b * ntile - (int64_t)b * (b - 1) / 2; };
+        while (bi > 0 && row_start(bi) > t) --bi;
+        while (bi + 1 < ntile && row_start(bi + 1) <= t) ++bi;
+        const int bj = bi + (int)(t - row_start(bi));
+        const int j = bj * kBatchTile + tid;
+        tile[tid] = j < n ? packed[off + j] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        const int i = bi * kBatchTile + tid;
+        const float4 a = i < n ? packed[off + i] : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        const int si = __float_as_int(a.w);
+        const bool has_a = i < n && (unsigned)si < (unsigned)P.nsp;
+        const int jcount = min(kBatchTile, n - bj * kBatchTile);
+        __syncthreads();
+        tested += P.floor_bins
+                      ? batch_tile_pairs<true>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab, myhist, pc)
+                      : batch_tile_pairs<false>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab, myhist, pc);
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 struct trj_rdf_plan {
@@ -1124,5 +1253,54 @@ extern "C" int trj_rdf_plan_set_wait(trj_rdf_plan* plan, int64_t clocks, int sta
                         (long long)clocks, (long long)TRJ_WAIT_CLOCKS);
     plan->wait_clocks = clocks ? clocks : TRJ_WAIT_CLOCKS;
     plan->stall_test = stall_test ? 1 : 0;
+    return TRJ_OK;
+}
+
+// ---- fused multi-request launch: host side of the pair kernel ----------------------------------
+
+size_t trj_batch_pairs_smem(int hist_words) { return kBatchTile * sizeof(float4) + 2 * (size_t)hist_words * 4; }
+
+int trj_batch_pairs_prepare(int hist_words) {
+    return cudaFuncSetAttribute(batch_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trj_batch_pairs_smem(hist_words)) == cudaSuccess ? 0 : -1;
+}
+
+void trj_batch_launch_pairs(BatchHeader* hdr, const BatchItem* items, const float4* packed, int hist_words,
+                            int grid, cudaStream_t s) {
+    batch_pairs_kernel<<<grid, kBatchThreads, trj_batch_pairs_smem(hist_words), s>>>(hdr, items, packed, hist_words);
+}
+
+int trj_batch_pairs_occupancy(int hist_words, int* per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, batch_pairs_kernel, kBatchThreads,
+                                                         trj_batch_pairs_smem(hist_words)) == cudaSuccess ? 0 : -1;
+}
+
+int trj_batch_fill_rdf(trj_rdf_plan* plan, const float box[3], int hist_words, BatchItem* it, int* nsp) {
+    trj_ctx* ctx = plan->ctx;
+    if (plan->dim != 3) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "batch: two-dimensional pair plans run unfused");
+    if (plan->nsp > kBatchMaxSpecies)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "batch: %d species (1..%d)", plan->nsp, kBatchMaxSpecies);
+    if ((int64_t)plan->nit * plan->lsmax > hist_words)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "batch: a histogram of %d x %d bins exceeds the batch's %d words",
+                        plan->nit, plan->lsmax, hist_words);
+    // the per-frame clip of trj_rdf_accumulate (netcdf.f90:610-617)
+    const float side = min_edge(box, plan->dim);
+    plan->rcrdf_eff = fminf(plan->rcrdf_eff, side / 2.0f);
+    plan->side2 = plan->rcrdf_eff * plan->rcrdf_eff;
+    plan->cells_valid = 0;
+    for (int d = 0; d < 3; ++d) {
+        it->t0[d] = (float)(0.49 * (double)box[d]);
+        it->t1[d] = (float)(0.51 * (double)box[d]);
+        it->t2[d] = (float)(1.49 * (double)box[d]);
+    }
+    it->side2 = plan->side2;
+    it->side2_lo = (float)((double)plan->side2 * (1.0 - 1.0 / 1048576.0));
+    it->side2_hi = (float)((double)plan->side2 * (1.0 + 1.0 / 1048576.0));
+    it->deltar = plan->deltar;
+    it->inv_deltar = 1.0f / plan->deltar;
+    it->lsmax = plan->lsmax;
+    it->nit = plan->nit;
+    it->floor_bins = plan->floor_bins;
+    *nsp = plan->nsp;
     return TRJ_OK;
 }

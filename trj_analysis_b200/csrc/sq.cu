@@ -18,6 +18,7 @@
 #include <numeric>
 #include <vector>
 
+#include "batch.cuh"
 #include "sq_plan.cuh"
 
 namespace {
@@ -61,22 +62,27 @@ __device__ __forceinline__ void sincos_turn(unsigned ph, const float2* __restric
     sn = fmaf(t.y, cl, t.x * sl);
 }
 
-// Direct sum: thread owns VPT vectors; block y-index selects a slice of every species.
-// Species qsp (if any) is the charge species: each term is weighted by the charge in the entry's w.
-template <int VPT>
-__global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
-    const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp, int qsp,
-    const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
-    int nsplit, double2* __restrict__ part) {
-    __shared__ uint4 atoms[kPlainChunk];
-    __shared__ float2 turn_tab[256];
-    const int tid = threadIdx.x;
-    const int64_t vbase = (int64_t)blockIdx.x * kPlainThreads * VPT;
-    for (int k = tid; k < 256; k += kPlainThreads) {
+// cos, sin(2 pi k / 256), k = 0..255, each rounded once from FP64 (the table of sincos_turn).
+__device__ __forceinline__ void fill_turn_table(float2* turn_tab) {
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) {
         double sd, cd;
         sincospi((double)k / 128.0, &sd, &cd);
         turn_tab[k] = make_float2((float)cd, (float)sd);
-    }  // ordered before the first use by the barrier at the top of the chunk loop
+    }
+}
+
+// Direct sum of one block of vectors (bx) over one slice (by of nsplit) of every species: thread owns
+// VPT vectors.  Species qsp (if any) is the charge species: each term is weighted by the charge in the
+// entry's w.  Partials by position in the subset: part[by][species][nsub].  turn_tab must be filled
+// (fill_turn_table) before the call; the barrier at the top of the chunk loop orders it.
+template <int VPT>
+__device__ __forceinline__ void plain_block(const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off,
+                                            int nsp, int qsp, const int4* __restrict__ vecs,
+                                            const int32_t* __restrict__ subset, int nsub, int nsplit,
+                                            double2* __restrict__ part, int64_t bx, int64_t by, uint4* atoms,
+                                            const float2* turn_tab) {
+    const int tid = threadIdx.x;
+    const int64_t vbase = bx * kPlainThreads * VPT;
     unsigned nx[VPT], ny[VPT], nz[VPT];
     int vidx[VPT];
 #pragma unroll
@@ -91,7 +97,7 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
     for (int a = 0; a < nsp; ++a) {
         int64_t a0 = sp_off[a], a1 = sp_off[a + 1];
         int64_t len = a1 - a0;
-        int64_t s0 = a0 + len * blockIdx.y / nsplit, s1 = a0 + len * (blockIdx.y + 1) / nsplit;
+        int64_t s0 = a0 + len * by / nsplit, s1 = a0 + len * (by + 1) / nsplit;
         double accr[VPT], acci[VPT];
 #pragma unroll
         for (int q = 0; q < VPT; ++q) accr[q] = acci[q] = 0.0;
@@ -130,9 +136,20 @@ __global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
 #pragma unroll
         for (int q = 0; q < VPT; ++q)
             if (vidx[q] >= 0)  // partials by position in the subset: [split][species][nsub]
-                part[((int64_t)blockIdx.y * nsp + a) * nsub + vbase + q * kPlainThreads + tid] =
-                    make_double2(accr[q], acci[q]);
+                part[(by * nsp + a) * nsub + vbase + q * kPlainThreads + tid] = make_double2(accr[q], acci[q]);
     }
+}
+
+template <int VPT>
+__global__ void __launch_bounds__(kPlainThreads) sq_plain_kernel(
+    const uint4* __restrict__ phase, const int64_t* __restrict__ sp_off, int nsp, int qsp,
+    const int4* __restrict__ vecs, const int32_t* __restrict__ subset, int nsub, int64_t nvec,
+    int nsplit, double2* __restrict__ part) {
+    __shared__ uint4 atoms[kPlainChunk];
+    __shared__ float2 turn_tab[256];
+    fill_turn_table(turn_tab);
+    plain_block<VPT>(phase, sp_off, nsp, qsp, vecs, subset, nsub, nsplit, part, blockIdx.x, blockIdx.y, atoms,
+                     turn_tab);
 }
 
 // rho[a][v] = sum over splits (fixed order) for the subset's vectors.
@@ -169,14 +186,11 @@ __global__ void gather_dense_kernel(const double* __restrict__ tc_out, const int
     }
 }
 
-// One CTA per bin: out[bin][pair] += sum_v w_v Re(rho_a conj(rho_b)), fixed order.
-__global__ void bin_reduce_kernel(const double2* __restrict__ rho, const double* __restrict__ w,
-                                  const int32_t* __restrict__ bin_start, int64_t nvec, int nsp,
-                                  double* __restrict__ out) {
-    __shared__ double red[32];
-    const int bin = blockIdx.x;
-    const int v0 = bin_start[bin], v1 = bin_start[bin + 1];
-    if (v0 >= v1) return;
+// out[bin][pair] += sum_v w_v Re(rho_a conj(rho_b)) over the bin's vectors [v0, v1), by one CTA of
+// 256 threads in a fixed order (thread-strided FP64 sums, warp shuffles, warps in order).
+__device__ __forceinline__ void bin_reduce_block(const double2* __restrict__ rho, const double* __restrict__ w,
+                                                 int v0, int v1, int64_t nvec, int nsp, int bin,
+                                                 double* __restrict__ out, double* red) {
     const int nit = nsp * (nsp + 1) / 2;
     for (int a = 0; a < nsp; ++a)
         for (int b = a; b < nsp; ++b) {
@@ -195,6 +209,83 @@ __global__ void bin_reduce_kernel(const double2* __restrict__ rho, const double*
             }
             __syncthreads();
         }
+}
+
+// One CTA per bin.
+__global__ void bin_reduce_kernel(const double2* __restrict__ rho, const double* __restrict__ w,
+                                  const int32_t* __restrict__ bin_start, int64_t nvec, int nsp,
+                                  double* __restrict__ out) {
+    __shared__ double red[32];
+    const int bin = blockIdx.x;
+    const int v0 = bin_start[bin], v1 = bin_start[bin + 1];
+    if (v0 >= v1) return;
+    bin_reduce_block(rho, w, v0, v1, nvec, nsp, bin, out, red);
+}
+
+// ---- fused multi-request launch: direct sum and shell reduction of every packed frame ----------
+//
+// The same blocks as sq_plain_kernel and gather_plain_kernel + bin_reduce_kernel with each item's own
+// plan, vector blocks and splits, so an item's sums are bit-identical to the single-request plain
+// method.  Units come from global counters: (item, vector block, split) for the direct sum, (item,
+// bin) for the reduction.
+__global__ void __launch_bounds__(kPlainThreads, 2) batch_sq_kernel(BatchHeader* __restrict__ hdr,
+                                                                    const BatchItem* __restrict__ items,
+                                                                    const uint4* __restrict__ phase) {
+    __shared__ uint4 atoms[kPlainChunk];
+    __shared__ float2 turn_tab[256];
+    __shared__ long long unit_s;
+    fill_turn_table(turn_tab);
+    const int nitems = hdr->nitems;
+    const int64_t total = hdr->total_sq;
+    while (true) {
+        if (threadIdx.x == 0) unit_s = (long long)atomicAdd(&hdr->counter[1], 1ull);
+        __syncthreads();
+        const int64_t u = unit_s;
+        __syncthreads();
+        if (u >= total) break;
+        const BatchItem& it = items[batch_item_of<&BatchItem::sq_begin>(items, nitems, u)];
+        const int64_t t = u - it.sq_begin, bx = t % it.nvblk, by = t / it.nvblk;
+        if (it.vpt == 1)
+            plain_block<1>(phase + it.atom_off, it.sp_off_dev, it.nsp, -1, it.vecs, it.subset, it.nvec, it.nsplit,
+                           it.part, bx, by, atoms, turn_tab);
+        else
+            plain_block<kPlainVPT>(phase + it.atom_off, it.sp_off_dev, it.nsp, -1, it.vecs, it.subset, it.nvec,
+                                   it.nsplit, it.part, bx, by, atoms, turn_tab);
+    }
+}
+
+__global__ void __launch_bounds__(256, 2) batch_reduce_kernel(BatchHeader* __restrict__ hdr,
+                                                           const BatchItem* __restrict__ items) {
+    __shared__ double red[32];
+    __shared__ long long unit_s;
+    const int nitems = hdr->nitems;
+    const int64_t total = hdr->total_red;
+    while (true) {
+        if (threadIdx.x == 0) unit_s = (long long)atomicAdd(&hdr->counter[2], 1ull);
+        __syncthreads();
+        const int64_t u = unit_s;
+        __syncthreads();
+        if (u >= total) break;
+        const BatchItem& it = items[batch_item_of<&BatchItem::red_begin>(items, nitems, u)];
+        const int bin = (int)(u - it.red_begin);
+        const int v0 = it.bin_start[bin], v1 = it.bin_start[bin + 1];
+        if (v0 >= v1) continue;  // block-uniform
+        // rho of the bin's vectors: the splits' partials in order (gather_plain_kernel; the subset is
+        // every vector, so position = vector)
+        const int nb = v1 - v0, nsp = it.nsp, nvec = it.nvec;
+        for (int q = threadIdx.x; q < nb * nsp; q += blockDim.x) {
+            const int a = q / nb, v = v0 + q % nb;
+            double re = 0.0, im = 0.0;
+            for (int s = 0; s < it.nsplit; ++s) {
+                const double2 p = it.part[((int64_t)s * nsp + a) * nvec + v];
+                re += p.x;
+                im += p.y;
+            }
+            it.rho[(int64_t)a * nvec + v] = make_double2(re, im);
+        }
+        __syncthreads();
+        bin_reduce_block(it.rho, it.w, v0, v1, nvec, nsp, bin, it.out, red);
+    }
 }
 
 __global__ void unpermute_rho_kernel(const double2* __restrict__ rho, const int4* __restrict__ vecs,
@@ -641,5 +732,46 @@ extern "C" int trj_sq_plan_set_z_from_y(trj_sq_plan* p, int mul) {
     if (!p) return TRJ_ERR_INVALID;
     if (mul < 0 || mul > 1024) return trj_fail(p->ctx, TRJ_ERR_INVALID, "sq plan: z-from-y multiplier %d", mul);
     p->z_from_y = (unsigned)mul;
+    return TRJ_OK;
+}
+
+// ---- fused multi-request launch: host side of the direct sum -----------------------------------
+
+void trj_batch_launch_sq(BatchHeader* hdr, const BatchItem* items, const uint4* phase, int grid_sq, int grid_red,
+                         cudaStream_t s) {
+    batch_sq_kernel<<<grid_sq, kPlainThreads, 0, s>>>(hdr, items, phase);
+    batch_reduce_kernel<<<grid_red, 256, 0, s>>>(hdr, items);
+}
+
+int trj_batch_sq_occupancy(int* per_sm_sq, int* per_sm_red) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_sq, batch_sq_kernel, kPlainThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm_red, batch_reduce_kernel, 256, 0) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
+int trj_batch_fill_sq(trj_sq_plan* p, int64_t n, BatchItem* it) {
+    trj_ctx* ctx = p->ctx;
+    if (p->qsp >= 0 || p->z_from_y)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "batch: charged and planar-tile S(Q) plans run unfused");
+    if (p->nsp > kBatchMaxSpecies)
+        return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "batch: %d species (1..%d)", p->nsp, kBatchMaxSpecies);
+    if (n != p->n_atoms)
+        return trj_fail(ctx, TRJ_ERR_INVALID, "batch: n=%lld but the S(Q) plan's species counts sum to %lld",
+                        (long long)n, (long long)p->n_atoms);
+    for (int a = 0; a <= p->nsp; ++a) it->sp_off[a] = p->species_off[a];
+    it->vecs = p->vec_dev;
+    it->subset = p->plain_all_dev;
+    it->w = p->weight_dev;
+    it->bin_start = p->bin_start_dev;
+    it->sp_off_dev = p->species_off_dev;
+    it->part = p->part_dev;
+    it->rho = p->rho_dev;
+    it->nvec = (int32_t)p->nvec;
+    it->nsplit = p->nsplit_all;
+    it->vpt = plain_vpt(p->nvec);
+    it->nbins = p->nbins;
+    it->nvblk = (int32_t)((p->nvec + (int64_t)kPlainThreads * it->vpt - 1) / ((int64_t)kPlainThreads * it->vpt));
+    p->last_method = TRJ_SQ_PLAIN_FP32;
     return TRJ_OK;
 }

@@ -274,6 +274,93 @@ class SqPlan:
             pass
 
 
+class Batch:
+    """Fused launches over one frame of each of several small requests per turn (``trj_batch_*``).
+
+    Per turn: ``begin(buf)``; for every request ``stage(buf, off, xyz, species)`` and
+    ``add(buf, rdf, sq, off, n, box, hist, out)``; then ``launch(buf, stream)`` (or a CUDA graph of
+    it, captured once per buffer).  Buffer ``buf`` may be refilled only after its previous launch
+    has run (``wait(buf)``)."""
+
+    def __init__(self, ctx: Context, max_items: int = 64, max_atoms: int = 1 << 20, hist_words: int = 4096):
+        self.ctx = ctx
+        h = vp()
+        check(ctx.lib.trj_batch_create(ctx.h, int(max_items), int(max_atoms), int(hist_words), ctypes.byref(h)),
+              ctx.h, "trj_batch_create")
+        self.h = h
+        self.max_items, self.max_atoms, self.hist_words = int(max_items), int(max_atoms), int(hist_words)
+        self.xyz, self.species, self.events = [], [], [None, None]
+        for b in range(2):
+            px, ps = vp(), vp()
+            check(ctx.lib.trj_batch_staging(h, b, ctypes.byref(px), ctypes.byref(ps)), ctx.h, "trj_batch_staging")
+            fx = ctypes.cast(px, ctypes.POINTER(ctypes.c_float))
+            fs = ctypes.cast(ps, ctypes.POINTER(ctypes.c_int32))
+            self.xyz.append(np.ctypeslib.as_array(fx, shape=(self.max_atoms, 3)))
+            self.species.append(np.ctypeslib.as_array(fs, shape=(self.max_atoms,)))
+        dbytes = ctypes.c_int64()
+        check(ctx.lib.trj_batch_info(h, 0, None, None, ctypes.byref(dbytes)), ctx.h, "trj_batch_info")
+        self.device_bytes = dbytes.value
+
+    def wait(self, buf: int) -> None:
+        """Blocks until the last launch from staging buffer ``buf`` has run."""
+        if self.events[buf] is not None:
+            self.events[buf].synchronize()
+
+    def begin(self, buf: int) -> None:
+        self.wait(buf)
+        check(self.ctx.lib.trj_batch_begin(self.h, int(buf)), self.ctx.h, "trj_batch_begin")
+
+    def stage(self, buf: int, off: int, xyz: np.ndarray, species: np.ndarray) -> None:
+        n = xyz.shape[0]
+        self.xyz[buf][off:off + n] = xyz
+        self.species[buf][off:off + n] = species
+
+    def add(self, buf: int, rdf: Optional["RdfPlan"], sq: Optional["SqPlan"], off: int, n: int, box,
+            hist: Optional[torch.Tensor], out: Optional[torch.Tensor], edge: Optional[torch.Tensor] = None) -> None:
+        if rdf is not None:
+            assert hist is not None and hist.dtype == torch.int64 and hist.shape == (rdf.nit, rdf.lsmax)
+        if sq is not None:
+            assert out is not None and out.dtype == torch.float64 and out.shape == (sq.kset.nbins, sq.nit)
+        rc = self.ctx.lib.trj_batch_add(self.h, int(buf), rdf.h if rdf is not None else vp(0),
+                                        sq.h if sq is not None else vp(0), int(off), int(n), box3(box),
+                                        _ptr(hist), _ptr(edge), _ptr(out))
+        check(rc, self.ctx.h, "trj_batch_add")
+
+    def info(self, buf: int):
+        """(items, [layout units, pair tiles, direct-sum blocks, shell bins]) of the buffer's turn."""
+        ni = ctypes.c_int()
+        units = (ctypes.c_int64 * 4)()
+        check(self.ctx.lib.trj_batch_info(self.h, int(buf), ctypes.byref(ni), units, None), self.ctx.h,
+              "trj_batch_info")
+        return ni.value, list(units)
+
+    def launch(self, buf: int, stream=None) -> None:
+        check(self.ctx.lib.trj_batch_launch(self.h, int(buf), _stream(stream)), self.ctx.h, "trj_batch_launch")
+
+    def mark(self, buf: int, stream=None) -> None:
+        """Records the end of buffer ``buf``'s launch on ``stream`` (what ``wait``/``begin`` wait for)."""
+        ev = torch.cuda.Event()
+        ev.record(stream if stream is not None else torch.cuda.current_stream())
+        self.events[buf] = ev
+
+    def kernel_ms(self) -> float:
+        ms = ctypes.c_float()
+        check(self.ctx.lib.trj_batch_kernel_ms(self.h, ctypes.byref(ms)), self.ctx.h, "trj_batch_kernel_ms")
+        return ms.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.xyz, self.species = [], []
+            self.ctx.lib.trj_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DynPlan:
     """Multiple-origin time correlations (F(Q,t), Fs(Q,t), MSD) over the vectors of an SqwSet."""
 

@@ -14,6 +14,11 @@ parameters.  The loop:
   after the first frame (double-buffered pinned input);
 * on the last frame reads the accumulated counts and sums back, normalises them on the
   host, stamps the latency and frees the slot for the next request;
+* packs small requests (at most ``fuse_max_atoms`` atoms, reference bins within the batch's shared
+  histogram) into one fused launch per turn instead of slots: one frame of each packed request goes
+  through a single table copy and five kernels (layout, all-pairs histogram, direct sum, shell
+  reduction) over all of them (``engine.Batch``), replayed from a CUDA graph captured once per staging
+  buffer; their S(Q) is the direct sum, bit-identical to the per-request plain method;
 * ``cancel(rid)`` (from any thread) drops a request that is still waiting, or stops a running one
   after the frames already on its stream: once they have finished its plans, slot and HBM budget
   are released and it yields no result (its id is listed in ``cancelled``).
@@ -201,11 +206,14 @@ class _Job:
         self.done_event = None
         self.footprint = 0
         self.cancelled = False
+        self.fused = False
 
 
 class Server:
     def __init__(self, device: int = 0, slots: int = 8, hbm_budget: Optional[int] = None, n_max: int = 1 << 18,
-                 use_graphs: bool = True, autotuner: Optional[Autotuner] = None, method: Optional[str] = None):
+                 use_graphs: bool = True, autotuner: Optional[Autotuner] = None, method: Optional[str] = None,
+                 fuse_max_atoms: int = 16384, fuse_items: int = 64, fuse_atoms: int = 1 << 20,
+                 fuse_hist_words: int = 4096):
         self.ctx = engine.Context(device)
         self.alloc = TorchAllocator(self.ctx.torch_device)
         self.alloc.install(self.ctx)
@@ -222,6 +230,18 @@ class Server:
         self.cancelled: List[int] = []
         self._cancel: set = set()
         self._cancel_lock = threading.Lock()
+        # fused launches of small requests
+        self.fuse_max_atoms = int(fuse_max_atoms)
+        self.fuse_items, self.fuse_atoms, self.fuse_hist_words = int(fuse_items), int(fuse_atoms), int(fuse_hist_words)
+        self.batch: Optional[engine.Batch] = None
+        self.fuse_stream = None
+        self.fuse_graphs = [None, None]
+        self.fuse_turns = 0
+        self.fused_requests = 0
+        self.fused_frames = 0
+        if self.fuse_max_atoms > 0:
+            self.batch = engine.Batch(self.ctx, self.fuse_items, self.fuse_atoms, self.fuse_hist_words)
+            self.fuse_stream = torch.cuda.Stream(device=self.ctx.torch_device)
 
     def cancel(self, rid: int) -> None:
         """Requests cancellation of request `rid` (thread-safe; takes effect at the loop's next turn)."""
@@ -248,7 +268,7 @@ class Server:
                 job.cancelled = True
                 job.next_frame = len(job.req.frames)
                 job.done_event = torch.cuda.Event()
-                job.done_event.record(job.slot.stream)
+                job.done_event.record(self.fuse_stream if job.fused else job.slot.stream)
                 done.add(job.req.rid)
         with self._cancel_lock:
             self._cancel -= done
@@ -258,7 +278,8 @@ class Server:
         job.rdf.close()
         job.sq.close()
         self.in_use -= job.footprint
-        job.slot.req = None
+        if job.slot is not None:
+            job.slot.req = None
 
     # ---- footprint / admission ---------------------------------------------------------
     def footprint(self, req: Request, ks: refsem.KSet, method: str) -> int:
@@ -268,6 +289,89 @@ class Server:
         if method == "split":
             sq += 2 * (2 * 64) * 2 * (n + 32 * nsp) + 2 * 8 * 128 * (n + 32 * nsp) + 8 * nsp * nv * 4
         return int(rdf + sq)
+
+    # ---- fused launches -------------------------------------------------------------------
+    def _fusable(self, req: Request) -> bool:
+        if self.batch is None or req.n > self.fuse_max_atoms or req.n > self.fuse_atoms:
+            return False
+        if (req.method or self.method or "plain") != "plain":
+            return False
+        p = refsem.rdf_params(req.nsp, req.deltar, req.rcrdf, req.frames[0].box)
+        return req.nsp * (req.nsp + 1) // 2 * p.lsmax <= self.fuse_hist_words
+
+    def _start_fused(self, req: Request, fused: List[_Job]) -> Optional[_Job]:
+        if len(fused) >= self.fuse_items or sum(j.req.n for j in fused) + req.n > self.fuse_atoms:
+            return None
+        fr0 = req.frames[0]
+        sel = sorted(set(int(t) for t in np.unique(fr0.types)))[: req.nsp]
+        sp, wtypes, perm = refsem.species_by_first_appearance(fr0.types, sel)
+        bsc = list(req.bsc) if req.bsc is not None else [1.0] * req.nsp
+        ks = refsem.make_kset(req.kset, fr0.box, req.qmax, req.qmin)
+        counts = np.bincount(sp[sp >= 0], minlength=req.nsp)
+        fp = self.footprint(req, ks, "plain") - 64 * req.n  # no cell arrays
+        if self.in_use + fp > self.hbm_budget and self.in_use > 0:
+            self.admission_waits += 1
+            return None
+        job = _Job(req, None)
+        job.fused = True
+        job.species = sp.astype(np.int32)
+        job.bsc = np.array([bsc[perm[s]] for s in range(req.nsp)], np.float32)
+        job.ntype = counts
+        job.ks = ks
+        with torch.cuda.stream(self.fuse_stream):
+            # the pair plan gives the batch its cutoff, bins and species; its cell arrays stay unused
+            job.rdf = engine.RdfPlan(self.ctx, req.nsp, req.deltar, req.rcrdf, fr0.box, 0)
+            job.sq = engine.SqPlan(self.ctx, req.nsp, ks, counts)
+            job.hist = job.rdf.new_hist()
+            job.out = job.sq.new_out()
+        job.method = "plain"
+        job.cols = 0
+        job.tune = False
+        job.footprint = fp
+        self.in_use += fp
+        self.peak_in_use = max(self.peak_in_use, self.in_use)
+        self.fused_requests += 1
+        return job
+
+    def _fused_turn(self, fused: List[_Job]) -> bool:
+        """One frame of every packed request with frames left, through one fused launch."""
+        active = [j for j in fused if j.next_frame < len(j.req.frames)]
+        if not active:
+            return False
+        b, s = self.batch, self.fuse_stream
+        buf = self.fuse_turns & 1
+        b.begin(buf)  # waits until this buffer's previous launch has run
+        off = 0
+        for job in active:
+            fr = job.req.frames[job.next_frame]
+            n = job.req.n
+            b.stage(buf, off, fr.xyz, job.species)
+            b.add(buf, job.rdf, job.sq, off, n, fr.box, job.hist, job.out)
+            off += n
+            job.next_frame += 1
+        with torch.cuda.stream(s):
+            if self.use_graphs:
+                if self.fuse_graphs[buf] is None:
+                    g = torch.cuda.CUDAGraph()
+                    g.capture_begin(capture_error_mode="relaxed")
+                    try:
+                        b.launch(buf, s)
+                    finally:
+                        g.capture_end()
+                    self.fuse_graphs[buf] = g
+                self.fuse_graphs[buf].replay()
+            else:
+                b.launch(buf, s)
+            b.mark(buf, s)
+            for job in active:
+                if job.next_frame == len(job.req.frames):
+                    job.h_hist = job.hist.to("cpu", non_blocking=True)
+                    job.h_out = job.out.to("cpu", non_blocking=True)
+                    job.done_event = torch.cuda.Event()
+                    job.done_event.record(s)
+        self.fuse_turns += 1
+        self.fused_frames += len(active)
+        return True
 
     # ---- request life cycle -------------------------------------------------------------
     def _start(self, req: Request, slot: _Slot) -> Optional[_Job]:
@@ -404,23 +508,25 @@ class Server:
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
-            # admission: fill free slots while the HBM budget allows
-            for slot in self.slots:
-                if not queue:
+            # admission, in arrival order: small requests join the fused launch, others take a free
+            # slot, while the HBM budget allows
+            while queue:
+                req = queue[0]
+                if req.n > self.n_max:
+                    raise ValueError(f"request {req.rid}: {req.n} atoms exceed the server's n_max {self.n_max}")
+                if self._fusable(req):
+                    job = self._start_fused(req, [j for j in jobs if j.fused])
+                else:
+                    slot = next((sl for sl in self.slots if sl.req is None), None)
+                    job = self._start(req, slot) if slot is not None else None
+                if job is None:
                     break
-                if slot.req is None:
-                    req = queue[0]
-                    if req.n > self.n_max:
-                        raise ValueError(f"request {req.rid}: {req.n} atoms exceed the server's n_max {self.n_max}")
-                    job = self._start(req, slot)
-                    if job is None:
-                        break
-                    queue.popleft()
-                    jobs.append(job)
-            # one frame per running request per turn
-            progressed = False
+                queue.popleft()
+                jobs.append(job)
+            # one frame per running request per turn: the packed requests in one fused launch
+            progressed = self._fused_turn([j for j in jobs if j.fused])
             for job in jobs:
-                if job.next_frame < len(job.req.frames):
+                if not job.fused and job.next_frame < len(job.req.frames):
                     self._enqueue_frame(job)
                     progressed = True
             # completions
