@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--serving", type=int, default=2000, help="requests in the serving run (0: skip)")
-    ap.add_argument("--row", default="main", choices=["main", "charges", "dyn", "extras"],
+    ap.add_argument("--row", default="main", choices=["main", "charges", "dyn", "extras", "fused"],
                     help="main: the g(r)+S(Q) frame rate; charges: the same frames with per-atom charges "
                          "(g_qq, S_qq); dyn: F(Q,t)/Fs(Q,t)/MSD over time origins; extras: number "
                          "fluctuations, a two-dimensional frame and the slab analysis")
@@ -657,6 +657,102 @@ def run_dyn(args):
                             "terms_per_clk_per_sm": self_tps / (ctx.sm_count * 1.9e9)}}
 
 
+def run_fused(args):
+    """One fused turn: frame 0 of 64 small serving requests (N log-uniform in [1e3, 16384], 1-3 species,
+    cubic or 1:1:2 boxes, deltar 0.02, rcrdf min(L/2, 8), reference k-set qmax 12 qmin 3) through
+    one batch launch replayed from a CUDA graph, against the same 64 frames through the per-request
+    calls (layout, g(r), plain S(Q): the path each request takes alone).  Both time device work only
+    (inputs already staged / resident), CUDA events on the launching stream, L2 flushed between steps."""
+    import torch
+    from trj_analysis_b200 import engine, refsem
+    from trj_analysis_b200.serve import serving_workload
+    reqs = serving_workload(64, seed=3, n_lo=1e3, n_hi=16384)
+    dev = torch.device("cuda", 0)
+    ctx = engine.Context(0)
+    batch = engine.Batch(ctx, 64, 1 << 20)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    st = []
+    for r in reqs:
+        fr0 = r.frames[0]
+        sel = sorted(set(int(t) for t in np.unique(fr0.types)))[: r.nsp]
+        sp = refsem.species_by_first_appearance(fr0.types, sel)[0].astype(np.int32)
+        ks = refsem.make_kset(r.kset, fr0.box, r.qmax, r.qmin)
+        counts = np.bincount(sp, minlength=r.nsp)
+        with torch.cuda.stream(stream):
+            rdf = engine.RdfPlan(ctx, r.nsp, r.deltar, r.rcrdf, fr0.box, r.n)
+            sq = engine.SqPlan(ctx, r.nsp, ks, counts)
+            hist, out = rdf.new_hist(), sq.new_out()
+            xyz = torch.from_numpy(np.ascontiguousarray(fr0.xyz, np.float32)).to(dev)
+            spd = torch.from_numpy(sp).to(dev)
+            packed = torch.empty((r.n, 4), dtype=torch.float32, device=dev)
+            cnt = torch.zeros(16, dtype=torch.int64, device=dev)
+        st.append(dict(r=r, sp=sp, ks=ks, rdf=rdf, sq=sq, hist=hist, out=out, xyz=xyz, spd=spd, packed=packed,
+                       cnt=cnt))
+    torch.cuda.synchronize()
+    for b in (0, 1):  # both staging buffers hold the same turn
+        batch.begin(b)
+        off = 0
+        for e in st:
+            r = e["r"]
+            batch.stage(b, off, r.frames[0].xyz, e["sp"])
+            batch.add(b, e["rdf"], e["sq"], off, r.n, r.frames[0].box, e["hist"], e["out"])
+            off += r.n
+    graphs = []
+    with torch.cuda.stream(stream):
+        for b in (0, 1):
+            g = torch.cuda.CUDAGraph()
+            g.capture_begin()
+            batch.launch(b, stream)
+            g.capture_end()
+            graphs.append(g)
+    launches0 = ctx.lib.trj_ctx_launches(ctx.h)
+
+    def fused_step(i):
+        graphs[i & 1].replay()
+
+    def unfused_step(i):
+        for e in st:
+            r, box = e["r"], e["r"].frames[0].box
+            engine.pack_frame(ctx, e["xyz"], e["spd"], r.nsp, box, e["packed"], e["cnt"], stream=stream)
+            e["rdf"].accumulate(e["packed"], r.n, box, e["hist"], stream=stream)
+            e["sq"].accumulate(e["packed"], r.n, box, e["out"], engine.METHODS["plain"], stream=stream)
+
+    def timed(step, k0, k):
+        ts = []
+        for i in range(k0 + k):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 255)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                step(i)
+                b.record(stream)
+            b.synchronize()
+            if i >= k0:
+                ts.append(a.elapsed_time(b))
+        return ts
+
+    l0 = ctx.lib.trj_ctx_launches(ctx.h)
+    unf = timed(unfused_step, args.warmup, args.steps)
+    unfused_launches = (ctx.lib.trj_ctx_launches(ctx.h) - l0) / (args.warmup + args.steps)
+    fus = timed(fused_step, args.warmup, args.steps)
+    ctx.check()
+    n = np.array([e["r"].n for e in st], np.float64)
+    nvec = np.array([e["ks"].nvec for e in st], np.float64)
+    pairs = float((n * (n - 1) / 2).sum())
+    terms = float((n * nvec).sum())
+    f_ms, u_ms = statistics.median(fus), statistics.median(unf)
+    return {"metric": "fused turn: frame 0 of 64 small requests (g(r) + plain S(Q))", "value": 64.0 / (f_ms * 1e-3),
+            "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": f_ms,
+            "higher_is_better": True, "dtype": "f32 terms, f64 sums", "data": "synthetic",
+            "config": {"workload": "64 serving requests, N log-uniform [1e3, 16384]", "atoms": int(n.sum()),
+                       "kvec": int(nvec.sum()), "l2": "256 MB buffer written between steps"},
+            "fused": {"ms": f_ms, "launches": 5, "copies": 1, "pair_tests_per_s": pairs / (f_ms * 1e-3),
+                      "sq_terms_per_s": terms / (f_ms * 1e-3)},
+            "per_request": {"ms": u_ms, "launches": unfused_launches, "frames_per_s": 64.0 / (u_ms * 1e-3)},
+            "fused_vs_per_request": u_ms / f_ms, "launches_before_timing": int(launches0)}
+
+
 def run_extras(args):
     """Timings of the remaining analyses on the benchmark frame's scale:
     s2n: trj_rdf_s2n with 4096 sample points after the c3 frame's pair pass;
@@ -725,7 +821,7 @@ def run_extras(args):
 def main():
     args = parse()
     if args.row != "main":
-        res = {"charges": run_charges, "dyn": run_dyn, "extras": run_extras}[args.row](args)
+        res = {"charges": run_charges, "dyn": run_dyn, "extras": run_extras, "fused": run_fused}[args.row](args)
         print(json.dumps(res), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

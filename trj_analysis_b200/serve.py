@@ -237,6 +237,7 @@ class Server:
         self.fuse_stream = None
         self.fuse_graphs = [None, None]
         self.fuse_turns = 0
+        self._fuse_cache: Dict[tuple, bool] = {}
         self.fused_requests = 0
         self.fused_frames = 0
         if self.fuse_max_atoms > 0:
@@ -292,12 +293,17 @@ class Server:
 
     # ---- fused launches -------------------------------------------------------------------
     def _fusable(self, req: Request) -> bool:
-        if self.batch is None or req.n > self.fuse_max_atoms or req.n > self.fuse_atoms:
-            return False
-        if (req.method or self.method or "plain") != "plain":
-            return False
-        p = refsem.rdf_params(req.nsp, req.deltar, req.rcrdf, req.frames[0].box)
-        return req.nsp * (req.nsp + 1) // 2 * p.lsmax <= self.fuse_hist_words
+        key = (req.rid, id(req))
+        hit = self._fuse_cache.get(key)
+        if hit is not None:
+            return hit
+        ok = (self.batch is not None and req.n <= min(self.fuse_max_atoms, self.fuse_atoms)
+              and (req.method or self.method or "plain") == "plain")
+        if ok:
+            p = refsem.rdf_params(req.nsp, req.deltar, req.rcrdf, req.frames[0].box)
+            ok = req.nsp * (req.nsp + 1) // 2 * p.lsmax <= self.fuse_hist_words
+        self._fuse_cache[key] = ok
+        return ok
 
     def _start_fused(self, req: Request, fused: List[_Job]) -> Optional[_Job]:
         if len(fused) >= self.fuse_items or sum(j.req.n for j in fused) + req.n > self.fuse_atoms:
@@ -508,21 +514,32 @@ class Server:
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.popleft())
-            # admission, in arrival order: small requests join the fused launch, others take a free
-            # slot, while the HBM budget allows
+            # admission in arrival order within each class: small requests join the fused launch,
+            # others take a free slot, while the HBM budget allows; a request that cannot start
+            # blocks the later ones of its own class only
+            blocked = set()
+            kept = collections.deque()
             while queue:
-                req = queue[0]
+                req = queue.popleft()
                 if req.n > self.n_max:
                     raise ValueError(f"request {req.rid}: {req.n} atoms exceed the server's n_max {self.n_max}")
-                if self._fusable(req):
-                    job = self._start_fused(req, [j for j in jobs if j.fused])
-                else:
-                    slot = next((sl for sl in self.slots if sl.req is None), None)
-                    job = self._start(req, slot) if slot is not None else None
+                fuse = self._fusable(req)
+                job = None
+                if fuse not in blocked:
+                    if fuse:
+                        job = self._start_fused(req, [j for j in jobs if j.fused])
+                    else:
+                        slot = next((sl for sl in self.slots if sl.req is None), None)
+                        job = self._start(req, slot) if slot is not None else None
                 if job is None:
-                    break
-                queue.popleft()
-                jobs.append(job)
+                    blocked.add(fuse)
+                    kept.append(req)
+                    if len(blocked) == 2:
+                        kept.extend(queue)
+                        queue.clear()
+                else:
+                    jobs.append(job)
+            queue.extend(kept)
             # one frame per running request per turn: the packed requests in one fused launch
             progressed = self._fused_turn([j for j in jobs if j.fused])
             for job in jobs:
@@ -547,6 +564,7 @@ class Server:
                 elif pending and not queue:
                     time.sleep(max(0.0, min(0.002, pending[0].arrival - (time.perf_counter() - t0))))
         self.ctx.check()
+        self._fuse_cache.clear()
         return results
 
 
