@@ -26,7 +26,7 @@ struct __align__(16) BatchItem {
     int32_t nit;
     int64_t sp_off[kBatchMaxSpecies + 1];  // species offsets of the S(Q) plan within the frame
     // pair histogram (the rdf plan's geometry after the per-frame clip)
-    float t0[3], t1[3], t2[3];
+    float h1[3], h2[3], pad_h[3];        // minimum-image thresholds (rdf.cu min_image)
     float side2, side2_lo, side2_hi, deltar, inv_deltar;
     int32_t lsmax, floor_bins;
     unsigned long long* hist;            // [nit][lsmax] accumulator

@@ -43,7 +43,7 @@ constexpr int kMaxOffsets = 14;
 
 struct RdfParams {
     float L[3];
-    float t0[3], t1[3], t2[3];  // |dx| < t0 -> n=0 ; t1 < |dx| < t2 -> n=+-1 ; else exact
+    float h1[3], h2[3];         // |dx| < h1: nint(dx/L) = 0; h1 <= |dx| < h2: +-1; else the division
     float side2, side2_lo, side2_hi;
     float deltar, inv_deltar;
     int lsmax, nsp, nit;
@@ -83,12 +83,15 @@ __device__ __forceinline__ float min_image_exact(float d, float L) {
     return __fsub_rn(d, __fmul_rn(L, n));
 }
 
-// Minimum image of the reference; exact shortcuts for |d| far from L/2 and 3L/2.
-__device__ __forceinline__ float min_image(float d, float L, float t0, float t1, float t2) {
-    float a = fabsf(d);
-    if (a < t0) return d;
-    if (a > t1 && a < t2) return __fsub_rn(d, __fmul_rn(L, copysignf(1.0f, d)));
-    return min_image_exact(d, L);
+// Minimum image of the reference, d - L*nint(fl(d/L)), without the division below 3L/2: h1 (h2) is the
+// least float x >= 0 whose quotient fl(x/L) is >= 1/2 (>= 3/2), found on the host with the same FP32
+// division.  Correctly rounded division is monotonic in x, so |d| < h1 <=> nint = 0 and
+// h1 <= |d| < h2 <=> nint = +-1 (sign of d): the result is the reference's, bit for bit.
+__device__ __forceinline__ float min_image(float d, float L, float h1, float h2) {
+    const float a = fabsf(d);
+    if (a < h1) return d;
+    if (a < h2) return __fsub_rn(d, __fmul_rn(L, copysignf(1.0f, d)));
+    return min_image_exact(d, L);  // also NaN
 }
 
 // Bin of a pair by the reference's arithmetic (0: not counted).
@@ -257,9 +260,9 @@ __device__ __forceinline__ void pair(const float4& a, const float4& b, bool vali
     float dy = __fsub_rn(b.y, a.y);
     float dz = __fsub_rn(b.z, a.z);
     if (!FAST) {
-        dx = min_image(dx, p.L[0], p.t0[0], p.t1[0], p.t2[0]);
-        dy = min_image(dy, p.L[1], p.t0[1], p.t1[1], p.t2[1]);
-        dz = min_image(dz, p.L[2], p.t0[2], p.t1[2], p.t2[2]);
+        dx = min_image(dx, p.L[0], p.h1[0], p.h2[0]);
+        dy = min_image(dy, p.L[1], p.h1[1], p.h2[1]);
+        dz = min_image(dz, p.L[2], p.h1[2], p.h2[2]);
     }
     const float x2 = __fmul_rn(dx, dx);
     const float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
@@ -808,9 +811,8 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_pairs_kernel(BatchHead
                 const BatchItem& it = items[r];
                 for (int d = 0; d < 3; ++d) {
                     P.L[d] = it.L[d];
-                    P.t0[d] = it.t0[d];
-                    P.t1[d] = it.t1[d];
-                    P.t2[d] = it.t2[d];
+                    P.h1[d] = it.h1[d];
+                    P.h2[d] = it.h2[d];
                 }
                 P.side2 = it.side2;
                 P.side2_lo = it.side2_lo;
@@ -883,6 +885,16 @@ struct trj_rdf_plan {
     int64_t scratch_bytes = 0;
     trj_kernel_timer timer;
 };
+
+// Least float x >= 0 with fl(x / L) >= q in FP32 (host SSE division, correctly rounded like the
+// device's __fdiv_rn): the minimum-image thresholds of min_image.
+static float nint_threshold(float L, float q) {
+    volatile float vl = L;  // keep the division in single precision at run time
+    float x = q * L;
+    for (int k = 0; k < 256 && x > 0.f && x / vl >= q; ++k) x = nextafterf(x, 0.f);
+    for (int k = 0; k < 256 && x / vl < q; ++k) x = nextafterf(x, INFINITY);
+    return x;
+}
 
 static int nint_host(float x) {  // Fortran NINT: half away from zero
     double v = (double)x;
@@ -1079,9 +1091,8 @@ static int rdf_accumulate_impl(trj_rdf_plan* plan, const float* packed_dev, cons
     memset(&P, 0, sizeof(P));
     for (int d = 0; d < 3; ++d) {
         P.L[d] = box[d];
-        P.t0[d] = (float)(0.49 * (double)box[d]);
-        P.t1[d] = (float)(0.51 * (double)box[d]);
-        P.t2[d] = (float)(1.49 * (double)box[d]);
+        P.h1[d] = nint_threshold(box[d], 0.5f);
+        P.h2[d] = nint_threshold(box[d], 1.5f);
     }
     P.side2 = plan->side2;
     P.side2_lo = (float)((double)plan->side2 * (1.0 - 1.0 / 1048576.0));
@@ -1289,9 +1300,8 @@ int trj_batch_fill_rdf(trj_rdf_plan* plan, const float box[3], int hist_words, B
     plan->side2 = plan->rcrdf_eff * plan->rcrdf_eff;
     plan->cells_valid = 0;
     for (int d = 0; d < 3; ++d) {
-        it->t0[d] = (float)(0.49 * (double)box[d]);
-        it->t1[d] = (float)(0.51 * (double)box[d]);
-        it->t2[d] = (float)(1.49 * (double)box[d]);
+        it->h1[d] = nint_threshold(box[d], 0.5f);
+        it->h2[d] = nint_threshold(box[d], 1.5f);
     }
     it->side2 = plan->side2;
     it->side2_lo = (float)((double)plan->side2 * (1.0 - 1.0 / 1048576.0));
