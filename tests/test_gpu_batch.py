@@ -200,3 +200,48 @@ def test_batch_species_count_mismatch_is_reported(ctx, requests):
     ctx.check()  # the status word is cleared once reported
     st.close()
     batch.close()
+
+
+def test_batch_partial_items_and_tiny_frames(ctx, requests):
+    """Items with only a pair plan (atoms keep their order), only an S(Q) plan, and frames of one and
+    two atoms: each equals its single-request calls."""
+    from trj_analysis_b200.frames import Frame
+    r = next(q for q in requests if q.nsp >= 2)
+    st_full = _State(ctx, r, n_max=0)
+    st_g = _State(ctx, r, n_max=0)
+    st_s = _State(ctx, r, n_max=0)
+    fr = r.frames[0]
+    tiny = []
+    for n in (1, 2):
+        t = Frame(xyz=np.ascontiguousarray(fr.xyz[:n]), types=np.ones(n, np.int32), box=fr.box)
+        q = type(r)(rid=1000 + n, frames=[t], nsp=1, deltar=r.deltar, rcrdf=r.rcrdf, qmax=r.qmax, qmin=r.qmin)
+        tiny.append((q, _State(ctx, q, n_max=0)))
+    batch = engine.Batch(ctx, max_items=8, max_atoms=1 << 16)
+    batch.begin(0)
+    off = 0
+    for st, rdf, sq in ((st_g, st_g.rdf, None), (st_s, None, st_s.sq), (st_full, st_full.rdf, st_full.sq)):
+        batch.stage(0, off, fr.xyz, st.sp)
+        batch.add(0, rdf, sq, off, r.n, fr.box, st.hist if rdf else None, st.out if sq else None)
+        off += r.n
+    for q, st in tiny:
+        batch.stage(0, off, q.frames[0].xyz, np.zeros(q.n, np.int32))
+        batch.add(0, st.rdf, st.sq, off, q.n, fr.box, st.hist, st.out)
+        off += q.n
+    batch.launch(0)
+    torch.cuda.synchronize()
+    ctx.check()
+    h, o, _ = _single(ctx, type(r)(rid=r.rid, frames=[fr], nsp=r.nsp, deltar=r.deltar, rcrdf=r.rcrdf,
+                                   qmax=r.qmax, qmin=r.qmin))
+    assert np.array_equal(st_g.hist.cpu().numpy(), h)
+    assert np.array_equal(st_s.out.cpu().numpy(), o)
+    assert np.array_equal(st_full.hist.cpu().numpy(), h) and np.array_equal(st_full.out.cpu().numpy(), o)
+    assert not st_s.hist.any() and not st_g.out.any()
+    for q, st in tiny:
+        th, to, _ = _single(ctx, q)
+        assert np.array_equal(st.hist.cpu().numpy(), th) and np.array_equal(st.out.cpu().numpy(), to)
+        if q.n == 1:
+            assert not st.hist.any()
+        st.close()
+    for st in (st_full, st_g, st_s):
+        st.close()
+    batch.close()
