@@ -87,11 +87,11 @@ __device__ __forceinline__ float min_image_exact(float d, float L) {
 // least float x >= 0 whose quotient fl(x/L) is >= 1/2 (>= 3/2), found on the host with the same FP32
 // division.  Correctly rounded division is monotonic in x, so |d| < h1 <=> nint = 0 and
 // h1 <= |d| < h2 <=> nint = +-1 (sign of d): the result is the reference's, bit for bit.
-// Below h1 the result d - (+-0) equals d (a zero d may change sign, which its square does not see).
 __device__ __forceinline__ float min_image(float d, float L, float h1, float h2) {
     const float a = fabsf(d);
-    if (a >= h2) return min_image_exact(d, L);
-    return __fsub_rn(d, copysignf(a >= h1 ? L : 0.0f, d));  // NaN: a >= h1 is false, NaN - 0 = NaN
+    if (a < h1) return d;
+    if (a < h2) return __fsub_rn(d, __fmul_rn(L, copysignf(1.0f, d)));
+    return min_image_exact(d, L);  // also NaN
 }
 
 // Bin of a pair by the reference's arithmetic (0: not counted).
@@ -737,55 +737,16 @@ __global__ void s2n_kernel(const float4* __restrict__ sorted, const int32_t* __r
 // are those of the reference's all-pairs sweep (rdf.cuf:449-475).  Units come from a global counter;
 // a CTA keeps the counts of one item in two shared replicas (even and odd warps) and merges them into
 // that item's uint64 histogram when its next unit belongs to another item, and at exit.
-// One tile: every home thread against the staged tile.  Pairs in range are not binned where they are
-// found (a third of the lanes or fewer would run the binning): each warp appends them to its own
-// shared list (ballot + prefix) and bins 32 at a time with every lane busy.  The binned pairs and
-// their bins are the same; only the order of the integer adds changes.
 template <bool FLOOR>
 __device__ __forceinline__ unsigned batch_tile_pairs(const float4* __restrict__ tile, int jcount, const float4& a,
                                                      bool has_a, int il, bool diag, int si, const RdfParams& P,
-                                                     const int* rowtab, unsigned* myhist, PairCounters& pc,
-                                                     float4* hits, int* hrow) {
-    const unsigned lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+                                                     const int* rowtab, unsigned* myhist, PairCounters& pc) {
     unsigned tested = 0;
-    int cnt = 0;  // warp-uniform: pairs waiting in the warp's list
     for (int jj = 0; jj < jcount; ++jj) {
-        const float4 b = tile[jj];
         const bool valid = has_a && (!diag || jj > il);
         tested += valid ? 1u : 0u;
-        const float dx = min_image(__fsub_rn(b.x, a.x), P.L[0], P.h1[0], P.h2[0]);
-        const float dy = min_image(__fsub_rn(b.y, a.y), P.L[1], P.h1[1], P.h2[1]);
-        const float dz = min_image(__fsub_rn(b.z, a.z), P.L[2], P.h1[2], P.h2[2]);
-        const float x2 = __fmul_rn(dx, dx);
-        const float rr2 = __fadd_rn(__fadd_rn(x2, __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-        const int sj = __float_as_int(b.w);
-        const bool hit = valid && rr2 < P.side2_hi && (unsigned)sj < (unsigned)P.nsp;
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-            const int pos = cnt + __popc(m & lt);
-            hits[pos] = make_float4(rr2, x2, dy, dz);
-            hrow[pos] = rowtab[si * P.nsp + sj];
-        }
-        cnt += __popc(m);
-        if (cnt >= 32) {
-            __syncwarp();
-            const float4 h = hits[lane];
-            bin_pair<FLOOR, false>(h.x, h.y, h.z, h.w, hrow[lane], P, myhist, pc, nullptr, 0.f, nullptr);
-            __syncwarp();
-            if ((int)lane < cnt - 32) {
-                hits[lane] = hits[32 + lane];
-                hrow[lane] = hrow[32 + lane];
-            }
-            __syncwarp();
-            cnt -= 32;
-        }
+        pair<false, FLOOR, false>(a, tile[jj], valid, si, P, rowtab, myhist, pc, nullptr, 0.f, nullptr);
     }
-    __syncwarp();
-    if ((int)lane < cnt) {
-        const float4 h = hits[lane];
-        bin_pair<FLOOR, false>(h.x, h.y, h.z, h.w, hrow[lane], P, myhist, pc, nullptr, 0.f, nullptr);
-    }
-    __syncwarp();
     return tested;
 }
 
@@ -827,12 +788,8 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_pairs_kernel(BatchHead
     unsigned* hist = reinterpret_cast<unsigned*>(smem + kBatchTile * sizeof(float4));  // [2][hist_words]
     __shared__ int rowtab[kBatchMaxSpecies * kBatchMaxSpecies];
     __shared__ long long unit_s;
-    __shared__ float4 hits_all[kBatchThreads / 32][64];  // per warp: pairs in range waiting to be binned
-    __shared__ int hrow_all[kBatchThreads / 32][64];
     const int tid = threadIdx.x;
     unsigned* myhist = hist + ((tid >> 5) & 1) * hist_words;
-    float4* hits = hits_all[tid >> 5];
-    int* hrow = hrow_all[tid >> 5];
     for (int k = tid; k < 2 * hist_words; k += kBatchThreads) hist[k] = 0u;
     const int nitems = hdr->nitems;
     const int64_t total = hdr->total_pair;
@@ -891,10 +848,9 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_pairs_kernel(BatchHead
         const bool has_a = i < n && (unsigned)si < (unsigned)P.nsp;
         const int jcount = min(kBatchTile, n - bj * kBatchTile);
         __syncthreads();
-        tested += P.floor_bins ? batch_tile_pairs<true>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab, myhist,
-                                                        pc, hits, hrow)
-                               : batch_tile_pairs<false>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab,
-                                                         myhist, pc, hits, hrow);
+        tested += P.floor_bins
+                      ? batch_tile_pairs<true>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab, myhist, pc)
+                      : batch_tile_pairs<false>(tile, jcount, a, has_a, tid, bi == bj, si, P, rowtab, myhist, pc);
         __syncthreads();
     }
 }
