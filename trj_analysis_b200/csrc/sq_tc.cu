@@ -59,11 +59,24 @@ constexpr int kEpiWarp0 = kXyWarp0 + kXyWarps;
 constexpr int kTmaWarp = kEpiWarp0 + kEpiWarps;    // 20
 constexpr int kMmaWarp = kTmaWarp + 1;             // 21
 constexpr int kTcThreads = (kMmaWarp + 1) * 32;    // 704 (CTA-pair form)
-// One-CTA form: the X/Y factors come from per-frame tables with the B rows, so it has no factor warps.
-constexpr int k1EpiWarp0 = kBuildWarps;            // warps 8-15: accumulator drains
-constexpr int k1TmaWarp = k1EpiWarp0 + kEpiWarps;  // 16
-constexpr int k1MmaWarp = k1TmaWarp + 1;           // 17
-constexpr int k1Threads = (k1MmaWarp + 1) * 32;    // 576
+// One-CTA form: the X/Y factors come from per-frame tables through their own stage ring, so it has
+// no factor warps; the FP32 running sum of the drains lives in the epilogue warps' registers, which
+// leaves TMEM to the accumulator and a deep ring of A buffers.
+constexpr int k1EpiWarps = 16;                     // warps 8-23: drains, four warps per lane quarter
+constexpr int k1EpiWarp0 = kBuildWarps;
+constexpr int k1TmaWarp = k1EpiWarp0 + k1EpiWarps;  // 24: B rows
+constexpr int k1XyWarp = k1TmaWarp + 1;             // 25: X/Y factor blocks
+constexpr int k1MmaWarp = k1XyWarp + 1;             // 26
+constexpr int k1Threads = (k1MmaWarp + 1) * 32;     // 864
+// Running sum of an epilogue thread: 8-column chunks cg, cg + 4, ..., the first k1RegChunks of them in
+// registers, the next (columns 192-223, tiles wider than 192 columns only) in shared memory
+// [warp][8][32 lanes] (16 KB), so that the epilogue fits the 72 registers a thread of 864 has.
+constexpr int k1RegChunks = 6;
+constexpr int k1TailCol = 8 * 4 * k1RegChunks;      // 192
+constexpr int k1TailBytes = k1EpiWarps * 8 * 32 * 4;  // 16 KB
+constexpr int k1MaxABufs = 9;                       // A half-stage buffers of 32 TMEM columns
+constexpr int kXyStages = 6;                        // X/Y factor-block ring
+static_assert(k1TailCol + 32 >= 224, "running-sum chunks cover the widest tile");
 constexpr int kStageSlots = 32;  // atoms per stage: K = 64 bf16 = one 128-byte swizzle row of B
 constexpr int kBuildGroups = kBuildWarps / 4;      // builder warps per lane quarter
 constexpr int kHalfAtoms = kStageSlots / 2 / kBuildGroups;  // atoms of a half-stage per builder warp
@@ -82,11 +95,10 @@ constexpr int kYBlockBytes = kStageSlots / 2 * kTcTileNy * 16;  // 2048
 constexpr int kMaxStages = 8;
 constexpr int kChunkAtoms = 12288;  // atom slots per chunk: the Z-table rows of one chunk are ~10 MB
 constexpr int kMaxTileCols = 224;
-// TMEM columns (512 allocated): the accumulator at 0 (bmax columns, the widest tile), the running sum
-// at bmax, then as many A half-stage buffers of 32 columns (16 of packed bf16 pairs for hi, then 16
-// for lo) as fit, up to kMaxABufs: 2 for bmax = 224, 3 for 208, 4 for <= 192.
+// TMEM columns of the one-CTA form (512 allocated): the accumulator at 0 (bmax columns, the widest
+// tile), then from the next multiple of 32 as many A half-stage buffers of 32 columns (16 of packed
+// bf16 pairs for hi, then 16 for lo) as fit, up to k1MaxABufs: 9 for every bmax <= 224.
 constexpr uint32_t kTmemCols = 512;
-constexpr int kMaxABufs = 4;
 // CTA-pair form: accumulator at 0, four full-stage A buffers (32 columns hi, 32 lo) from 224; its
 // FP32 running sum lives in shared memory.
 constexpr uint32_t kPairACol = 224;
@@ -111,16 +123,16 @@ struct TcParams {
     const int32_t* cta_items;  // item ids (chunk * ntiles + tile) of every CTA, concatenated
     const int32_t* cta_off;    // gridDim.x + 1 offsets into cta_items
     const uint2* uxy;          // per slot: x and y phase fractions
-    double* part;              // [chunk][acc_stride]
+    float* part;               // [chunk][acc_stride]: each item's FP32 running sum (exact in FP64)
     int64_t acc_stride;
     int ntiles, nchunks;
     int nstages;
     int flush_stages;
-    int stage_bytes;
+    int stage_bytes;  // one B stage: hi then lo rows
     int bmax;  // B rows of a stage buffer
     int table_rows;  // Z-table rows per 32-slot block
-    uint32_t sum_col, a_col;  // TMEM columns of the running sum and of the first A buffer
-    int nabuf;                // A half-stage buffers
+    uint32_t a_col;  // TMEM column of the first A buffer
+    int nabuf;       // A half-stage buffers
     const float4* xtab;       // X factor blocks [stage][nx block][pair][16]
     const float4* ytab;       // Y factor blocks [stage][ny block][pair][8]
     int nxb, nyb, nx0min, ny0min;
@@ -144,7 +156,7 @@ struct Tc2Params {
     const int32_t* cl_items;  // item ids (chunk * npairs + pair) of every cluster, concatenated
     const int32_t* cl_off;    // nclusters + 1 offsets into cl_items
     const uint2* uxy;
-    double* part;
+    float* part;
     int64_t acc_stride;
     int npairs, nchunks;
     int nstages;
@@ -172,11 +184,12 @@ struct TcState {
     float4* xtab = nullptr;  // X/Y factor blocks of the one-CTA form
     float4* ytab = nullptr;
     int nxb = 0, nyb = 0, nx0min = 0, ny0min = 0;
-    double* part = nullptr;
+    float* part = nullptr;  // per-item FP32 sums, summed per species in FP64 by tc_reduce_kernel
     int64_t acc_stride = 0;
     CUtensorMap map_hi, map_lo, map_hi64, map_lo64;  // 16-row and 64-row boxes
     int nstages = 2, stage_bytes = 0, smem_bytes = 0, bmax = 0;
     int nabuf = 2;  // A half-stage buffers in TMEM
+    int a_col = 0;  // TMEM column of the first A buffer
     int flush_stages = 8;  // 256 atoms per FP32 tensor-core run between drains
     int grid = 0;
     // CTA-pair (cta_group::2) form
@@ -240,6 +253,12 @@ __device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[1
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, uint32_t (&r)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -435,8 +454,8 @@ __global__ void __launch_bounds__(k1Threads, 1)
                  const __grid_constant__ CUtensorMap map_hi64, const __grid_constant__ CUtensorMap map_lo64, TcParams p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages];
-    __shared__ __align__(8) uint64_t full_a[kMaxABufs], empty_a[kMaxABufs], acc_full, acc_empty, mma_done;
+    __shared__ __align__(8) uint64_t full_b[kMaxStages], empty_b[kMaxStages], full_xy[kXyStages], empty_xy[kXyStages];
+    __shared__ __align__(8) uint64_t full_a[k1MaxABufs], empty_a[k1MaxABufs], acc_full, acc_empty, mma_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag_s;
     volatile int& abort_flag = abort_flag_s;
@@ -446,8 +465,11 @@ __global__ void __launch_bounds__(k1Threads, 1)
     const int NA = p.nabuf;
     const int F = p.flush_stages;
     const int item0 = p.cta_off[blockIdx.x], item1 = p.cta_off[blockIdx.x + 1];
-    // stage layout: B hi [bmax rows x 128 B], B lo, the X factor block, the Y factor block
+    // shared memory: the ring of B stages (hi rows, then lo rows), then the ring of X/Y factor blocks
     auto stage_ptr = [&](int slot) { return smem + (size_t)slot * p.stage_bytes; };
+    uint8_t* const xy_base = smem + (size_t)NS * p.stage_bytes;
+    auto xy_ptr = [&](int slot) { return xy_base + (size_t)slot * (kXBlockBytes + kYBlockBytes); };
+    uint8_t* const tail_base = xy_base + (size_t)kXyStages * (kXBlockBytes + kYBlockBytes);  // if bmax > 192
 
     if (tid == 0) {
         abort_flag = 0;
@@ -455,12 +477,16 @@ __global__ void __launch_bounds__(k1Threads, 1)
             trj_mbar_init(&full_b[s], 1);
             trj_mbar_init(&empty_b[s], 1);
         }
-        for (int b = 0; b < kMaxABufs; ++b) {
+        for (int s = 0; s < kXyStages; ++s) {
+            trj_mbar_init(&full_xy[s], 1);
+            trj_mbar_init(&empty_xy[s], kBuildWarps);
+        }
+        for (int b = 0; b < k1MaxABufs; ++b) {
             trj_mbar_init(&full_a[b], kBuildWarps);
             trj_mbar_init(&empty_a[b], 1);
         }
         trj_mbar_init(&acc_full, 1);
-        trj_mbar_init(&acc_empty, kEpiWarps);
+        trj_mbar_init(&acc_empty, k1EpiWarps);
         trj_mbar_init(&mma_done, 1);
         trj_fence_mbar_init();
     }
@@ -486,8 +512,7 @@ __global__ void __launch_bounds__(k1Threads, 1)
                 const TcTile T = p.tiles[it % p.ntiles];
                 const TcChunk C = p.chunks[it / p.ntiles];
                 const int nst = (C.slot1 - C.slot0) / kStageSlots;
-                const unsigned bytes = (unsigned)(2 * T.ncols * 128 + kXBlockBytes + kYBlockBytes);
-                const int bx = (T.nx0 - p.nx0min) / kTcTileNx, by = (T.ny0 - p.ny0min) / kTcTileNy;
+                const unsigned bytes = (unsigned)(2 * T.ncols * 128);
                 const int n64 = T.ncols / 64;  // B rows as 64-row boxes, then 16-row boxes
                 for (int s = 0; s < nst; ++s) {
                     if (!timed_wait(&empty_b[slot], phase ^ 1, p.status)) {
@@ -496,7 +521,6 @@ __global__ void __launch_bounds__(k1Threads, 1)
                     }
                     uint8_t* bh = stage_ptr(slot);
                     uint8_t* bl = bh + p.bmax * 128;
-                    uint8_t* xf = bl + p.bmax * 128;
                     trj_mbar_arrive_expect_tx(&full_b[slot], bytes);
                     const int slot0 = C.slot0 + s * kStageSlots;
                     // rows of this stage's 32-slot block: contiguous 128-byte rows from row0
@@ -510,10 +534,6 @@ __global__ void __launch_bounds__(k1Threads, 1)
                         tma_load_2d(bh + r * 128, &map_hi, 0, row0 + r, &full_b[slot]);
                         tma_load_2d(bl + r * 128, &map_lo, 0, row0 + r, &full_b[slot]);
                     }
-                    const int64_t stg = slot0 / kStageSlots;
-                    trj_bulk_g2s(xf, p.xtab + (stg * p.nxb + bx) * (kXBlockBytes / 16), kXBlockBytes, &full_b[slot]);
-                    trj_bulk_g2s(xf + kXBlockBytes, p.ytab + (stg * p.nyb + by) * (kYBlockBytes / 16), kYBlockBytes,
-                                 &full_b[slot]);
                     ++issued;
                     if (++slot == NS) {
                         slot = 0;
@@ -529,6 +549,43 @@ __global__ void __launch_bounds__(k1Threads, 1)
                     phase ^= 1;
                 }
                 trj_mbar_wait(&full_b[slot], phase);
+            }
+        }
+    } else if (warp == k1XyWarp) {
+        if (lane == 0) {
+            // X and Y factor blocks of every stage, released by the builders once they have read them
+            int slot = 0, issued = 0;
+            unsigned phase = 0;
+            for (int li = item0; li < item1 && !abort_flag; ++li) {
+                const int it = p.cta_items[li];
+                const TcTile T = p.tiles[it % p.ntiles];
+                const TcChunk C = p.chunks[it / p.ntiles];
+                const int nst = (C.slot1 - C.slot0) / kStageSlots;
+                const int bx = (T.nx0 - p.nx0min) / kTcTileNx, by = (T.ny0 - p.ny0min) / kTcTileNy;
+                for (int s = 0; s < nst; ++s) {
+                    if (!timed_wait(&empty_xy[slot], phase ^ 1, p.status)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t* xf = xy_ptr(slot);
+                    trj_mbar_arrive_expect_tx(&full_xy[slot], (unsigned)(kXBlockBytes + kYBlockBytes));
+                    const int64_t stg = (C.slot0 + s * kStageSlots) / kStageSlots;
+                    trj_bulk_g2s(xf, p.xtab + (stg * p.nxb + bx) * (kXBlockBytes / 16), kXBlockBytes, &full_xy[slot]);
+                    trj_bulk_g2s(xf + kXBlockBytes, p.ytab + (stg * p.nyb + by) * (kYBlockBytes / 16), kYBlockBytes,
+                                 &full_xy[slot]);
+                    ++issued;
+                    if (++slot == kXyStages) {
+                        slot = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            for (int q = 0; q < kXyStages && q < issued; ++q) {
+                if (--slot < 0) {
+                    slot = kXyStages - 1;
+                    phase ^= 1;
+                }
+                trj_mbar_wait(&full_xy[slot], phase);
             }
         }
     } else if (warp == k1MmaWarp) {
@@ -608,12 +665,18 @@ __global__ void __launch_bounds__(k1Threads, 1)
             trj_mbar_wait(&mma_done, 0);
         }
     } else if (warp >= k1EpiWarp0) {
-        // ---- epilogue: add each run of the accumulator into the TMEM running sum; the item's
-        //      last run writes (sum + run) to this CTA's FP64 block once ----
+        // ---- epilogue: each run of the accumulator is added (round to nearest) into an FP32 running
+        //      sum; the item's last run writes sum + run to this CTA's FP32 block once.  Warp (quarter
+        //      q4, group cg) owns the 8-column chunks cg, cg + 4, cg + 8, ... of TMEM lanes
+        //      32 q4 .. 32 q4 + 31 (the tile's rows): the first k1RegChunks in registers, the one at
+        //      columns >= k1TailCol in this warp's shared-memory tail. ----
         const int q4 = warp & 3;
-        const int c0 = 16 * ((warp - k1EpiWarp0) >> 2);  // first 16-column chunk of this warp
+        const int cg = (warp - k1EpiWarp0) >> 2;
         const int row = 32 * q4 + lane;
-        const uint32_t lanes = (uint32_t)(32 * q4) << 16;
+        // this warp's first column in TMEM (lane quarter in the high half); chunk i sits 32 i further
+        const uint32_t ta = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(8 * cg);
+        float* tail = reinterpret_cast<float*>(tail_base) + (warp - k1EpiWarp0) * 256 + lane;  // [8][32]
+        float sum[k1RegChunks][8];
         int fg = 0;
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
@@ -623,7 +686,8 @@ __global__ void __launch_bounds__(k1Threads, 1)
             const TcChunk C = p.chunks[chunk];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
             const int nflush = (nst + F - 1) / F;
-            double* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + row;
+            const int lim = T.ncols - 8 * cg;  // chunk i is in the tile when 32 i < lim
+            float* dst = p.part + (int64_t)chunk * p.acc_stride + T.acc_off + (int64_t)(8 * cg) * 128 + row;
             for (int f = 0; f < nflush; ++f, ++fg) {
                 const bool ok = trj_mbar_wait(&acc_full, fg & 1);
                 if (!__all_sync(0xffffffffu, ok)) {
@@ -634,28 +698,40 @@ __global__ void __launch_bounds__(k1Threads, 1)
                 }
                 tc_fence_after();
                 const bool last = f == nflush - 1;
-                const uint32_t ta = tmem + lanes, ts = tmem + lanes + p.sum_col;
-                for (int c = c0; c < T.ncols; c += 32) {  // ncols is a multiple of 16
-                    uint32_t a0[16], s0[16];
-                    tmem_ld16_nowait(ta + (uint32_t)c, a0);
-                    if (f > 0) tmem_ld16_nowait(ts + (uint32_t)c, s0);
-                    tmem_wait_ld();
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
-                        const float v = __uint_as_float(a0[k]);
-                        s0[k] = __float_as_uint(f > 0 ? __fadd_rn(v, __uint_as_float(s0[k])) : v);
-                    }
-                    if (last) {
+                for (int i = 0; i < k1RegChunks; ++i) {
+                    if (32 * i < lim) {  // warp-uniform
+                        uint32_t a[8];
+                        tmem_ld8_nowait(ta + (uint32_t)(32 * i), a);
+                        tmem_wait_ld();
 #pragma unroll
-                        for (int k = 0; k < 16; ++k) dst[(int64_t)(c + k) * 128] = (double)__uint_as_float(s0[k]);
-                    } else {
-                        tmem_st16(ts + (uint32_t)c, s0);
+                        for (int k = 0; k < 8; ++k)
+                            sum[i][k] = f > 0 ? __fadd_rn(__uint_as_float(a[k]), sum[i][k]) : __uint_as_float(a[k]);
                     }
                 }
-                if (!last) tmem_wait_st();
+                if (k1TailCol < lim) {
+                    uint32_t a[8];
+                    tmem_ld8_nowait(ta + (uint32_t)k1TailCol, a);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const float v = f > 0 ? __fadd_rn(__uint_as_float(a[k]), tail[32 * k]) : __uint_as_float(a[k]);
+                        if (last) dst[(k1TailCol + k) * 128] = v;
+                        else tail[32 * k] = v;
+                    }
+                }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&acc_empty);
+                if (last) {
+#pragma unroll
+                    for (int i = 0; i < k1RegChunks; ++i) {
+                        if (32 * i < lim) {
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) dst[(32 * i + k) * 128] = sum[i][k];
+                        }
+                    }
+                }
             }
         }
     } else {
@@ -666,23 +742,22 @@ __global__ void __launch_bounds__(k1Threads, 1)
         const int nxl = m & 15, nyl = m >> 4;
         const uint32_t lanes = (uint32_t)(32 * q) << 16;
         int ab = 0, slot = 0;
-        unsigned aphase = 0, phase = 0;  // A ring (NA half-stage buffers) in the MMA warp's order; B ring
+        unsigned aphase = 0, phase = 0;  // A ring (NA half-stage buffers) in the MMA warp's order; X/Y ring
         bool stop = false;
         for (int li = item0; li < item1 && !stop; ++li) {
             const int it = p.cta_items[li];
             const TcChunk C = p.chunks[it / p.ntiles];
             const int nst = (C.slot1 - C.slot0) / kStageSlots;
             for (int s = 0; s < nst && !stop; ++s) {
-                // the stage's B rows and factor blocks (released by the MMA warp's commit, which follows
-                // this stage's full_a arrivals and so every read below)
-                const bool ok = trj_mbar_wait(&full_b[slot], phase);
+                // the stage's X and Y factor blocks
+                const bool ok = trj_mbar_wait(&full_xy[slot], phase);
                 if (__any_sync(0xffffffffu, !ok || abort_flag)) {
                     if (lane == 0) trj_raise(p.status, TRJ_DEV_TIMEOUT);
                     abort_flag = 1;
                     stop = true;
                     break;
                 }
-                const float4* xf = reinterpret_cast<const float4*>(stage_ptr(slot) + 2 * p.bmax * 128);
+                const float4* xf = reinterpret_cast<const float4*>(xy_ptr(slot));
                 const float4* yf = xf + kXBlockBytes / 16;
                 // Half-stage 0 is built and stored, half-stage 1 built while those stores drain; then
                 // each half is released to the MMA warp once its own stores are complete.
@@ -711,6 +786,9 @@ __global__ void __launch_bounds__(k1Threads, 1)
                 }
                 uint32_t hw1[kHalfAtoms], lw1[kHalfAtoms];
                 build_row_tab(xf, yf, nxl, nyl, (16 + kHalfAtoms * g) / 2, hw1, lw1);
+                // every read of this stage's factor blocks is done: hand the buffer back
+                __syncwarp();
+                if (lane == 0) trj_mbar_arrive(&empty_xy[slot]);
                 tmem_wait_st();  // half-stage 0's stores
                 tc_fence_before();
                 __syncwarp();
@@ -729,7 +807,7 @@ __global__ void __launch_bounds__(k1Threads, 1)
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) trj_mbar_arrive(&full_a[hb1]);
-                if (++slot == NS) {
+                if (++slot == kXyStages) {
                     slot = 0;
                     phase ^= 1;
                 }
@@ -1017,7 +1095,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const int tile = P.tile[rank];
             const int coff = P.coff[rank];
             int own = 0;
-            double* dst = nullptr;
+            float* dst = nullptr;
             if (tile >= 0) {
                 const TcTile T = p.tiles[tile];
                 own = T.ncols;
@@ -1054,7 +1132,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
                                 for (int e = 0; e < 4; ++e) {
                                     const int oc = c + 4 * k4 + e - coff;  // own column
-                                    if (oc >= 0 && oc < own) dst[(int64_t)oc * 128] = (double)vv[e];
+                                    if (oc >= 0 && oc < own) dst[(int64_t)oc * 128] = vv[e];
                                 }
                             }
                         } else {
@@ -1162,7 +1240,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
 // tc_out[tile][a][col][row] = sum over species a's chunks (fixed order) of the FP64 blocks.
 // Grid (element blocks, tile, species): one thread per output element.
-__global__ void tc_reduce_kernel(const double* __restrict__ part, int64_t acc_stride, const TcTile* __restrict__ tiles,
+__global__ void tc_reduce_kernel(const float* __restrict__ part, int64_t acc_stride, const TcTile* __restrict__ tiles,
                                  const SqTile* __restrict__ stiles, const int32_t* __restrict__ chunk_begin, int nsp,
                                  double* __restrict__ out) {
     const int t = blockIdx.y, a = blockIdx.z;
@@ -1171,9 +1249,9 @@ __global__ void tc_reduce_kernel(const double* __restrict__ part, int64_t acc_st
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     const int k0 = chunk_begin[a], k1 = chunk_begin[a + 1];
-    const double* src = part + T.acc_off + e;
+    const float* src = part + T.acc_off + e;
     double s = 0.0;
-    for (int k = k0; k < k1; ++k) s += __ldcs(src + (int64_t)k * acc_stride);
+    for (int k = k0; k < k1; ++k) s += (double)__ldcs(src + (int64_t)k * acc_stride);
     out[stiles[t].out_off + (int64_t)a * n + e] = s;
 }
 
@@ -1359,7 +1437,9 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
         return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile of %d columns > %d", st->bmax, kMaxTileCols);
     st->nz_min = nz_min;
     st->table_rows = 2 * (nz_max - nz_min + 1);
-    st->nabuf = std::min(kMaxABufs, (int)(kTmemCols - 2 * st->bmax) / 32);  // bmax <= 224: at least 2
+    // A ring from the first multiple of 32 columns after the accumulator
+    st->a_col = (st->bmax + 31) / 32 * 32;
+    st->nabuf = std::min(k1MaxABufs, (int)(kTmemCols - st->a_col) / 32);  // 9 for every bmax <= 224
     const int ntiles = (int)plan->tiles.size();
     std::vector<TcTile> tt(ntiles);
     int64_t acc = 0;
@@ -1391,13 +1471,17 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     }
     st->chunk_of_species_begin[nsp] = (int)st->chunks.size();
     if (st->chunks.empty()) return TRJ_OK;
-    // shared memory: a ring of B stages (hi, lo, x/y phases), then the two X/Y factor buffers
-    // shared memory: a ring of stages, each B hi, B lo and the stage's X and Y factor blocks
-    st->stage_bytes = (2 * st->bmax * 128 + kXBlockBytes + kYBlockBytes + 1023) / 1024 * 1024;
-    const int avail = (int)ctx->smem_optin - 2048;
+    // shared memory: a ring of B stages (hi rows, then lo rows; 256 * bmax bytes, a multiple of 4096,
+    // so every stage starts on the 1024-byte boundary of the 128-byte swizzle), then the ring of
+    // kXyStages X/Y factor-block stages
+    st->stage_bytes = 2 * st->bmax * 128;
+    // kXyStages X/Y factor-block stages, and for tiles wider than k1TailCol columns the epilogue's
+    // shared-memory tail of the running sum
+    const int xy_bytes = kXyStages * (kXBlockBytes + kYBlockBytes) + (st->bmax > k1TailCol ? k1TailBytes : 0);
+    const int avail = (int)ctx->smem_optin - 2048 - xy_bytes;
     st->nstages = std::min(kMaxStages, avail / st->stage_bytes);
     if (st->nstages < 2) return trj_fail(ctx, TRJ_ERR_UNSUPPORTED, "tensor path: tile too wide for shared memory");
-    st->smem_bytes = st->nstages * st->stage_bytes + 1024;
+    st->smem_bytes = st->nstages * st->stage_bytes + xy_bytes + 1024;
     // X/Y factor blocks: every 16-nx (8-ny) block a tile starts at
     int nxmax = tt[0].nx0, nymax = tt[0].ny0;
     st->nx0min = tt[0].nx0;
@@ -1450,7 +1534,7 @@ int trj_sq_tc_prepare(trj_sq_plan* plan) {
     const int64_t nstage_tot = st->total_slots / kStageSlots;
     const size_t xtab_bytes = (size_t)nstage_tot * st->nxb * kXBlockBytes;
     const size_t ytab_bytes = (size_t)nstage_tot * st->nyb * kYBlockBytes;
-    size_t part_bytes = sizeof(double) * (size_t)st->acc_stride * st->chunks.size();
+    size_t part_bytes = sizeof(float) * (size_t)st->acc_stride * st->chunks.size();
     std::vector<int32_t> cb(st->chunk_of_species_begin.begin(), st->chunk_of_species_begin.end());
     if (trj_dev_alloc(ctx, (void**)&st->tab_hi, tab_bytes) != cudaSuccess ||
         trj_dev_alloc(ctx, (void**)&st->tab_lo, tab_bytes) != cudaSuccess ||
@@ -1544,8 +1628,7 @@ int trj_sq_tc_run(trj_sq_plan* plan, const float box[3], cudaStream_t s) {
     P.stage_bytes = st->stage_bytes;
     P.bmax = st->bmax;
     P.table_rows = st->table_rows;
-    P.sum_col = (uint32_t)st->bmax;
-    P.a_col = (uint32_t)(2 * st->bmax);
+    P.a_col = (uint32_t)st->a_col;
     P.nabuf = st->nabuf;
     P.xtab = st->xtab;
     P.ytab = st->ytab;
